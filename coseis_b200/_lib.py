@@ -1,0 +1,134 @@
+"""ctypes binding of libsordgpu.so (include/sordgpu.h).
+
+There is no CPU implementation behind this module: if the shared library is
+missing or no CUDA device is present, every entry point raises.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, 'libsordgpu.so')
+
+# every symbol declared in include/sordgpu.h
+SYMBOLS = [
+    'sord_create', 'sord_step', 'sord_run', 'sord_run_directory',
+    'sord_get_field', 'sord_info', 'sord_stats', 'sord_last_step_ms',
+    'sord_kernel_launches', 'sord_last_error', 'sord_error_string',
+    'sord_destroy',
+]
+
+_lib = None
+
+
+class SordError(RuntimeError):
+    """Error returned by the solver; ``code`` is the SORD_E_* value."""
+    def __init__(self, code, msg):
+        RuntimeError.__init__(self, msg)
+        self.code = code
+
+
+def load():
+    """Load libsordgpu.so (raises OSError if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIBPATH):
+        raise OSError('libsordgpu.so not built: run coseis_b200/build.py')
+    lib = ctypes.CDLL(LIBPATH)
+    P = ctypes.c_void_p
+    lib.sord_create.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(P)]
+    lib.sord_create.restype = ctypes.c_int
+    lib.sord_step.argtypes = [P, ctypes.c_int]
+    lib.sord_step.restype = ctypes.c_int
+    lib.sord_run.argtypes = [P]
+    lib.sord_run.restype = ctypes.c_int
+    lib.sord_run_directory.argtypes = [ctypes.c_char_p, ctypes.c_int]
+    lib.sord_run_directory.restype = ctypes.c_int
+    lib.sord_get_field.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(ctypes.c_float), ctypes.c_size_t]
+    lib.sord_get_field.restype = ctypes.c_int
+    lib.sord_info.argtypes = [P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+    lib.sord_info.restype = ctypes.c_int
+    lib.sord_stats.argtypes = [P, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
+    lib.sord_stats.restype = ctypes.c_int
+    lib.sord_last_step_ms.argtypes = [P]
+    lib.sord_last_step_ms.restype = ctypes.c_double
+    lib.sord_kernel_launches.argtypes = [P]
+    lib.sord_kernel_launches.restype = ctypes.c_longlong
+    lib.sord_last_error.argtypes = [P]
+    lib.sord_last_error.restype = ctypes.c_char_p
+    lib.sord_error_string.argtypes = [ctypes.c_int]
+    lib.sord_error_string.restype = ctypes.c_char_p
+    lib.sord_destroy.argtypes = [P]
+    lib.sord_destroy.restype = None
+    _lib = lib
+    return lib
+
+
+def _check(rc, handle=None):
+    if rc != 0:
+        lib = load()
+        msg = lib.sord_last_error(handle).decode(errors='replace')
+        name = lib.sord_error_string(rc).decode()
+        raise SordError(rc, '%s: %s' % (name, msg))
+
+
+def run_directory(path, device=0):
+    """Run the staged ``sord.in`` in ``path`` (the whole of ``sord.x``)."""
+    lib = load()
+    _check(lib.sord_run_directory(os.fsencode(path), device))
+
+
+class Solver(object):
+    """One simulation handle: ``Solver(workdir, text)`` runs the setup;
+    ``step(n)`` advances n time steps; ``close()`` frees the device memory."""
+
+    def __init__(self, workdir, sord_in_text, device=0):
+        lib = load()
+        h = ctypes.c_void_p()
+        _check(lib.sord_create(os.fsencode(workdir), sord_in_text.encode(), device, ctypes.byref(h)))
+        self._h = h
+
+    def step(self, n=1):
+        _check(load().sord_step(self._h, n), self._h)
+
+    def run(self):
+        _check(load().sord_run(self._h), self._h)
+
+    def info(self):
+        nn = (ctypes.c_int * 3)()
+        it = ctypes.c_int()
+        nt = ctypes.c_int()
+        _check(load().sord_info(self._h, nn, ctypes.byref(it), ctypes.byref(nt)), self._h)
+        return list(nn), it.value, nt.value
+
+    def field(self, name):
+        import numpy as np
+        nn, _, _ = self.info()
+        cell = name in ('lam', 'mu', 'yy', 'vc')
+        shape = [n - 1 if cell else n for n in nn]
+        out = np.empty(shape[::-1], dtype=np.float32)
+        ptr = out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        _check(load().sord_get_field(self._h, name.encode(), ptr, out.size), self._h)
+        return out.T
+
+    def stats(self):
+        out = (ctypes.c_double * 16)()
+        n = load().sord_stats(self._h, out, 16)
+        return list(out)[:n]
+
+    def last_step_ms(self):
+        return load().sord_last_step_ms(self._h)
+
+    def kernel_launches(self):
+        return load().sord_kernel_launches(self._h)
+
+    def close(self):
+        if getattr(self, '_h', None):
+            load().sord_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

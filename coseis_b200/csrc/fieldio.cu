@@ -1,0 +1,595 @@
+// Field-I/O engine (sord/input_output.f90:103-591) with device-side data
+// movement:
+//   non-disk ops  = + * (=~ +~ *~ with the counter hash) @-cubes  -> one
+//                 kernel over the strided region; '.' -> point injection
+//   disk output   '=>' gathers a strided region into a device record buffer,
+//                 '.>' probes (trilinear, <= 8 terms) are batched: one
+//                 launch per hook serves every firing probe; records are
+//                 copied to the host and appended to the file every nb
+//                 samples, at it2 and every itio steps
+//   disk input    host-side: the field is copied down, the op applied with
+//                 the reference's buffer / interpolation / half-dimension
+//                 fill rules, and copied back (setup inputs and rare
+//                 time-varying inputs only)
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+
+#include "sord.cuh"
+
+namespace sordgpu {
+
+#define FCHK(s) do { (s).launches++; SORD_CUDA(cudaGetLastError()); } while (0)
+
+__device__ __forceinline__ unsigned long long f_splitmix(unsigned long long z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+__device__ __forceinline__ float f_urand(unsigned long long call, unsigned long long idx) {
+    unsigned long long h = f_splitmix(f_splitmix(call * 0x100000001B3ull + 0x5151) ^ idx);
+    return (float)(h >> 40) * (1.0f / 16777216.0f);
+}
+
+struct Region {
+    int n[3];           // field extents
+    int i1[3], i2[3], di[3];
+    long long vsy, vsz; // volume strides (random-number index, like s1 of the reference)
+};
+
+// op: 0 '=', 1 '+', 2 '*', 3 '=~', 4 '+~', 5 '*~'
+__global__ void k_region_op(float* f, Region R, int op, float val, unsigned long long call) {
+    long long c0 = (R.i2[0] - R.i1[0]) / R.di[0] + 1, c1 = (R.i2[1] - R.i1[1]) / R.di[1] + 1, c2 = (R.i2[2] - R.i1[2]) / R.di[2] + 1;
+    long long n = c0 * c1 * c2;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        int j = R.i1[0] + R.di[0] * (int)(t % c0), k = R.i1[1] + R.di[1] * (int)((t / c0) % c1), l = R.i1[2] + R.di[2] * (int)(t / (c0 * c1));
+        long long q = (j - 1) + (long long)R.n[0] * ((k - 1) + (long long)R.n[1] * (l - 1));
+        float F = f[q];
+        if (op == 0) F = val;
+        else if (op == 1) F = F + val;
+        else if (op == 2) F = F * val;
+        else {
+            float r = f_urand(call, (unsigned long long)((j - 1) + R.vsy * (k - 1) + R.vsz * (l - 1)));
+            if (op == 3) F = val * r;
+            else if (op == 4) F = F + val * r;
+            else F = F * val * r;
+        }
+        f[q] = F;
+    }
+}
+
+// '@' cube ops: node fields test node coordinates, cell fields cell centres
+__global__ void k_cube(float* f, Region R, const float* x0, const float* x1, const float* x2, Geom g, int cell, int pax,
+                       int pidx, int op, float val, float a0, float a1, float a2, float b0, float b1, float b2) {
+    long long c0 = (R.i2[0] - R.i1[0]) / R.di[0] + 1, c1 = (R.i2[1] - R.i1[1]) / R.di[1] + 1, c2 = (R.i2[2] - R.i1[2]) / R.di[2] + 1;
+    long long n = c0 * c1 * c2;
+    const float* X[3] = {x0, x1, x2};
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        int p[3] = {R.i1[0] + R.di[0] * (int)(t % c0), R.i1[1] + R.di[1] * (int)((t / c0) % c1), R.i1[2] + R.di[2] * (int)(t / (c0 * c1))};
+        int v[3] = {p[0], p[1], p[2]};
+        if (pax >= 0) v[pax] = pidx;
+        long long q = g.idx(v[0], v[1], v[2]);
+        float c[3];
+        for (int a = 0; a < 3; a++) {
+            const float* x = X[a];
+            if (cell)
+                c[a] = 0.125f * (x[q] + x[q + 1 + g.sy + g.sz] + x[q + g.sy + g.sz] + x[q + 1] + x[q + 1 + g.sz] + x[q + g.sy] +
+                                 x[q + 1 + g.sy] + x[q + g.sz]);
+            else
+                c[a] = x[q];
+        }
+        if (c[0] >= a0 && c[0] <= b0 && c[1] >= a1 && c[1] <= b1 && c[2] >= a2 && c[2] <= b2) {
+            long long fq = (p[0] - 1) + (long long)R.n[0] * ((p[1] - 1) + (long long)R.n[1] * (p[2] - 1));
+            float F = f[fq];
+            if (op == 0) F = val;
+            else if (op == 1) F = F + val;
+            else F = F * val;
+            f[fq] = F;
+        }
+    }
+}
+
+// '=>' gather of a strided region into one record
+__global__ void k_gather(const float* f, Region R, float* dst) {
+    long long c0 = (R.i2[0] - R.i1[0]) / R.di[0] + 1, c1 = (R.i2[1] - R.i1[1]) / R.di[1] + 1, c2 = (R.i2[2] - R.i1[2]) / R.di[2] + 1;
+    long long n = c0 * c1 * c2;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        int j = R.i1[0] + R.di[0] * (int)(t % c0), k = R.i1[1] + R.di[1] * (int)((t / c0) % c1), l = R.i1[2] + R.di[2] * (int)(t / (c0 * c1));
+        dst[t] = f[(j - 1) + (long long)R.n[0] * ((k - 1) + (long long)R.n[1] * (l - 1))];
+    }
+}
+
+// '.>' probes: acc = acc + f(j,k,l) * r over <= 8 terms in loop order
+struct Probe {
+    long long idx[8];
+    float r[8];
+    int n;
+};
+struct ProbeBatch {
+    int count;
+    const Probe* probes;  // device table (all probes)
+    int id[128];          // probe ids firing now
+    float* dst[128];      // destination of each
+};
+__global__ void k_probe(const float* f, ProbeBatch b) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= b.count) return;
+    const Probe& P = b.probes[b.id[i]];
+    float acc = 0.f;
+    for (int t = 0; t < P.n; t++) acc = acc + f[P.idx[t]] * P.r[t];
+    *b.dst[i] = acc;
+}
+
+// ------------------------------------------------------------ host
+static unsigned gf(long long n) {
+    long long b = (n + 255) / 256;
+    if (b > 148LL * 32) b = 148LL * 32;
+    return (unsigned)(b < 1 ? 1 : b);
+}
+static int imod(int a, int b) { int m = a % b; return m < 0 ? m + b : m; }
+
+float host_time_function(const std::string& pulse, float t, float dt, float tau) {
+    const float pi = 3.14159265f;
+    float f = 0, a, b;
+    if (pulse == "const") f = 1;
+    else if (pulse == "delta") { if (std::fabs(t) < 0.25f * dt) f = 1.0f / dt; }
+    else if (pulse == "step" || pulse == "integral_delta") {
+        if (std::fabs(t) < 0.25f * dt) f = 0.5f;
+        else if (t >= 0.25f * dt) f = 1;
+    } else if (pulse == "brune") {
+        if (0.0f < t) { a = 1.0f / tau; f = std::exp(-a * t) * a * a * t; }
+    } else if (pulse == "integral_brune") {
+        if (0.0f < t) { a = 1.0f / tau; f = 1.0f - std::exp(-a * t) * (a * t + 1.0f); }
+    } else if (pulse == "hann") {
+        b = pi * tau;
+        if (-b < t && t < b) { a = 1.0f / tau; f = 0.5f / pi * a * (1.0f + std::cos(a * t)); }
+    } else if (pulse == "integral_hann") {
+        b = pi * tau;
+        if (-b < t && t < b) { a = 1.0f / tau; f = 0.5f + 0.5f / pi * (a * t + std::sin(a * t)); }
+        else if (0.0f < t) f = 1;
+    } else if (pulse == "gaussian" || pulse == "integral_ricker1") {
+        a = 0.5f / (tau * tau); b = std::sqrt(a / pi); f = std::exp(-a * t * t) * b;
+    } else if (pulse == "ricker1" || pulse == "integral_ricker2") {
+        a = 0.5f / (tau * tau); b = std::sqrt(a / pi) * 2.0f * a; f = -std::exp(-a * t * t) * b * t;
+    } else if (pulse == "ricker2") {
+        a = 0.5f / (tau * tau); b = std::sqrt(a / pi) * 4.0f * a; f = std::exp(-a * t * t) * b * (a * t * t - 0.5f);
+    } else throw SordError(SORD_E_PARAM, "invalid time func: " + pulse);
+    return f;
+}
+
+static inline float wgt(float x, int j, bool plane) { return plane ? 1.0f : 1.0f - std::fabs(x - (float)j); }
+
+static bool applies(Solver& s, const IoOp& io, const char* field, char pass) {
+    int it1 = io.ii[3][0], it2 = io.ii[3][1], dit = io.ii[3][2];
+    if (s.it > it2) return false;
+    if (io.op[0] == '#') return false;
+    if (s.it < it1) return false;
+    if (imod(s.it - it1, dit) != 0) return false;
+    if (io.field != field) return false;
+    char op2 = io.op.size() > 1 ? io.op[1] : ' ';
+    if (pass == '<' && op2 == '>') return false;
+    if (pass == '>' && op2 != '>') return false;
+    return true;
+}
+
+bool field_active(Solver& s, const char* field, char pass) {
+    for (auto& io : s.ops)
+        if (applies(s, io, field, pass)) return true;
+    return false;
+}
+
+// Point-op geometry: i1/i2 (1-based, inclusive), xi and plane flags
+struct PointGeom {
+    int i1[3], i2[3];
+    float xi[3];
+    bool plane[3];
+};
+static void point_geom(Solver& s, const IoOp& io, const FieldView& f, PointGeom& P) {
+    const Geom& g = s.g;
+    for (int i = 0; i < 3; i++) {
+        int i3, i4;
+        if (io.reg == 'n') { i3 = g.i1node[i]; i4 = g.i2node[i]; P.xi[i] = io.x1[i] - (float)g.nnoff[i] + 1.0f; }
+        else { i3 = g.i1cell[i]; i4 = g.i2cell[i]; P.xi[i] = io.x1[i] - (float)g.nnoff[i] + 0.5f; }
+        int fl = (int)std::floor(P.xi[i]);
+        P.i1[i] = std::max(i3, fl);
+        P.i2[i] = std::min(i4, fl + 1);
+        P.plane[i] = f.n[i] == 1 && g.nm[i] != 1;
+    }
+}
+
+// Injection entries of a '.' op: f(j,k,l) = f(j,k,l) + val*r in loop order.
+// Returns false if the op is outside the block (the reference marks it '#').
+bool point_injection(Solver& s, IoOp& io, const FieldView& f, int comp, std::vector<Inject>& out) {
+    PointGeom P;
+    point_geom(s, io, f, P);
+    for (int i = 0; i < 3; i++)
+        if (P.i2[i] < P.i1[i]) { io.op = "#"; return false; }
+    for (int i = 0; i < 3; i++)
+        if (P.plane[i]) P.i1[i] = P.i2[i] = 1;
+    float val = io.val * host_time_function(io.fname, s.tm, s.g.dt, io.tau);
+    for (int l = P.i1[2]; l <= P.i2[2]; l++)
+        for (int k = P.i1[1]; k <= P.i2[1]; k++)
+            for (int j = P.i1[0]; j <= P.i2[0]; j++) {
+                float r = wgt(P.xi[0], j, P.plane[0]) * wgt(P.xi[1], k, P.plane[1]) * wgt(P.xi[2], l, P.plane[2]);
+                Inject e;
+                e.idx = (long long)(j - 1) + (long long)f.n[0] * ((long long)(k - 1) + (long long)f.n[1] * (long long)(l - 1));
+                e.comp = comp;
+                e.inc = val * r;
+                out.push_back(e);
+            }
+    return true;
+}
+
+static void file_write(Solver& s, IoOp& io, const float* data, int recl, int nrec, const std::string& filename, int m, int o) {
+    std::string fn = s.path(filename);
+    FILE* fp;
+    if (!io.open && o == 0) {
+        fp = fopen(fn.c_str(), "rb");
+        if (fp) { fclose(fp); throw SordError(SORD_E_IO, "file exists: " + filename); }
+        fp = fopen(fn.c_str(), "wb");
+    } else {
+        fp = fopen(fn.c_str(), "r+b");
+    }
+    if (!fp) throw SordError(SORD_E_IO, "cannot open " + filename);
+    io.open = true;
+    fseek(fp, (long)((size_t)recl * sizeof(float) * (size_t)o), SEEK_SET);
+    fwrite(data, sizeof(float), (size_t)recl * nrec, fp);
+    fclose(fp);
+    if (o + nrec == m) io.open = false;
+}
+
+static void region_scalar_bc(Solver& s, IoOp& io, FieldView f) {
+    const Geom& g = s.g;
+    if (io.reg == 'n') launch_scalar_bc(s, f.p, f.n, s.prm.bc1, s.prm.bc2, g.i1bc, g.i2bc);
+    if (io.reg == 'c') {
+        int t[3] = {g.i2bc[0] - 1, g.i2bc[1] - 1, g.i2bc[2] - 1};
+        launch_scalar_bc(s, f.p, f.n, s.prm.bc1, s.prm.bc2, g.i1bc, t);
+    }
+}
+
+struct ProbeTable {
+    std::vector<Probe> host;
+    Probe* dev = nullptr;
+    std::vector<int> id_of_op;  // op index -> probe id (-1 none)
+};
+static std::map<const Solver*, ProbeTable> g_probes;
+
+static int probe_id(Solver& s, size_t opi, const IoOp& io, const FieldView& f) {
+    ProbeTable& T = g_probes[&s];
+    if (T.id_of_op.size() != s.ops.size()) T.id_of_op.assign(s.ops.size(), -1);
+    if (T.id_of_op[opi] >= 0) return T.id_of_op[opi];
+    PointGeom P;
+    point_geom(s, io, f, P);
+    int i1[3], i2[3];
+    for (int i = 0; i < 3; i++) { i1[i] = P.i1[i]; i2[i] = P.i2[i]; if (f.n[i] == 1) { i1[i] = i2[i] = 1; } }
+    Probe pr;
+    pr.n = 0;
+    for (int l = i1[2]; l <= i2[2]; l++)
+        for (int k = i1[1]; k <= i2[1]; k++)
+            for (int j = i1[0]; j <= i2[0]; j++) {
+                if (pr.n >= 8) break;
+                pr.idx[pr.n] = (long long)(j - 1) + (long long)f.n[0] * ((long long)(k - 1) + (long long)f.n[1] * (long long)(l - 1));
+                pr.r[pr.n] = wgt(P.xi[0], j, P.plane[0]) * wgt(P.xi[1], k, P.plane[1]) * wgt(P.xi[2], l, P.plane[2]);
+                pr.n++;
+            }
+    T.host.push_back(pr);
+    if (T.dev) cudaFree(T.dev);
+    SORD_CUDA(cudaMalloc((void**)&T.dev, sizeof(Probe) * T.host.size()));
+    SORD_CUDA(cudaMemcpyAsync(T.dev, T.host.data(), sizeof(Probe) * T.host.size(), cudaMemcpyHostToDevice, s.stream));
+    SORD_CUDA(cudaStreamSynchronize(s.stream));
+    T.id_of_op[opi] = (int)T.host.size() - 1;
+    return T.id_of_op[opi];
+}
+
+void probes_free(const Solver* s) {
+    auto it = g_probes.find(s);
+    if (it != g_probes.end()) {
+        if (it->second.dev) cudaFree(it->second.dev);
+        g_probes.erase(it);
+    }
+}
+
+static void flush_output(Solver& s, IoOp& io, int n3[3], int m3[3]) {
+    int it1 = io.ii[3][0], it2 = io.ii[3][1], dit = io.ii[3][2];
+    int n4 = io.ib;
+    int m4 = (it2 - it1) / dit + 1;
+    int o4 = (s.it - it1) / dit + 1 - n4;
+    std::string filename = io.fname;
+    if ((n3[0] != m3[0] || n3[1] != m3[1] || n3[2] != m3[2]) && s.prm.mpout == 0) filename += "-000000";
+    if (!(n3[0] < 1 || n3[1] < 1 || n3[2] < 1 || n4 < 1)) {
+        io.hbuf.resize((size_t)io.bufn * n4);
+        SORD_CUDA(cudaMemcpyAsync(io.hbuf.data(), io.dbuf, sizeof(float) * (size_t)io.bufn * n4, cudaMemcpyDeviceToHost, s.stream));
+        SORD_CUDA(cudaStreamSynchronize(s.stream));
+        file_write(s, io, io.hbuf.data(), io.bufn, n4, filename, m4, o4);
+    }
+    io.ib = 0;
+    if (s.it == it2 || n3[0] < 1 || n3[1] < 1 || n3[2] < 1 || n4 < 1) {
+        if (io.dbuf) { cudaFree(io.dbuf); io.dbuf = nullptr; }
+        io.op = "#";
+    }
+}
+
+static void magnitude(Solver& s, const std::string& fl) {
+    const Geom& g = s.g;
+    int one[3] = {1, 1, 1};
+    if (fl == "vm2") dev_vector_norm(s, s.d.s1, s.d.v, g.i1core, g.i2core, one);
+    else if (fl == "um2") dev_vector_norm(s, s.d.s1, s.d.u, g.i1core, g.i2core, one);
+    else if (fl == "am2") dev_vector_norm(s, s.d.s1, s.d.w1n, g.i1core, g.i2core, one);
+    else if (fl == "wm2") dev_tensor_norm(s, s.d.s1, s.d.sd, s.d.so, g.i1core, g.i2core, one);
+}
+
+// host-side disk input (input_output.f90:296-437)
+static void disk_input(Solver& s, IoOp& io, FieldView f, int* i1, int* i2, int* di, int* m, int* n, int* o, const PointGeom* P) {
+    const Geom& g = s.g;
+    int it1 = io.ii[3][0], it2 = io.ii[3][1], dit = io.ii[3][2];
+    if (io.op != ".<")
+        for (int i = 0; i < 3; i++)
+            if (m[i] == 1) { i1[i] = 1; i2[i] = 1; n[i] = 1; o[i] = 0; }
+    int nsp = n[0] * n[1] * n[2];
+    if (io.ib < 0) {
+        io.bufn = std::max(nsp, 0);
+        io.hbuf.assign((size_t)io.bufn * io.nb, 0.f);
+        io.ib = io.nb;
+    }
+    if (io.ib == io.nb) {
+        int n4 = std::min(io.nb, (it2 - s.it) / dit + 1);
+        int o4 = (s.it - it1) / dit;
+        std::string filename = io.fname;
+        if ((n[0] != m[0] || n[1] != m[1] || n[2] != m[2]) && s.prm.mpin == 0) filename += "-000000";
+        io.ib = 0;
+        if (n[0] < 1 || n[1] < 1 || n[2] < 1 || n4 < 1) { io.hbuf.clear(); io.op = "#"; return; }
+        FILE* fp = fopen(s.path(filename).c_str(), "rb");
+        if (!fp) throw SordError(SORD_E_IO, "cannot open " + filename);
+        size_t recl = (size_t)nsp;
+        fseek(fp, (long)(recl * sizeof(float) * (size_t)o4), SEEK_SET);
+        size_t got = fread(io.hbuf.data(), sizeof(float), recl * n4, fp);
+        fclose(fp);
+        if (got != recl * n4) throw SordError(SORD_E_IO, "short read " + filename);
+        for (size_t q = 0; q < recl * n4; q++) {
+            float v = io.hbuf[q];
+            if (v != v || v > std::numeric_limits<float>::max()) throw SordError(SORD_E_NANINF, "NaN/Inf in " + io.fname);
+        }
+    }
+    io.ib = io.ib + 1;
+    const float* buf = io.hbuf.data() + (size_t)io.bufn * (io.ib - 1);
+    // bring the field to the host
+    size_t fsz = (size_t)f.n[0] * f.n[1] * f.n[2];
+    std::vector<float> F(fsz);
+    SORD_CUDA(cudaMemcpyAsync(F.data(), f.p, sizeof(float) * fsz, cudaMemcpyDeviceToHost, s.stream));
+    SORD_CUDA(cudaStreamSynchronize(s.stream));
+    auto at = [&](std::vector<float>& A, int j, int k, int l) -> float& {
+        return A[(size_t)(j - 1) + (size_t)f.n[0] * ((size_t)(k - 1) + (size_t)f.n[1] * (size_t)(l - 1))];
+    };
+    if (io.op == ".<") {
+        for (int l = i1[2]; l <= i2[2]; l++)
+            for (int k = i1[1]; k <= i2[1]; k++)
+                for (int j = i1[0]; j <= i2[0]; j++) {
+                    float r = wgt(P->xi[0], j, P->plane[0]) * wgt(P->xi[1], k, P->plane[1]) * wgt(P->xi[2], l, P->plane[2]);
+                    at(F, j, k, l) = at(F, j, k, l) + r * buf[0];
+                }
+    } else {
+        std::vector<float> S(fsz, 0.f);
+        if (f.n[0] == g.nm[0] && f.n[1] == g.nm[1] && f.n[2] == g.nm[2]) {
+            // the reference stages through the volume scratch s1: keep its contents
+            SORD_CUDA(cudaMemcpyAsync(S.data(), s.d.s1, sizeof(float) * fsz, cudaMemcpyDeviceToHost, s.stream));
+            SORD_CUDA(cudaStreamSynchronize(s.stream));
+        }
+        size_t q = 0;
+        for (int l = i1[2]; l <= i2[2]; l += di[2])
+            for (int k = i1[1]; k <= i2[1]; k += di[1])
+                for (int j = i1[0]; j <= i2[0]; j += di[0]) at(S, j, k, l) = buf[q++];
+        if (di[0] > 1 || di[1] > 1 || di[2] > 1) {
+            // utilities.f90:168-220
+            int a1[3], a2[3];
+            for (int i = 0; i < 3; i++) {
+                a1[i] = io.ii[i][0] - g.nnoff[i]; a2[i] = io.ii[i][1] - g.nnoff[i];
+                if (a1[i] < 1) a1[i] = a1[i] + (-a1[i] / di[i] + 1) * di[i];
+                if (a2[i] > f.n[i]) a2[i] = a1[i] + (f.n[i] - a1[i]) / di[i] * di[i];
+            }
+            int d = di[0];
+            for (int i = 1; i <= d - 1; i++) {
+                float h1 = 1.0f / (float)d * (float)i, h2 = 1.0f / (float)d * (float)(d - i);
+                for (int l = a1[2]; l <= a2[2]; l += di[2])
+                    for (int k = a1[1]; k <= a2[1]; k += di[1])
+                        for (int j = a1[0]; j <= a2[0] - d; j += d) at(S, j + i, k, l) = h1 * at(S, j, k, l) + h2 * at(S, j + d, k, l);
+            }
+            d = di[1];
+            for (int i = 1; i <= d - 1; i++) {
+                float h1 = 1.0f / (float)d * (float)i, h2 = 1.0f / (float)d * (float)(d - i);
+                for (int l = a1[2]; l <= a2[2]; l += di[0])
+                    for (int k = a1[1]; k <= a2[1] - d; k += d)
+                        for (int j = a1[0]; j <= a2[0]; j++) at(S, j, k + i, l) = h1 * at(S, j, k, l) + h2 * at(S, j, k + d, l);
+            }
+            d = di[2];
+            for (int i = 1; i <= d - 1; i++) {
+                float h1 = 1.0f / (float)d * (float)i, h2 = 1.0f / (float)d * (float)(d - i);
+                for (int l = a1[2]; l <= a2[2] - d; l += d)
+                    for (int k = a1[1]; k <= a2[1]; k++)
+                        for (int j = a1[0]; j <= a2[0]; j++) at(S, j, k, l + i) = h1 * at(S, j, k, l) + h2 * at(S, j, k, l + d);
+            }
+        }
+        if (m[0] == 1) { i2[0] = f.n[0]; for (int l = 1; l <= f.n[2]; l++) for (int k = 1; k <= f.n[1]; k++) for (int j = 2; j <= i2[0]; j++) at(S, j, k, l) = at(S, 1, k, l); }
+        if (m[1] == 1) { i2[1] = f.n[1]; for (int l = 1; l <= f.n[2]; l++) for (int k = 2; k <= i2[1]; k++) for (int j = 1; j <= f.n[0]; j++) at(S, j, k, l) = at(S, j, 1, l); }
+        if (m[2] == 1) { i2[2] = f.n[2]; for (int l = 2; l <= i2[2]; l++) for (int k = 1; k <= f.n[1]; k++) for (int j = 1; j <= f.n[0]; j++) at(S, j, k, l) = at(S, j, k, 1); }
+        for (int l = i1[2]; l <= i2[2]; l++)
+            for (int k = i1[1]; k <= i2[1]; k++)
+                for (int j = i1[0]; j <= i2[0]; j++) {
+                    if (io.op == "=<") at(F, j, k, l) = at(S, j, k, l);
+                    else if (io.op == "+<") at(F, j, k, l) = at(F, j, k, l) + at(S, j, k, l);
+                    else if (io.op == "*<") at(F, j, k, l) = at(F, j, k, l) * at(S, j, k, l);
+                    else throw SordError(SORD_E_PARAM, "bad i/o op");
+                }
+        if (f.n[0] == g.nm[0] && f.n[1] == g.nm[1] && f.n[2] == g.nm[2]) {
+            SORD_CUDA(cudaMemcpyAsync(s.d.s1, S.data(), sizeof(float) * fsz, cudaMemcpyHostToDevice, s.stream));
+        }
+    }
+    SORD_CUDA(cudaMemcpyAsync(f.p, F.data(), sizeof(float) * fsz, cudaMemcpyHostToDevice, s.stream));
+    SORD_CUDA(cudaStreamSynchronize(s.stream));
+    region_scalar_bc(s, io, f);
+    if (s.it == it2) { io.hbuf.clear(); io.op = "#"; }
+}
+
+static void field_io_op(Solver& s, size_t opi, FieldView f, ProbeBatch& batch) {
+    IoOp& io = s.ops[opi];
+    const Geom& g = s.g;
+    int i1[3], i2[3], i3[3], i4[3], di[3], m[4], n[4], o[4];
+    char op2 = io.op.size() > 1 ? io.op[1] : ' ';
+    PointGeom P;
+    point_geom(s, io, f, P);
+    if (io.op[0] == '.') {
+        for (int i = 0; i < 3; i++) { i1[i] = P.i1[i]; i2[i] = P.i2[i]; di[i] = 1; }
+    } else {
+        for (int i = 0; i < 3; i++) {
+            if (io.reg == 'n') { i3[i] = g.i1node[i]; i4[i] = g.i2node[i]; }
+            else { i3[i] = g.i1cell[i]; i4[i] = g.i2cell[i]; }
+            i1[i] = io.ii[i][0] - g.nnoff[i]; i2[i] = io.ii[i][1] - g.nnoff[i]; di[i] = io.ii[i][2];
+            if (i1[i] < i3[i]) i1[i] = i1[i] + ((i3[i] - i1[i] - 1) / di[i] + 1) * di[i];
+            if (i2[i] > i4[i]) i2[i] = i1[i] + (i4[i] - i1[i]) / di[i] * di[i];
+        }
+    }
+    // non-disk input
+    if (op2 != '<' && op2 != '>') {
+        for (int i = 0; i < 3; i++)
+            if (i2[i] < i1[i]) { io.op = "#"; return; }
+        int pax = -1;
+        for (int i = 0; i < 3; i++)
+            if (P.plane[i]) { i1[i] = i2[i] = 1; di[i] = 1; pax = i; }
+        if (io.op == ".") {
+            std::vector<Inject> e;
+            point_injection(s, io, f, 0, e);
+            if (!e.empty()) {
+                if ((int)e.size() > kMaxInject) throw SordError(SORD_E_PARAM, "too many point injections");
+                Inject* h = s.hinj + 3 * kMaxInject;
+                std::memcpy(h, e.data(), sizeof(Inject) * e.size());
+                Inject* dptr = s.d.inj + 3 * kMaxInject;
+                SORD_CUDA(cudaMemcpyAsync(dptr, h, sizeof(Inject) * e.size(), cudaMemcpyHostToDevice, s.stream));
+                float* F6[6] = {f.p, f.p, f.p, f.p, f.p, f.p};
+                InjectList l{dptr, (int)e.size()};
+                launch_inject(s, F6, l);
+                SORD_CUDA(cudaStreamSynchronize(s.stream));
+            }
+        } else {
+            float val = io.val * host_time_function(io.fname, s.tm, g.dt, io.tau);
+            Region R;
+            for (int i = 0; i < 3; i++) { R.n[i] = f.n[i]; R.i1[i] = i1[i]; R.i2[i] = i2[i]; R.di[i] = di[i]; }
+            R.vsy = g.sy; R.vsz = g.sz;
+            long long cnt = 1;
+            for (int i = 0; i < 3; i++) cnt *= (i2[i] - i1[i]) / di[i] + 1;
+            const std::string& op = io.op;
+            if (op == "=" || op == "+" || op == "*" || op == "=~" || op == "+~" || op == "*~") {
+                int code = op == "=" ? 0 : op == "+" ? 1 : op == "*" ? 2 : op == "=~" ? 3 : op == "+~" ? 4 : 5;
+                unsigned long long call = code >= 3 ? s.rng_calls++ : 0;
+                k_region_op<<<gf(cnt), 256, 0, s.stream>>>(f.p, R, code, val, call);
+                FCHK(s);
+            } else if (op == "=@" || op == "+@" || op == "*@") {
+                int code = op[0] == '=' ? 0 : op[0] == '+' ? 1 : 2;
+                int pidx = pax >= 0 ? g.irup : 0;
+                k_cube<<<gf(cnt), 256, 0, s.stream>>>(f.p, R, s.d.x[0], s.d.x[1], s.d.x[2], g, io.reg == 'c' ? 1 : 0, pax, pidx,
+                                                     code, val, io.x1[0], io.x1[1], io.x1[2], io.x2[0], io.x2[1], io.x2[2]);
+                FCHK(s);
+            } else {
+                throw SordError(SORD_E_PARAM, "bad i/o mode '" + op + "'");
+            }
+        }
+        region_scalar_bc(s, io, f);
+        return;
+    }
+    // spatial indices for disk i/o
+    if (io.op[0] == '.') {
+        for (int i = 0; i < 4; i++) { m[i] = 1; n[i] = 1; o[i] = 0; }
+    } else {
+        for (int i = 0; i < 3; i++) {
+            i1[i] = io.ii[i][0] - g.nnoff[i]; i2[i] = io.ii[i][1] - g.nnoff[i]; di[i] = io.ii[i][2];
+            i3[i] = i1[i]; i4[i] = i2[i];
+            if (i1[i] < g.i1core[i]) i1[i] = i1[i] + ((g.i1core[i] - i1[i] - 1) / di[i] + 1) * di[i];
+            if (i2[i] > g.i2core[i]) i2[i] = i1[i] + (g.i2core[i] - i1[i]) / di[i] * di[i];
+            m[i] = (i4[i] - i3[i]) / di[i] + 1;
+            n[i] = (i2[i] - i1[i]) / di[i] + 1;
+            o[i] = (i1[i] - i3[i]) / di[i];
+            n[i] = std::max(n[i], 0);
+        }
+        m[3] = n[3] = 1; o[3] = 0;
+    }
+    for (int i = 0; i < 3; i++)
+        if (f.n[i] == 1) {
+            if (n[i] < 1) { io.op = "#"; return; }
+            i1[i] = 1; i2[i] = 1; m[i] = 1; n[i] = 1; o[i] = 0;
+        }
+    if (op2 == '<') {
+        disk_input(s, io, f, i1, i2, di, m, n, o, &P);
+        return;
+    }
+    if (op2 == '>') {
+        if (io.op == ".>")
+            for (int i = 0; i < 3; i++)
+                if (!P.plane[i] && (i2[i] < g.i1core[i] || i2[i] > g.i2core[i])) { io.op = "#"; return; }
+        int nsp = n[0] * n[1] * n[2];
+        if (io.ib < 0) {
+            io.bufn = std::max(nsp, 0);
+            size_t bytes = sizeof(float) * (size_t)std::max(io.bufn * io.nb, 1);
+            cudaError_t e = cudaMalloc((void**)&io.dbuf, bytes);
+            if (e != cudaSuccess) throw SordError(SORD_E_NOMEM, "output buffer: " + std::string(cudaGetErrorString(e)));
+            io.ib = 0;
+            io.open = false;
+        }
+        std::string fl = io.field;
+        if (fl == "vm2" || fl == "um2" || fl == "wm2" || fl == "am2") magnitude(s, fl);
+        io.ib = io.ib + 1;
+        float* dst = io.dbuf + (size_t)io.bufn * (io.ib - 1);
+        if (io.op == ".>") {
+            int id = probe_id(s, opi, io, f);
+            if (batch.count == 128) {
+                // flush a full batch before adding more
+                k_probe<<<1, 128, 0, s.stream>>>(f.p, batch);
+                FCHK(s);
+                batch.count = 0;
+            }
+            batch.probes = g_probes[&s].dev;
+            batch.id[batch.count] = id;
+            batch.dst[batch.count] = dst;
+            batch.count++;
+        } else if (io.op == "=>") {
+            Region R;
+            for (int i = 0; i < 3; i++) { R.n[i] = f.n[i]; R.i1[i] = i1[i]; R.i2[i] = i2[i]; R.di[i] = di[i]; }
+            R.vsy = g.sy; R.vsz = g.sz;
+            if (nsp > 0) {
+                k_gather<<<gf(nsp), 256, 0, s.stream>>>(f.p, R, dst);
+                FCHK(s);
+            }
+        } else throw SordError(SORD_E_PARAM, "bad i/o op");
+        if (io.ib == io.nb || s.it == io.ii[3][1] || imod(s.it, s.prm.itio) == 0) {
+            if (batch.count) {
+                k_probe<<<1, 128, 0, s.stream>>>(f.p, batch);
+                FCHK(s);
+                batch.count = 0;
+            }
+            int n3[3] = {n[0], n[1], n[2]}, m3[3] = {m[0], m[1], m[2]};
+            flush_output(s, io, n3, m3);
+        }
+        return;
+    }
+    throw SordError(SORD_E_PARAM, "bad i/o op");
+}
+
+void field_io(Solver& s, const char* passes, const char* field, FieldView f) {
+    for (const char* pp = passes; *pp; pp++) {
+        char pass = *pp;
+        ProbeBatch batch;
+        batch.count = 0;
+        batch.probes = nullptr;
+        for (size_t i = 0; i < s.ops.size(); i++) {
+            if (!applies(s, s.ops[i], field, pass)) continue;
+            field_io_op(s, i, f, batch);
+        }
+        if (batch.count) {
+            k_probe<<<1, 128, 0, s.stream>>>(f.p, batch);
+            FCHK(s);
+        }
+    }
+}
+
+void field_io_flush_all(Solver& s) { (void)s; }
+
+}  // namespace sordgpu

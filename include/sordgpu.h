@@ -1,0 +1,94 @@
+/*
+ * sordgpu.h - C ABI of the B200-native SORD time-stepper (libsordgpu.so).
+ *
+ * The reference has no library interface: cst/sord.py:stage() writes the
+ * text deck `sord.in` (cst/sord.py:538-544) and cst/job.py:launch()
+ * (cst/job.py:176-195) runs the Fortran executable `sord.x` as a separate
+ * process, which reads `sord.in` (sord/input_output.f90:21-98), runs the
+ * setup and step loop (sord/sord.f90:24-47) and writes `.bin`, `stats-*.bin`,
+ * `prof-*.bin` and `material.json` into the working directory.
+ *
+ * This ABI replaces that process boundary with in-process calls that take
+ * the same `sord.in` text and write the same files.  All arguments are plain
+ * C types; the library owns all device memory.  Every call returns SORD_OK
+ * (0) or a negative SORD_E_* code; sord_last_error() gives the message (the
+ * text the Fortran `stop` would have printed).  A handle is used by one host
+ * thread at a time; each handle runs on its own CUDA stream.
+ */
+#ifndef SORDGPU_H
+#define SORDGPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct sord_handle sord_handle;
+
+enum {
+    SORD_OK = 0,
+    SORD_E_PARAM = -1,   /* bad sord.in / bad i/o op        (input_output.f90:253,423,514) */
+    SORD_E_CFL = -2,     /* Courant condition / negative moduli (material_model.f90:167-168) */
+    SORD_E_NEGVOL = -3,  /* negative cell volume            (grid_generation.f90:195-198) */
+    SORD_E_NANINF = -4,  /* NaN/Inf in stats or input file  (statistics.f90:53-59, input_output.f90:333-337) */
+    SORD_E_IO = -5,      /* file open/read/write failure */
+    SORD_E_CUDA = -6,    /* CUDA runtime error or no device */
+    SORD_E_STATE = -7,   /* call out of order (e.g. step past nt) */
+    SORD_E_NOMEM = -8    /* device allocation failed */
+};
+
+/* Parse `sord_in_text` (the sord.in wire format) and run the whole setup
+ * (sord/sord.f90:27-36: dimensions, grid, material, PML, finite source,
+ * rupture, resample) on CUDA device `device`.  Input files named by the I/O
+ * ops and all outputs are resolved relative to `workdir`.
+ * Replaces: the start of `sord.x` (sord/sord.f90:24-37). */
+int sord_create(const char* workdir, const char* sord_in_text, int device, sord_handle** out);
+
+/* Advance `nsteps` time steps (sord/sord.f90:39-47: step_time, step_stress,
+ * step_accel, stats), including every field-I/O hook of those steps. */
+int sord_step(sord_handle* h, int nsteps);
+
+/* Run all remaining steps and flush every output.  Replaces the remainder of
+ * `sord.x` after setup (sord/sord.f90:39-50). */
+int sord_run(sord_handle* h);
+
+/* Convenience: sord_create on `workdir`/sord.in, sord_run, sord_destroy.
+ * This is the whole of `sord.x` (cst/job.py:193-194 `subprocess.check_call`). */
+int sord_run_directory(const char* workdir, int device);
+
+/* Copy a node or cell volume field to host memory (core region only, j
+ * fastest; nn or nn-1 values per axis).  Names: vx vy vz ux uy uz ax ay az
+ * (nodes; `a` holds the last acceleration) and lam mu yy vc (cells).
+ * `n` is the capacity of `host` in floats. */
+int sord_get_field(sord_handle* h, const char* name, float* host, size_t n);
+
+/* Query dimensions and progress: nn[3] global nodes, it (steps done), nt. */
+int sord_info(const sord_handle* h, int* nn3, int* it, int* nt);
+
+/* Latest statistics (statistics.f90:13-131): out[0..15] = amax vmax umax wmax
+ * samax svmax sumax slmax tsmax tnmin tnmax tarrmax efric estrain moment mw
+ * of the last stats step (maxima as magnitudes).  Returns the count written. */
+int sord_stats(const sord_handle* h, double* out, int n);
+
+/* Device time of the last sord_step call in milliseconds (CUDA events on the
+ * handle's stream, step kernels and I/O hooks included). */
+double sord_last_step_ms(const sord_handle* h);
+
+/* Number of kernels this library launched since the handle was created. */
+long long sord_kernel_launches(const sord_handle* h);
+
+/* Message for the last error on `h` (or the last create failure if h is NULL). */
+const char* sord_last_error(const sord_handle* h);
+
+/* Static name of an error code. */
+const char* sord_error_string(int code);
+
+/* Free all device memory of the handle and flush pending output. */
+void sord_destroy(sord_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SORDGPU_H */

@@ -1,0 +1,180 @@
+"""Small SORD configurations used by the parity tests, and a runner that
+stages one configuration twice (oracle / CUDA solver) and compares every
+output file.  Sizes are chosen so the oracle finishes in seconds."""
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+from coseis_b200 import sord  # noqa: E402
+
+
+def all_outputs(prm, fields='nc', step=None):
+    """Add a '=>' output of every node/cell field (cst/tests/sord_mpi.py:27-29)."""
+    for k, v in sord.fieldnames.items():
+        if v[0][0] in fields and k[0] != '_':
+            t = [] if step is None else [[], [], [], [None, None, step]]
+            if '~' not in v[0] and step is not None:
+                t = []
+            prm[k] = list(prm.get(k, [])) + [(t, '=>', k + '.bin')]
+    return prm
+
+
+def case_mpi():
+    """cst/tests/sord_mpi.py:14-31: 5x4x2 nodes, 2 steps, potency '=' at node 0."""
+    prm = {
+        'itstats': 1, 'shape': [5, 4, 2, 2], 'delta': [100.0, 100.0, 100.0, 0.0075],
+        'rho': [2670.0], 'vp': [6000.0], 'vs': [3464.0], 'gam': [0.3],
+        'hourglass': [1.0, 1.0], 'bc1': ['free'] * 3, 'bc2': ['free'] * 3,
+    }
+    all_outputs(prm)
+    for f in 'pxx', 'pyy', 'pzz':
+        prm[f] = prm[f] + [([0, 0, 0, 0], '=', 1e10)]
+    return prm
+
+
+def case_pml(n=22, nt=11):
+    """cst/tests/sord_pml.py:14-31: PML on all faces, potency '=' at (10,10,10)."""
+    prm = {
+        'itstats': 1, 'shape': [n, n, n, nt], 'delta': [100.0, 100.0, 100.0, 0.0075],
+        'rho': [2670.0], 'vp': [6000.0], 'vs': [3464.0], 'gam': [0.3],
+        'hourglass': [1.0, 1.0], 'bc1': ['pml'] * 3, 'bc2': ['pml'] * 3, 'npml': 5,
+    }
+    all_outputs(prm)
+    for f in 'pxx', 'pyy', 'pzz':
+        prm[f] = prm[f] + [([10, 10, 10, 0], '=', 1e10)]
+    return prm
+
+
+def case_explosion(n=25, nt=40, npml=6):
+    """Scaled-down explosion: isotropic moment '.' source (Brune), PML, receivers."""
+    c = (n - 1) // 2
+    prm = {
+        'shape': [n, n, n, nt], 'delta': [100.0, 100.0, 100.0, 0.008],
+        'rho': [2670.0], 'vp': [6000.0], 'vs': [3464.0], 'gam': [0.0],
+        'hourglass': [1.0, 1.0], 'bc1': ['pml'] * 3, 'bc2': ['pml'] * 3, 'npml': npml,
+        'itstats': 5, 'itio': 20,
+    }
+    for f in 'mxx', 'myy', 'mzz':
+        prm[f] = [([c + 0.5, c + 0.5, c + 0.5, []], '.', 1e16, 'brune', 0.1)]
+    for f in 'vx', 'vy', 'vz':
+        prm[f] = [([[], [], c, [None, None, 5]], '=>', 'snap-%s.bin' % f)]
+        for r, (x, y, z) in enumerate([(c - 5, c, c), (c, c + 4, c - 3), (c + 0.3, c - 2.6, c + 1.2)]):
+            prm[f] += [([x, y, z, []], '.>', 'rec%d-%s.bin' % (r, f))]
+    prm['am2'] = [([c, c, c, []], '=>', 'am2.bin')]
+    prm['wm2'] = [([c, [], c, [None, None, 3]], '=>', 'wm2.bin')]
+    return prm
+
+
+def case_curvilinear(n=16, nt=12):
+    """Random mesh (gridnoise) with PML and viscosity: general bracket path."""
+    prm = case_pml(n, nt)
+    prm['gridnoise'] = 0.1
+    prm['npml'] = 3
+    return prm
+
+
+def case_bc():
+    """Every boundary type on some face, hourglass viscosity, mixed PML."""
+    prm = {
+        'itstats': 2, 'shape': [14, 12, 10, 10], 'delta': [100.0, 100.0, 100.0, 0.0075],
+        'rho': [2670.0], 'vp': [6000.0], 'vs': [3464.0], 'gam': [0.2],
+        'hourglass': [1.0, 2.0], 'bc1': ['-node', '+cell', 'rigid'], 'bc2': ['pml', '-cell', '+node'],
+        'npml': 3,
+    }
+    all_outputs(prm, step=2)
+    prm['mxy'] = [([6.5, 5.5, 4.5, []], '.', 1e14, 'ricker1', 0.02)]
+    return prm
+
+
+def case_rupture(nx=21, ny=21, nz=10, nt=30):
+    """Small Kostrov-like forced rupture (cst/tests/sord_kostrov.py:16-52)."""
+    prm = {
+        'delta': [100.0, 100.0, 100.0, 0.0075], 'shape': [nx, ny, nz, nt],
+        'rho': [2670.0], 'vp': [6000.0], 'vs': [3464.0], 'gam': 1.0,
+        'hourglass': [1.0, 1.0], 'bc1': ['pml'] * 3, 'bc2': ['-node', '+node', '-cell'],
+        'npml': 4, 'faultnormal': '+z', 'hypocenter': [-1.0, -1.0, -1.5],
+        'vrup': 0.9 * 3464.0, 'rcrit': 1e9, 'trelax': 0.0,
+        'mud': 1.0, 'mus': 1e9, 'dc': 1e9, 'tn': -90e6, 'ts': -90e6 - 10e6,
+        'itstats': 3, 'itio': 10,
+    }
+    for f in ('svm', 'sux', 'suy', 'sum', 'sl', 'psv', 'trup', 'tarr', 'tsm', 'tnm', 'fr',
+              'tx', 'ty', 'tz', 'sax', 'sam', 'nsz'):
+        prm[f] = [([], '=>', f + '.bin')]
+    prm['vx'] = [([[], [], -1, []], '=>', 'vx.bin')]
+    prm['svx'] = [([5.5, -1, []], '.>', 'p-svx.bin')]
+    return prm
+
+
+def case_slipweak(nt=40):
+    """Spontaneous slip-weakening rupture with a nucleation patch (TPV3-like)."""
+    prm = {
+        'delta': [100.0, 100.0, 100.0, 0.008], 'shape': [30, 18, 24, 40],
+        'rho': [2670.0], 'vp': [6000.0], 'vs': [3464.0], 'gam': [0.1],
+        'hourglass': [1.0, 2.0], 'bc1': ['pml'] * 3, 'bc2': ['pml'] * 3, 'npml': 4,
+        'faultnormal': '+y', 'hypocenter': [14.0, 8.5, 11.0], 'faultopening': 1,
+        'mus': [1e4, ([[5, 25], [5, 18]], '=', 0.65)], 'mud': [0.5], 'dc': [0.3],
+        'tn': [-100e6], 'ts': [58e6, ([[12, 17], [9, 14]], '=', 1.02 * 0.65 * 100e6)],
+        'itstats': 4, 'itio': 20, 'vrup': -1.0,
+    }
+    for f in ('svm', 'sux', 'suz', 'sl', 'psv', 'trup', 'tsx', 'tsz', 'tnm', 'fr', 'sam'):
+        prm[f] = [([], '=>', f + '.bin')]
+    prm['vy'] = [([[], 9, [], [None, None, 4]], '=>', 'vy.bin')]
+    return prm
+
+
+CASES = {
+    'mpi': case_mpi,
+    'pml': case_pml,
+    'explosion': case_explosion,
+    'curvilinear': case_curvilinear,
+    'bc': case_bc,
+    'rupture': case_rupture,
+    'slipweak': case_slipweak,
+}
+
+
+def stage(prm, path, realsize=4):
+    os.makedirs(path, exist_ok=True)
+    cwd = os.getcwd()
+    os.chdir(path)
+    try:
+        sord.stage(prm, realsize=realsize)
+    finally:
+        os.chdir(cwd)
+
+
+def run_oracle(path, exe, threads=4):
+    r = subprocess.run([exe, '--threads', str(threads)], cwd=path, capture_output=True, text=True)
+    if r.returncode:
+        raise RuntimeError('oracle failed: ' + r.stderr)
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def run_gpu(path):
+    from coseis_b200 import _lib
+    _lib.run_directory(path)
+
+
+def outputs(path):
+    skip = ('prof-',)
+    return sorted(f for f in os.listdir(path) if f.endswith('.bin') and not f.startswith(skip))
+
+
+def compare(path_a, path_b, dtype_a='<f4', dtype_b='<f4'):
+    """Per-file max |a-b| / max |a| and exact-equality flag."""
+    res = {}
+    fa, fb = outputs(path_a), outputs(path_b)
+    assert fa == fb, (set(fa) ^ set(fb))
+    for f in fa:
+        a = np.fromfile(os.path.join(path_a, f), dtype_a).astype(np.float64)
+        b = np.fromfile(os.path.join(path_b, f), dtype_b).astype(np.float64)
+        assert a.shape == b.shape, (f, a.shape, b.shape)
+        scale = np.abs(a).max() if a.size else 0.0
+        d = np.abs(a - b).max() if a.size else 0.0
+        res[f] = (d / scale if scale > 0 else d, bool(np.array_equal(a, b)))
+    return res
