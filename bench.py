@@ -1,0 +1,461 @@
+"""Benchmark of the SORD time loop on the large wave-propagation workload.
+
+Workload "wave226" (N = 768 x 768 x 384 = 226,492,416 nodes, dx = 50 m,
+dt = 0.004 s): layered half-space (vs 1000 / 2500 / 3500 m/s above 1 km,
+1-4 km, below 4 km; vp = sqrt(3) vs; rho 2200 / 2500 / 2700) with a seeded
+von Karman perturbation (5 % std, correlation length 1 km, Hurst 0.3) on
+vp, vs and rho; terrain-following mesh from a seeded Gaussian hill (peak
+500 m, sigma 5 km) stretched linearly to a flat bottom; free surface at the
+l = 1 face, 12-node PML on the other five; seeded random moment-tensor
+point source at 5 km depth (Brune, 0.1 s); 64 seeded surface receivers
+(vx, vy, vz).  All inputs go through the cst.sord-compatible front end as
+'=<' files and '.' / '.>' ops, exactly like a user run.
+
+A step is one time step of the whole mesh.  `value` is node-updates/s with
+every input resident in HBM; `e2e` is the same metric for the user call
+(staged files on the host -> setup -> K steps -> outputs written); the
+reference arm (--impl reference) runs the CPU oracle, the restatement of the
+Fortran solver, on a bounded sample of the same workload.
+"""
+import argparse
+import json
+import math
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SHAPE = (768, 768, 384)
+DX, DT = 50.0, 0.004
+NPML = 12
+SEED = 20261203
+HBM_FALLBACK = 6650.0
+
+
+# ------------------------------------------------------------------ workload
+def von_karman(shape, dx, a, hurst, std, seed, use_torch=True):
+    """Seeded von Karman random field on a cell grid (numpy order (l,k,j))."""
+    n = shape
+    if use_torch:
+        try:
+            import torch
+            if torch.cuda.is_available():
+                dev = torch.device('cuda')
+                g = torch.Generator(device=dev).manual_seed(seed)
+                w = torch.randn(n, generator=g, device=dev, dtype=torch.float32)
+                F = torch.fft.rfftn(w)
+                del w
+                k0 = torch.fft.fftfreq(n[0], d=dx, device=dev) * 2 * math.pi
+                k1 = torch.fft.fftfreq(n[1], d=dx, device=dev) * 2 * math.pi
+                k2 = torch.fft.rfftfreq(n[2], d=dx, device=dev) * 2 * math.pi
+                k2sq = (k0[:, None, None] ** 2 + k1[None, :, None] ** 2 + k2[None, None, :] ** 2)
+                F *= (1.0 + k2sq * a * a) ** (-(hurst + 1.5) / 2.0)
+                del k2sq
+                f = torch.fft.irfftn(F, s=n)
+                del F
+                f = f - f.mean()
+                f = f * (std / f.std())
+                out = f.cpu().numpy().astype(np.float32)
+                del f
+                torch.cuda.empty_cache()
+                return out
+        except Exception:
+            pass
+    rng = np.random.default_rng(seed)
+    w = rng.standard_normal(n).astype(np.float32)
+    F = np.fft.rfftn(w)
+    k0 = np.fft.fftfreq(n[0], d=dx) * 2 * np.pi
+    k1 = np.fft.fftfreq(n[1], d=dx) * 2 * np.pi
+    k2 = np.fft.rfftfreq(n[2], d=dx) * 2 * np.pi
+    k2sq = k0[:, None, None] ** 2 + k1[None, :, None] ** 2 + k2[None, None, :] ** 2
+    F *= (1.0 + k2sq * a * a) ** (-(hurst + 1.5) / 2.0)
+    f = np.fft.irfftn(F, s=n, axes=(0, 1, 2))
+    f -= f.mean()
+    f *= std / f.std()
+    return f.astype(np.float32)
+
+
+def make_inputs(shape, outdir, seed=SEED, use_torch=True):
+    """Write rho.bin, vp.bin, vs.bin (cells) and z.bin (nodes), j fastest."""
+    os.makedirs(outdir, exist_ok=True)
+    mark = os.path.join(outdir, 'ok.json')
+    if os.path.exists(mark):
+        return
+    nx, ny, nz = shape
+    # terrain-following z: surface elevation h(x, y), flat bottom
+    x = DX * np.arange(nx, dtype=np.float32)
+    y = DX * np.arange(ny, dtype=np.float32)
+    xc, yc = x[-1] * 0.5, y[-1] * 0.5
+    sig = 5000.0 * min(1.0, min(nx, ny) / 768.0)
+    h = 500.0 * np.exp(-((x[None, :] - xc) ** 2 + (y[:, None] - yc) ** 2) / (2 * sig * sig))
+    h = h.astype(np.float32)
+    with open(os.path.join(outdir, 'z.bin'), 'wb') as fh:
+        for l in range(nz):
+            frac = np.float32(1.0 - l / (nz - 1.0))
+            zl = np.float32(DX * l) - h * frac
+            fh.write(zl.astype(np.float32).tobytes())
+    # layered model + perturbation on cells
+    cshape = (nz - 1, ny - 1, nx - 1)
+    dv = von_karman(cshape, DX, 1000.0, 0.3, 0.05, seed, use_torch=use_torch)
+    depth = DX * (np.arange(nz - 1, dtype=np.float32) + 0.5)
+    vs_l = np.where(depth < 1000.0, 1000.0, np.where(depth < 4000.0, 2500.0, 3500.0)).astype(np.float32)
+    rho_l = np.where(depth < 1000.0, 2200.0, np.where(depth < 4000.0, 2500.0, 2700.0)).astype(np.float32)
+    for name, base in (('vs', vs_l), ('vp', vs_l * np.float32(math.sqrt(3.0))), ('rho', rho_l)):
+        with open(os.path.join(outdir, name + '.bin'), 'wb') as fh:
+            for l in range(nz - 1):
+                fh.write((base[l] * (1.0 + dv[l])).astype(np.float32).tobytes())
+    del dv
+    json.dump({'shape': list(shape), 'seed': seed}, open(mark, 'w'))
+
+
+def wave_prm(shape, nt, seed=SEED, nrec=64):
+    """cst.sord parameter dict of the wave226 workload (any shape)."""
+    nx, ny, nz = shape
+    rng = np.random.default_rng(seed + 1)
+    m = rng.standard_normal(6)
+    m *= 1e16 / math.sqrt((m[:3] ** 2).sum() + 2 * (m[3:] ** 2).sum())
+    zsrc = min(5000.0 / DX, nz - NPML - 3)
+    src = [nx * 0.5 + 0.37, ny * 0.5 - 0.21, zsrc + 0.13]
+    prm = {
+        'shape': [nx, ny, nz, nt], 'delta': [DX, DX, DX, DT],
+        'bc1': ['pml', 'pml', 'free'], 'bc2': ['pml', 'pml', 'pml'], 'npml': NPML,
+        'hourglass': [1.0, 1.0], 'gam': [0.0],
+        'rho': [([], '=<', 'rho.bin')], 'vp': [([], '=<', 'vp.bin')], 'vs': [([], '=<', 'vs.bin')],
+        'z': [([], '=<', 'z.bin')],
+        'vp_max': 6800.0, 'vs_max': 6800.0 / math.sqrt(3.0), 'vs_min': 600.0, 'vp_min': 1000.0,
+        'itstats': 10, 'itio': 50,
+    }
+    for f, v in zip(('mxx', 'myy', 'mzz', 'myz', 'mzx', 'mxy'), m):
+        prm[f] = [([src[0], src[1], src[2], []], '.', float(v), 'brune', 0.1)]
+    lo = NPML + 1
+    for r in range(nrec):
+        xr = float(rng.uniform(lo, nx - 1 - lo))
+        yr = float(rng.uniform(lo, ny - 1 - lo))
+        for f in ('vx', 'vy', 'vz'):
+            prm.setdefault(f, []).append(([xr, yr, 0.0, []], '.>', 'r%02d-%s.bin' % (r, f)))
+    return prm
+
+
+def stage_in(prm, workdir, inputs):
+    from coseis_b200 import sord
+    os.makedirs(workdir, exist_ok=True)
+    for f in ('rho.bin', 'vp.bin', 'vs.bin', 'z.bin'):
+        dst = os.path.join(workdir, f)
+        if not os.path.exists(dst):
+            os.symlink(os.path.join(inputs, f), dst)
+    cwd = os.getcwd()
+    os.chdir(workdir)
+    try:
+        sord.stage(prm)
+    finally:
+        os.chdir(cwd)
+    return open(os.path.join(workdir, 'sord.in')).read()
+
+
+def pml_memberships(shape):
+    """Node and cell PML slab memberships (one per node/cell per PML face)."""
+    nn = np.array(shape)
+    faces = [(0, 1), (0, 2), (1, 1), (1, 2), (2, 2)]  # (axis, side): l=1 face is free
+    nodes = cells = 0
+    for ax, _ in faces:
+        other = int(np.prod(nn)) // nn[ax]
+        otherc = int(np.prod(nn - 1)) // (nn[ax] - 1)
+        nodes += NPML * other
+        cells += NPML * otherc
+    return nodes, cells
+
+
+def algorithmic_bytes_per_node(shape):
+    """Compulsory FP32 traffic per node-update with perfect on-chip reuse:
+    v, u read + write (48 B), node statics mr, gam (8 B), cell statics lam,
+    mu, yy, 1/V (16 B), node coordinates x, y, z (12 B) = 84 B, plus 24 B
+    (3-component r/w) per node PML-slab membership (p memory) and per cell
+    membership (g memory)."""
+    n = float(np.prod(shape))
+    pn, pc = pml_memberships(shape)
+    return 84.0 + 24.0 * (pn + pc) / n
+
+
+# ------------------------------------------------------------------ helpers
+class Clocks(object):
+    """nvidia-smi sampling during the timed region."""
+    Q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+         'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+         'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(['nvidia-smi', '-i', str(self.index), '--query-gpu=' + self.Q,
+                                       '--format=csv,noheader,nounits', '-lms', '200'],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.p = None
+
+    def _read(self):
+        for line in self.p.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.p:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for line in self.lines:
+            f = [x.strip() for x in line.split(',')]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith('active'):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {'sm_mhz': statistics.median(sm), 'sm_max_mhz': max(mx), 'reasons': sorted(reasons),
+                'samples': len(sm)}
+
+
+def peaks():
+    try:
+        p = json.load(open(os.path.join(ROOT, 'MEASURED_PEAKS.json')))
+        return float(p['hbm_gbs']), 'measured'
+    except Exception:
+        return HBM_FALLBACK, 'fallback'
+
+
+def traffic_per_node():
+    """DRAM bytes per node-update of the step kernels from the committed ncu summary."""
+    try:
+        t = json.load(open(os.path.join(ROOT, 'profiles', 'traffic_wave.json')))
+        return float(t['dram_bytes_per_node_update'])
+    except Exception:
+        return None
+
+
+def oracle_exe():
+    from oracle import build as ob
+    return ob.build()['f32']
+
+
+def cpu_sample(shape_s, steps, warm, threads):
+    """Run the oracle on a scaled sample of the workload; node-updates/s."""
+    exe = oracle_exe()
+    d = tempfile.mkdtemp(prefix='sord_cpu_')
+    try:
+        inp = os.path.join(d, 'in')
+        make_inputs(shape_s, inp, use_torch=False)
+        prm = wave_prm(shape_s, warm + steps)
+        stage_in(prm, os.path.join(d, 'run'), inp)
+        r = subprocess.run([exe, '--threads', str(threads), '--timed-from', str(warm)],
+                           cwd=os.path.join(d, 'run'), capture_output=True, text=True, timeout=900)
+        if r.returncode:
+            raise RuntimeError(r.stderr[-2000:])
+        info = json.loads(r.stdout.strip().splitlines()[-1])
+        nodes = float(np.prod(shape_s))
+        return nodes * steps / info['timed_seconds'], info
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
+# ------------------------------------------------------------------ arms
+def dist_init():
+    ws = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        os.environ.setdefault('MASTER_ADDR', '127.0.0.1')
+        torch.cuda.set_device(local)
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return ws, rank, local, pg
+
+
+def reduce_max(pg, v):
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device='cuda')
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def run_ours(args):
+    from coseis_b200 import build as cb
+    cb.build()
+    from coseis_b200 import _lib
+    ws, rank, local, pg = dist_init()
+    shape = tuple(args.shape)
+    nodes = float(np.prod(shape))
+    inputs = os.path.join(args.cache, 'wave_%dx%dx%d_%d' % (shape + (SEED,)))
+    if rank == 0:
+        make_inputs(shape, inputs)
+    barrier(pg)
+    prof_steps = 3
+    nt = args.warmup + args.steps + prof_steps
+    work = tempfile.mkdtemp(prefix='sord_bench_%d_' % rank)
+    try:
+        text = stage_in(wave_prm(shape, nt), work, inputs)
+        t0 = time.time()
+        s = _lib.Solver(work, text, device=local)
+        setup_s = time.time() - t0
+        s.step(args.warmup)
+        barrier(pg)
+        clk = Clocks(local)
+        clk.start()
+        l0 = s.kernel_launches()
+        w0 = time.time()
+        s.step(args.steps)
+        wall = time.time() - w0
+        ms = s.last_step_ms()
+        launches = s.kernel_launches() - l0
+        clocks = clk.stop()
+        ms_max = reduce_max(pg, ms)
+        s.set_profiling(True)
+        s.step(prof_steps)
+        kt = s.kernel_times()
+        s.set_profiling(False)
+        s.close()
+        e2e = None
+        if not args.no_e2e:
+            e2e = run_e2e(args, shape, inputs, local)
+            barrier(pg)
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+    if rank != 0:
+        return
+    value = ws * nodes * args.steps / (ms_max / 1e3)
+    hbm, src = peaks()
+    alg = algorithmic_bytes_per_node(shape)
+    step_ms = sum(kt[k][0] for k in ('time', 'stress', 'accel', 'mass')) / prof_steps
+    achieved = alg * nodes / (step_ms / 1e3) / 1e9
+    tr = traffic_per_node()
+    out = {
+        'metric': 'node-updates/s', 'value': value, 'unit': 'node-updates/s',
+        'n_gpus': ws, 'steps': args.steps, 'warmup': args.warmup,
+        'ms_per_step': ms_max / args.steps, 'higher_is_better': True, 'scaling': 'weak',
+        'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic (seeded)',
+        'config': {'workload': 'wave226: %dx%dx%d nodes curvilinear terrain, layered von Karman medium, '
+                               '12-node PML on 5 faces, moment-tensor source, 64 receivers' % shape,
+                   'nodes': int(nodes), 'dx_m': DX, 'dt_s': DT, 'parallelism': 'replicas' if ws > 1 else 'single',
+                   'l2': 'inputs larger than L2 (%.1f GB resident)' % (nodes * 100 / 1e9),
+                   'setup_s': round(setup_s, 2), 'host_wall_s': round(wall, 4)},
+        'roofline': {'bound': 'hbm', 'kernel': 'step = k_time + k_stress + k_accel',
+                     'achieved': achieved, 'peak': hbm, 'unit': 'GB/s', 'frac': achieved / hbm,
+                     'peak_source': src, 'algorithmic_bytes_per_node': alg,
+                     'traffic': (tr * nodes if tr else None)},
+        'kernels_ms_per_step': {k: v[0] / prof_steps for k, v in kt.items() if v[1]},
+        'gpu_launches': int(launches),
+        'clocks': clocks,
+        'e2e': e2e,
+    }
+    if ws == 1 and not args.no_cpu:
+        try:
+            thr = os.cpu_count() or 1
+            v, info = cpu_sample(tuple(args.cpu_shape), args.cpu_steps, 1, thr)
+            out['cpu_baseline'] = {'value': v, 'unit': 'node-updates/s', 'cores': thr, 'kind': 'port',
+                                   'sample': 'oracle on the same workload at %dx%dx%d nodes, %d timed steps'
+                                             % (tuple(args.cpu_shape) + (args.cpu_steps,))}
+        except Exception as e:
+            out['cpu_baseline'] = {'value': None, 'error': str(e)[:200]}
+    print(json.dumps(out))
+
+
+def run_e2e(args, shape, inputs, device):
+    """User call end to end: staged files on the host -> sord_run_directory."""
+    from coseis_b200 import _lib
+    nodes = float(np.prod(shape))
+    work = tempfile.mkdtemp(prefix='sord_e2e_')
+    try:
+        stage_in(wave_prm(shape, args.steps), work, inputs)
+        h2d = sum(os.path.getsize(os.path.join(inputs, f)) for f in ('rho.bin', 'vp.bin', 'vs.bin', 'z.bin'))
+        h2d += os.path.getsize(os.path.join(work, 'sord.in'))
+        t0 = time.time()
+        _lib.run_directory(work, device)
+        wall = time.time() - t0
+        d2h = sum(os.path.getsize(os.path.join(work, f)) for f in os.listdir(work)
+                  if f.endswith('.bin') and not os.path.islink(os.path.join(work, f)))
+        return {'value': nodes * args.steps / wall, 'unit': 'node-updates/s',
+                'h2d_bytes_per_step': h2d / args.steps, 'd2h_bytes_per_step': d2h / args.steps,
+                'wall_s': round(wall, 3), 'includes': 'setup from staged host files, %d steps, output files'
+                                                      % args.steps}
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
+def run_reference(args):
+    ws = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    if rank != 0:
+        return
+    thr = os.cpu_count() or 1
+    shape_s = tuple(args.cpu_shape)
+    v, info = cpu_sample(shape_s, args.steps, args.warmup, thr)
+    sample = ('CPU oracle (C++ restatement of sord/*.f90, OpenMP) on the same workload at %dx%dx%d '
+              'nodes, %d timed steps after %d warm-up steps' % (shape_s + (args.steps, args.warmup)))
+    out = {
+        'impl': 'reference', 'metric': 'node-updates/s', 'value': v, 'unit': 'node-updates/s',
+        'n_gpus': ws, 'steps': args.steps, 'warmup': args.warmup,
+        'ms_per_step': info['timed_seconds'] * 1e3 / args.steps, 'higher_is_better': True,
+        'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic (seeded)',
+        'config': {'workload': 'wave226 sample %dx%dx%d' % shape_s, 'nodes': int(np.prod(shape_s))},
+        'cpu_baseline': {'value': v, 'unit': 'node-updates/s', 'cores': thr, 'kind': 'port', 'sample': sample},
+        'e2e': {'value': v, 'unit': 'node-updates/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+    }
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=100)
+    ap.add_argument('--warmup', type=int, default=5)
+    ap.add_argument('--impl', default='ours')
+    ap.add_argument('--shape', type=int, nargs=3, default=list(SHAPE))
+    ap.add_argument('--cpu-shape', type=int, nargs=3, default=[192, 192, 96])
+    ap.add_argument('--cpu-steps', type=int, default=8)
+    ap.add_argument('--cache', default=os.environ.get('SORD_BENCH_CACHE', os.path.join(tempfile.gettempdir(), 'sord_bench')))
+    ap.add_argument('--no-e2e', action='store_true')
+    ap.add_argument('--no-cpu', action='store_true')
+    args = ap.parse_args()
+    if args.impl == 'reference':
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == '__main__':
+    main()

@@ -13,8 +13,8 @@ LIBPATH = os.path.join(HERE, 'libsordgpu.so')
 SYMBOLS = [
     'sord_create', 'sord_step', 'sord_run', 'sord_run_directory',
     'sord_get_field', 'sord_info', 'sord_stats', 'sord_last_step_ms',
-    'sord_kernel_launches', 'sord_last_error', 'sord_error_string',
-    'sord_destroy',
+    'sord_kernel_launches', 'sord_set_profiling', 'sord_kernel_times',
+    'sord_last_error', 'sord_error_string', 'sord_destroy',
 ]
 
 _lib = None
@@ -54,6 +54,10 @@ def load():
     lib.sord_last_step_ms.restype = ctypes.c_double
     lib.sord_kernel_launches.argtypes = [P]
     lib.sord_kernel_launches.restype = ctypes.c_longlong
+    lib.sord_set_profiling.argtypes = [P, ctypes.c_int]
+    lib.sord_set_profiling.restype = ctypes.c_int
+    lib.sord_kernel_times.argtypes = [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
+    lib.sord_kernel_times.restype = ctypes.c_int
     lib.sord_last_error.argtypes = [P]
     lib.sord_last_error.restype = ctypes.c_char_p
     lib.sord_error_string.argtypes = [ctypes.c_int]
@@ -118,6 +122,19 @@ class Solver(object):
 
     def last_step_ms(self):
         return load().sord_last_step_ms(self._h)
+
+    def set_profiling(self, on=True):
+        _check(load().sord_set_profiling(self._h, 1 if on else 0), self._h)
+
+    def kernel_times(self):
+        """{class: (ms, launches)} for time, stress, accel, mass, fault, io, other."""
+        ms = (ctypes.c_double * 7)()
+        cnt = (ctypes.c_longlong * 7)()
+        n = load().sord_kernel_times(self._h, ms, cnt, 7)
+        if n < 0:
+            _check(n, self._h)
+        names = ['time', 'stress', 'accel', 'mass', 'fault', 'io', 'other']
+        return {names[i]: (ms[i], cnt[i]) for i in range(n)}
 
     def kernel_launches(self):
         return load().sord_kernel_launches(self._h)

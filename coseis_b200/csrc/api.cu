@@ -400,6 +400,33 @@ void Solver::write_stats(const std::string& name, const std::vector<float>& col,
     if (o + (int)col.size() == m) opened = false;
 }
 
+void Solver::prof_begin(int cls, cudaEvent_t* e0) {
+    (void)cls;
+    if (!profiling) return;
+    SORD_CUDA(cudaEventCreate(e0));
+    SORD_CUDA(cudaEventRecord(*e0, stream));
+}
+void Solver::prof_end(int cls, cudaEvent_t e0) {
+    if (!profiling || !e0) return;
+    cudaEvent_t e1;
+    SORD_CUDA(cudaEventCreate(&e1));
+    SORD_CUDA(cudaEventRecord(e1, stream));
+    prof_ev.push_back({cls, {e0, e1}});
+}
+void Solver::prof_collect() {
+    if (prof_ev.empty()) return;
+    SORD_CUDA(cudaStreamSynchronize(stream));
+    for (auto& p : prof_ev) {
+        float ms = 0;
+        SORD_CUDA(cudaEventElapsedTime(&ms, p.second.first, p.second.second));
+        kernel_ms[p.first] += ms;
+        kernel_n[p.first] += 1;
+        cudaEventDestroy(p.second.first);
+        cudaEventDestroy(p.second.second);
+    }
+    prof_ev.clear();
+}
+
 void Solver::destroy() {
     if (device >= 0) cudaSetDevice(device);
     if (stream) cudaStreamSynchronize(stream);
@@ -409,6 +436,8 @@ void Solver::destroy() {
     for (int i = 0; i < 6; i++) { fr(d.slabs.p[i]); fr(d.slabs.g[i]); }
     for (auto& io : ops) fr(io.dbuf);
     probes_free(this);
+    for (auto& p : prof_ev) { cudaEventDestroy(p.second.first); cudaEventDestroy(p.second.second); }
+    prof_ev.clear();
     if (hinj) cudaFreeHost(hinj);
     for (auto& e : inj_done) if (e) cudaEventDestroy(e);
     if (ev0) cudaEventDestroy(ev0);
@@ -561,6 +590,33 @@ int sord_stats(const sord_handle* h, double* out, int n) {
 }
 
 double sord_last_step_ms(const sord_handle* h) { return h ? h->s.last_step_ms : 0.0; }
+
+int sord_set_profiling(sord_handle* h, int on) {
+    if (!h) return SORD_E_PARAM;
+    try {
+        h->s.prof_collect();
+        h->s.profiling = on != 0;
+        for (int i = 0; i < 8; i++) { h->s.kernel_ms[i] = 0; h->s.kernel_n[i] = 0; }
+    } catch (const std::exception& e) {
+        return fail(h, e);
+    }
+    return SORD_OK;
+}
+
+int sord_kernel_times(sord_handle* h, double* ms, long long* count, int n) {
+    if (!h) return SORD_E_PARAM;
+    try {
+        h->s.prof_collect();
+    } catch (const std::exception& e) {
+        return fail(h, e);
+    }
+    int m = n < 7 ? n : 7;
+    for (int i = 0; i < m; i++) {
+        if (ms) ms[i] = h->s.kernel_ms[i];
+        if (count) count[i] = h->s.kernel_n[i];
+    }
+    return m;
+}
 
 long long sord_kernel_launches(const sord_handle* h) { return h ? h->s.launches : 0; }
 

@@ -513,10 +513,13 @@ static unsigned grid_1d(long long n) {
 
 void launch_time_update(Solver& s, bool stats) {
     Device& d = s.d;
+    cudaEvent_t e0 = nullptr;
+    s.prof_begin(KC_TIME, &e0);
     k_time<<<grid_1d(s.g.nv), 256, 0, s.stream>>>(s.g, d.v[0], d.v[1], d.v[2], d.u[0], d.u[1], d.u[2], d.w1n[0], d.w1n[1],
                                                   d.w1n[2], d.gam, stats ? 1 : 0, (unsigned*)d.red);
     s.launches++;
     SORD_CUDA(cudaGetLastError());
+    s.prof_end(KC_TIME, e0);
 }
 
 void launch_stress(Solver& s, const InjectList& pot, const InjectList& mom, bool hooke) {
@@ -537,10 +540,13 @@ void launch_stress(Solver& s, const InjectList& pot, const InjectList& mom, bool
     int n0 = s.g.i2cell[0] - s.g.i1cell[0] + 1, n1 = s.g.i2cell[1] - s.g.i1cell[1] + 1, n2 = s.g.i2cell[2] - s.g.i1cell[2] + 1;
     if (n0 < 1 || n1 < 1 || n2 < 1) return;
     dim3 gr(div_up(n0, b.x), div_up(n1, b.y), div_up(n2, b.z));
+    cudaEvent_t e0 = nullptr;
+    s.prof_begin(KC_STRESS, &e0);
     if (s.rect) k_stress<true><<<gr, b, 0, s.stream>>>(A);
     else k_stress<false><<<gr, b, 0, s.stream>>>(A);
     s.launches++;
     SORD_CUDA(cudaGetLastError());
+    s.prof_end(KC_STRESS, e0);
 }
 
 void launch_hooke(Solver& s) {
@@ -582,6 +588,8 @@ void launch_accel(Solver& s, bool mass, bool stats, const InjectList& force) {
     dim3 b(TX, TY, TZ);
     dim3 gr(div_up(n0, TX), div_up(n1, TY), div_up(n2, TZ));
     size_t sm = accel_smem(s.rect);
+    cudaEvent_t e0 = nullptr;
+    s.prof_begin(KC_ACCEL, &e0);
     if (s.rect) {
         static bool set = false;
         if (!set) { SORD_CUDA(cudaFuncSetAttribute(k_accel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)accel_smem(true))); set = true; }
@@ -593,13 +601,17 @@ void launch_accel(Solver& s, bool mass, bool stats, const InjectList& force) {
     }
     s.launches++;
     SORD_CUDA(cudaGetLastError());
+    s.prof_end(KC_ACCEL, e0);
 }
 
 void launch_mass(Solver& s, bool stats) {
     Device& d = s.d;
+    cudaEvent_t e0 = nullptr;
+    s.prof_begin(KC_MASS, &e0);
     k_mass<<<grid_1d(s.g.nv), 256, 0, s.stream>>>(s.g, d.w1n[0], d.w1n[1], d.w1n[2], d.mr, stats ? 1 : 0, (unsigned*)d.red);
     s.launches++;
     SORD_CUDA(cudaGetLastError());
+    s.prof_end(KC_MASS, e0);
 }
 
 static void plane(Solver& s, const int* fn, float* f0, float* f1, float* f2, int d, int p, int ps, int mode, int mask,

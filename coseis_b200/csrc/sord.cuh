@@ -145,6 +145,9 @@ enum FaultArr {
 
 struct Solver;
 
+// kernel classes for sord_kernel_times
+enum { KC_TIME = 0, KC_STRESS = 1, KC_ACCEL = 2, KC_MASS = 3, KC_FAULT = 4, KC_IO = 5, KC_OTHER = 6 };
+
 // kernels.cu entry points
 void launch_time_update(Solver& s, bool stats);
 void launch_stress(Solver& s, const InjectList& pot, const InjectList& mom, bool hooke);
@@ -195,6 +198,15 @@ struct Solver {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_step_ms = 0;
     long long launches = 0;
+    // optional per-kernel device timing (sord_set_profiling): class id per
+    // launch, events recorded around the launch on the solver stream
+    bool profiling = false;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof_ev;
+    double kernel_ms[8] = {};
+    long long kernel_n[8] = {};
+    void prof_begin(int cls, cudaEvent_t* e0);
+    void prof_end(int cls, cudaEvent_t e0);
+    void prof_collect();
     // time
     float tm = 0;
     int it = 0, nt = 0;

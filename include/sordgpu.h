@@ -75,6 +75,17 @@ int sord_stats(const sord_handle* h, double* out, int n);
  * handle's stream, step kernels and I/O hooks included). */
 double sord_last_step_ms(const sord_handle* h);
 
+/* Per-kernel device timing for performance reports.  With profiling on,
+ * CUDA events are recorded around each step kernel on the handle's stream
+ * and accumulated per class: 0 time update, 1 stress, 2 acceleration,
+ * 3 mass, 4 fault, 5 field I/O, 6 other.  Turning it on or off resets the
+ * sums.  sord_kernel_times writes min(n, 7) totals (ms) and launch counts
+ * and returns that number.  No reference counterpart (the reference writes
+ * host timers to prof-*.bin, statistics.f90:116-129; those files are
+ * written here too). */
+int sord_set_profiling(sord_handle* h, int on);
+int sord_kernel_times(sord_handle* h, double* ms, long long* count, int n);
+
 /* Number of kernels this library launched since the handle was created. */
 long long sord_kernel_launches(const sord_handle* h);
 

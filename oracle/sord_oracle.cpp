@@ -183,6 +183,8 @@ struct Sord {
     bool stats_open[20];
     std::chrono::steady_clock::time_point clock0;
     int nt_limit = -1;
+    int timed_from = -1;              // report the time of steps timed_from+1 .. nt
+    double timed_seconds = 0;
 
     long long clock_ticks() {
         return (long long)std::chrono::duration_cast<std::chrono::microseconds>(std::chrono::steady_clock::now() - clock0).count();
@@ -1969,23 +1971,27 @@ struct Sord {
         init_finite_source();
         init_rupture();
         resample_material();
+        std::chrono::steady_clock::time_point tw = std::chrono::steady_clock::now();
         for (it = 1; it <= nt; it++) {
+            if (it == timed_from + 1) tw = std::chrono::steady_clock::now();
             timers[0] = timers[1] = timers[2] = timers[3] = 0;
             step_time();
             step_stress();
             step_accel();
             stats();
         }
+        if (timed_from >= 0) timed_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - tw).count();
     }
 };
 
 int main(int argc, char** argv) {
     std::string path = "sord.in";
-    int threads = 1, ntl = -1;
+    int threads = 1, ntl = -1, tfrom = -1;
     for (int i = 1; i < argc; i++) {
         std::string a = argv[i];
         if (a == "--threads" && i + 1 < argc) threads = atoi(argv[++i]);
         else if (a == "--nt-limit" && i + 1 < argc) ntl = atoi(argv[++i]);
+        else if (a == "--timed-from" && i + 1 < argc) tfrom = atoi(argv[++i]);
         else path = a;
     }
 #ifdef _OPENMP
@@ -1995,12 +2001,14 @@ int main(int argc, char** argv) {
 #endif
     Sord* s = new Sord();
     s->nt_limit = ntl;
+    s->timed_from = tfrom;
     try {
         auto t0 = std::chrono::steady_clock::now();
         s->run(path);
         double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-        fprintf(stdout, "{\"oracle\": \"%s\", \"nt\": %d, \"nodes\": %lld, \"seconds\": %.6f}\n",
-                sizeof(real) == 4 ? "f32" : "f64", s->nt, (long long)s->nn[0] * s->nn[1] * s->nn[2], el);
+        fprintf(stdout, "{\"oracle\": \"%s\", \"nt\": %d, \"nodes\": %lld, \"seconds\": %.6f, \"timed_from\": %d, \"timed_seconds\": %.6f, \"threads\": %d}\n",
+                sizeof(real) == 4 ? "f32" : "f64", s->nt, (long long)s->nn[0] * s->nn[1] * s->nn[2], el, s->timed_from,
+                s->timed_seconds, threads);
     } catch (SordStop& e) {
         fprintf(stderr, "%s\n", e.what());
         return 1;
