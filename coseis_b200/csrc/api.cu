@@ -212,13 +212,84 @@ static float norm_max(Solver& s, float* const w[3]) {
     return dev_reduce_max(s, vol(s, s.d.s1), s.g.i1core, s.g.i2core);
 }
 
+// Can step `n` run as one fused kernel?  Every field-I/O op firing at that
+// step must be an output of v, u, a or their magnitudes (read between
+// kernels) or a '.' point op on the potency / moment tensor (applied inside
+// the kernel); no fault, and no boundary condition that copies planes.
+bool Solver::fusable(int n) const {
+    if (!use_fused || g.ifn != 0 || !bc_noop(prm)) return false;
+    for (auto& io : ops) {
+        int it1 = io.ii[3][0], it2 = io.ii[3][1], dit = io.ii[3][2];
+        if (n > it2 || io.op[0] == '#' || n < it1 || ((n - it1) % dit) != 0) continue;
+        const std::string& f = io.field;
+        char op2 = io.op.size() > 1 ? io.op[1] : ' ';
+        bool out = op2 == '>';
+        if (out) {
+            bool ok = f == "vx" || f == "vy" || f == "vz" || f == "ux" || f == "uy" || f == "uz" || f == "ax" ||
+                      f == "ay" || f == "az" || f == "vm2" || f == "um2" || f == "am2";
+            if (!ok) return false;
+        } else {
+            bool tensor = f[0] == 'p' || f[0] == 'm';
+            if (!(tensor && io.op == "." && bc_cells_noop(prm))) return false;
+        }
+    }
+    return true;
+}
+
 void Solver::step() {
     it++;
     for (auto& t : timers) t = 0;
     long long t_step = clock_us();
     const bool st = it % prm.itstats == 0;
-    Geom& G = g;
     if (st) SORD_CUDA(cudaMemsetAsync(d.red, 0, sizeof(unsigned) * 8, stream));
+    if (!fusable(it)) {
+        folded = false;
+        step_general(st);
+        timers[3] = clock_us() - t_step;
+        stats();
+        return;
+    }
+    long long tio = 0;
+    auto io = [&](const char* passes, const char* field, FieldView f) {
+        long long t0 = clock_us();
+        field_io(*this, passes, field, f);
+        tio += clock_us() - t0;
+    };
+    // leapfrog update of this step, unless the previous fused step did it
+    tm = prm.tm0 + g.dt * (float)(it - 1);
+    if (!folded) launch_time_update(*this, false);
+    for (int i = 0; i < 3; i++) io("<>", kVel[i], vol(*this, d.v[i]));
+    io(">", "vm2", vol(*this, d.s1));
+    for (int i = 0; i < 3; i++) io("<>", kDis[i], vol(*this, d.u[i]));
+    io(">", "um2", vol(*this, d.s1));
+    std::vector<Inject> pot, mom, frc;
+    if (prm.source == "potency") finite_source_entries(*this, pot);
+    if (prm.source == "moment") finite_source_entries(*this, mom);
+    if (prm.source == "force") finite_source_entries(*this, frc);
+    tensor_point_ops(*this, kPot, pot);
+    tensor_point_ops(*this, kMom, mom);
+    const bool fold = it < nt && fusable(it + 1);
+    const bool write_a = any_pass(*this, kAcc, 3, '>') || field_active(*this, "am2", '>') || it == nt;
+    InjectList lp = upload(*this, 0, pot), lm = upload(*this, 1, mom), lf = upload(*this, 2, frc);
+    launch_fused(*this, lp, lm, lf, fold, write_a, st);
+    folded = fold;
+    for (int i = 0; i < 3; i++) io("<>", kAcc[i], vol(*this, d.w1n[i]));
+    io(">", "am2", vol(*this, d.s1));
+    if (st) {
+        amax = read_max(*this, 0);
+        vmax = read_max(*this, 1);
+        umax = read_max(*this, 2);
+        wmax = read_max(*this, 3);
+    }
+    timers[1] = tio;
+    timers[3] = clock_us() - t_step;
+    stats();
+}
+
+// One step with separate kernels and every field-I/O hook of
+// time_integration.f90, stress.f90 and acceleration.f90 in place.
+void Solver::step_general(bool st) {
+    Geom& G = g;
     long long tio = 0;
     auto io = [&](const char* passes, const char* field, FieldView f) {
         long long t0 = clock_us();
@@ -289,8 +360,6 @@ void Solver::step() {
     if (st) amax = ain ? norm_max(*this, d.w1n) : read_max(*this, 0);
     io(">", "am2", vol(*this, d.s1));
     timers[1] = tio;
-    timers[3] = clock_us() - t_step;
-    stats();
 }
 
 // statistics.f90:13-131 (maxima exact in FP32; energy sums in FP64)
@@ -433,7 +502,9 @@ void Solver::destroy() {
     auto fr = [](void* p) { if (p) cudaFree(p); };
     for (int i = 0; i < 3; i++) { fr(d.x[i]); fr(d.v[i]); fr(d.u[i]); fr(d.w1n[i]); fr(d.sd[i]); fr(d.so[i]); }
     fr(d.vc); fr(d.mr); fr(d.lam); fr(d.mu); fr(d.gam); fr(d.yy); fr(d.s1); fr(d.s2); fr(d.pmlc); fr(d.red); fr(d.inj); fr(d.fp);
-    for (int i = 0; i < 6; i++) { fr(d.slabs.p[i]); fr(d.slabs.g[i]); }
+    for (int i = 0; i < 6; i++) { fr(d.slabs.p[i]); fr(d.slabs.g[i]); fr(d.gb[i]); }
+    for (int i = 0; i < 3; i++) { fr(d.vb[i]); fr(d.ub[i]); }
+    fr(d.x1d); fr(d.y1d);
     for (auto& io : ops) fr(io.dbuf);
     probes_free(this);
     for (auto& p : prof_ev) { cudaEventDestroy(p.second.first); cudaEventDestroy(p.second.second); }

@@ -151,10 +151,10 @@ __global__ void __launch_bounds__(256) k_stress(StressArgs A) {
             float W[8], U[8], V[8];
             if (anyS) {
 #pragma unroll
-                for (int t = 0; t < 8; t++) { U[t] = A.u[ic][cq[kTermCorner[t]]]; V[t] = A.v[ic][cq[kTermCorner[t]]]; }
+                for (int t = 0; t < 8; t++) { U[t] = A.u[ic][cq[term_corner(t)]]; V[t] = A.v[ic][cq[term_corner(t)]]; }
             } else {
 #pragma unroll
-                for (int t = 0; t < 8; t++) W[t] = A.w[ic][cq[kTermCorner[t]]];
+                for (int t = 0; t < 8; t++) W[t] = A.w[ic][cq[term_corner(t)]];
             }
 #pragma unroll
             for (int iid = 0; iid < 3; iid++) {
@@ -400,7 +400,8 @@ __global__ void __launch_bounds__(NT_ACC) k_accel(AccelArgs A) {
                         float Wc[8], Vc[8];
 #pragma unroll
                         for (int t = 0; t < 8; t++) {
-                            int n = (cj + kHgOff[t][0]) + NX * ((ck + kHgOff[t][1]) + NY * (cl + kHgOff[t][2]));
+                            int hc = hg_corner(t);
+                            int n = (cj + (hc & 1)) + NX * ((ck + ((hc >> 1) & 1)) + NY * (cl + (hc >> 2)));
                             Wc[t] = sW[ic * NNODE + n];
                             Vc[t] = sV[ic * NNODE + n];
                         }
@@ -418,7 +419,7 @@ __global__ void __launch_bounds__(NT_ACC) k_accel(AccelArgs A) {
                         float Hc[8];
 #pragma unroll
                         for (int t = 0; t < 8; t++)
-                            Hc[t] = H[(tj + 1 - kHgOff[t][0]) + CX * ((tk + 1 - kHgOff[t][1]) + CY * (tl + 1 - kHgOff[t][2]))];
+                            Hc[t] = H[(tj + 1 - (hg_corner(t) & 1)) + CX * ((tk + 1 - ((hg_corner(t) >> 1) & 1)) + CY * (tl + 1 - (hg_corner(t) >> 2)))];
                         s2 = hg_sum(Hc, iq);
                     }
                     f[ic] = f[ic] - s2;

@@ -10,6 +10,7 @@
 // so the fast path computes exactly what the general operator would.
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "sord.cuh"
@@ -110,7 +111,7 @@ __global__ void k_volume(Geom g, const float* x0, const float* x1, const float* 
                 for (int n = 0; n < 8; n++) X[c][n] = X_[c][q + (n & 1) + ((n >> 1) & 1) * g.sy + ((n >> 2) & 1) * g.sz];
             float B[8], F[8];
             brackets_nc(X, 2, B);
-            for (int t = 0; t < 8; t++) F[t] = X[2][kTermCorner[t]];
+            for (int t = 0; t < 8; t++) F[t] = X[2][term_corner(t)];
             v = stencil8(F, B, g.h);
             if (g.ifn && (g.ifn == 1 ? j : g.ifn == 2 ? k : l) == g.irup) v = 0.f;
         }
@@ -215,7 +216,7 @@ __global__ void k_rect_check(Geom g, const float* x0, const float* x1, const flo
                 float B[8];
                 brackets_nc(X, a, B);
                 for (int t = 0; t < 8; t++)
-                    if (!(B[t] == ref[8 * a + t])) atomicOr(bad, 1u);
+                    if (!(B[t] == ref[8 * a + t])) atomicOr(bad, 1u << a);
             }
         }
         // node test: terms whose cell is real and off the fault plane
@@ -235,11 +236,23 @@ __global__ void k_rect_check(Geom g, const float* x0, const float* x1, const flo
                     bool real = true;
                     for (int d = 0; d < 3; d++) real = real && c[d] >= g.i1cell[d] && c[d] <= g.i2cell[d];
                     if (g.ifn && c[g.ifn - 1] == g.irup) real = false;
-                    if (real && !(B[t] == ref[24 + 8 * a + t])) atomicOr(bad, 2u);
+                    if (real && !(B[t] == ref[24 + 8 * a + t])) atomicOr(bad, 8u << a);
                 }
             }
         }
     }
+}
+
+// terrain mesh test: x depends on j only and y on k only (bit 64 if not)
+__global__ void k_terrain_check(Geom g, const float* x0, const float* x1, const float* x1d, const float* y1d, unsigned* bad) {
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < g.nv; q += (long long)gridDim.x * blockDim.x) {
+        int j = (int)(q % g.sy) + 1, k = (int)((q / g.sy) % g.nm[1]) + 1;
+        if (!(x0[q] == x1d[j - 1]) || !(x1[q] == y1d[k - 1])) atomicOr(bad, 64u);
+    }
+}
+__global__ void k_line(const float* src, float* dst, int n, long long stride, long long base) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = src[base + stride * i];
 }
 
 // ------------------------------------------------------------ host side
@@ -331,6 +344,9 @@ static void allocate_arrays(Solver& s) {
     alloc(s, &d.vc, nv); alloc(s, &d.mr, nv); alloc(s, &d.lam, nv); alloc(s, &d.mu, nv); alloc(s, &d.gam, nv);
     alloc(s, &d.yy, nv); alloc(s, &d.s1, nv); alloc(s, &d.s2, nv);
     alloc(s, &d.red, kRedFloats);
+    for (int i = 0; i < 3; i++) { alloc(s, &d.vb[i], nv); alloc(s, &d.ub[i], nv); }
+    const char* fz = getenv("SORD_FUSED");
+    s.use_fused = !(fz && fz[0] == '0');
     SORD_CUDA(cudaMalloc((void**)&d.inj, sizeof(Inject) * kInjectSlots * kMaxInject));
     SORD_CUDA(cudaMallocHost((void**)&s.hinj, sizeof(Inject) * kInjectSlots * kMaxInject));
 }
@@ -473,7 +489,10 @@ static void init_pml(Solver& s) {
     Params& P = s.prm;
     int np = P.npml;
     if (np < 1) {
-        for (int i = 0; i < 6; i++) { s.d.slabs.p[i] = s.d.slabs.g[i] = nullptr; s.d.slabs.tp[i] = s.d.slabs.tg[i] = 0; }
+        for (int i = 0; i < 6; i++) {
+            s.d.slabs.p[i] = s.d.slabs.g[i] = s.d.gb[i] = nullptr;
+            s.d.slabs.tp[i] = s.d.slabs.tg[i] = 0;
+        }
         alloc(s, &s.d.pmlc, 4);
         return;
     }
@@ -508,6 +527,7 @@ static void init_pml(Solver& s) {
             int sidx = side * 3 + a;
             alloc(s, &sl.p[sidx], other * sl.tp[sidx] * 3);
             alloc(s, &sl.g[sidx], other * sl.tg[sidx] * 3);
+            alloc(s, &s.d.gb[sidx], other * sl.tg[sidx] * 3);
         }
     }
 }
@@ -605,9 +625,13 @@ static void resample_material(Solver& s) {
     dev_fill(s, d.s2, nv, 0.f);
 }
 
+// Mesh class of the step kernels: rectilinear (every real cell's brackets
+// equal the reference cell's, bit for bit), terrain (x = x(j), y = y(k) and
+// the z-free direction's brackets constant) or general.
 static void rect_check(Solver& s) {
     Geom& g = s.g;
     s.rect = false;
+    s.geom = GEOM_GENERAL;
     int jc[3], jn[3];
     for (int a = 0; a < 3; a++) {
         if (g.i2cell[a] - g.i1cell[a] < 2) return;  // too small to have interior references
@@ -631,10 +655,27 @@ static void rect_check(Solver& s) {
     SORD_CUDA(cudaMemcpyAsync(&hb, bad, sizeof(unsigned), cudaMemcpyDeviceToHost, s.stream));
     SORD_CUDA(cudaMemcpyAsync(hr, ref, sizeof(float) * 48, cudaMemcpyDeviceToHost, s.stream));
     SORD_CUDA(cudaStreamSynchronize(s.stream));
+    for (int a = 0; a < 3; a++)
+        for (int t = 0; t < 8; t++) { s.br.bnc[a][t] = hr[8 * a + t]; s.br.bcn[a][t] = hr[24 + 8 * a + t]; }
     if (hb == 0) {
         s.rect = true;
-        for (int a = 0; a < 3; a++)
-            for (int t = 0; t < 8; t++) { s.br.bnc[a][t] = hr[8 * a + t]; s.br.bcn[a][t] = hr[24 + 8 * a + t]; }
+        s.geom = GEOM_RECT;
+        return;
+    }
+    if ((hb & (4u | 32u)) == 0) {
+        // direction 3 (x-y brackets) constant: test x = x(j), y = y(k)
+        alloc(s, &s.d.x1d, g.nm[0]);
+        alloc(s, &s.d.y1d, g.nm[1]);
+        k_line<<<div_up(g.nm[0], 128), 128, 0, s.stream>>>(s.d.x[0], s.d.x1d, g.nm[0], 1, g.idx(1, g.i1core[1], g.i1core[2]));
+        LAUNCH_CHECK(s);
+        k_line<<<div_up(g.nm[1], 128), 128, 0, s.stream>>>(s.d.x[1], s.d.y1d, g.nm[1], g.sy, g.idx(g.i1core[0], 1, g.i1core[2]));
+        LAUNCH_CHECK(s);
+        SORD_CUDA(cudaMemsetAsync(bad, 0, sizeof(unsigned), s.stream));
+        k_terrain_check<<<gfor(g.nv), 256, 0, s.stream>>>(g, s.d.x[0], s.d.x[1], s.d.x1d, s.d.y1d, bad);
+        LAUNCH_CHECK(s);
+        SORD_CUDA(cudaMemcpyAsync(&hb, bad, sizeof(unsigned), cudaMemcpyDeviceToHost, s.stream));
+        SORD_CUDA(cudaStreamSynchronize(s.stream));
+        if (hb == 0) s.geom = GEOM_TERRAIN;
     }
 }
 

@@ -118,6 +118,33 @@ struct InjectList {
     int n;
 };
 
+// Mesh classes of the fused step kernel: rectilinear (all support-operator
+// brackets equal at every real cell), terrain (x = x(j), y = y(k), and the
+// z-free direction's brackets constant), general.
+enum { GEOM_RECT = 0, GEOM_TERRAIN = 1, GEOM_GENERAL = 2 };
+
+struct StepArgs {
+    Geom g;
+    Brackets br;
+    const float* x1d;  // terrain: x at nodes j = 1..nm0
+    const float* y1d;  // terrain: y at nodes k = 1..nm1
+    const float* x[3];
+    const float* vin[3];
+    const float* uin[3];
+    float* vout[3];
+    float* uout[3];
+    float* aout[3];
+    const float *gam, *mr, *lam, *mu, *vc, *yy;
+    const float* pmlc;
+    Slabs sl;
+    float* gout[6];
+    InjectList pot, mom, force;
+    float hg1, dh2;
+    int hourglass, hgvisc, fold, stats;
+    unsigned* red;
+    int segl;
+};
+
 // Device state of one handle.
 struct Device {
     float* x[3] = {};
@@ -130,6 +157,11 @@ struct Device {
     float *s1 = nullptr, *s2 = nullptr;  // volume scratch (field-I/O, setup, magnitudes)
     float* pmlc = nullptr;               // dn1, dn2, dc1, dc2 (npml each)
     Slabs slabs{};
+    float* vb[3] = {};                   // second v / u buffers of the fused step
+    float* ub[3] = {};
+    float* gb[6] = {};                   // second PML g buffers
+    float* x1d = nullptr;                // terrain meshes: x(j), y(k)
+    float* y1d = nullptr;
     float* red = nullptr;                // reduction scratch (uint bit patterns / doubles)
     Inject* inj = nullptr;               // device injection lists (3 * kMaxInject)
     // fault plane (nm with extent 1 along ifn)
@@ -158,6 +190,8 @@ void launch_mass(Solver& s, bool stats);
 void launch_vector_bc(Solver& s, float* const f[3], const int* bc1, const int* bc2, const int* i1, const int* i2);
 void launch_scalar_bc(Solver& s, float* f, const int* fn, const int* bc1, const int* bc2, const int* i1, const int* i2);
 void launch_inject(Solver& s, float* const f[6], const InjectList& l);
+void launch_fused(Solver& s, const InjectList& pot, const InjectList& mom, const InjectList& force, bool fold, bool write_a,
+                  bool stats);
 
 // setup.cu
 void setup_all(Solver& s);
@@ -192,6 +226,9 @@ struct Solver {
     Device d{};
     Brackets br{};
     bool rect = false;        // rectilinear fast path verified
+    int geom = GEOM_GENERAL;  // mesh class of the fused kernel
+    bool use_fused = true;    // fused step kernel allowed (SORD_FUSED=0 disables)
+    bool folded = false;      // previous step already applied this step's leapfrog update
     std::string workdir;
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -240,6 +277,8 @@ struct Solver {
     std::string path(const std::string& f) const;
 
     void step();
+    void step_general(bool st);
+    bool fusable(int step) const;
     void stats();
     void write_stats(const std::string& name, const std::vector<float>& col, int m, int o, bool& opened);
     void destroy();

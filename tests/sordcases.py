@@ -127,6 +127,42 @@ def case_slipweak(nt=40):
     return prm
 
 
+def case_visc(n=23, nt=30):
+    """Viscosity, viscous hourglass in the PML, receivers only (every step fused)."""
+    prm = case_explosion(n, nt, npml=5)
+    prm['gam'] = [0.4]
+    prm['hourglass'] = [1.0, 2.0]
+    prm.pop('am2')
+    prm.pop('wm2')
+    prm['bc1'] = ['pml', 'pml', 'free']
+    return prm
+
+
+def case_noise(n=18, nt=16):
+    """Random mesh (gridnoise), PML, moment source, receivers only: general fused path."""
+    prm = case_visc(n, nt)
+    prm['gridnoise'] = 0.15
+    prm['npml'] = 4
+    return prm
+
+
+def case_wave(shape=(40, 36, 30), nt=24):
+    """The benchmark workload (terrain mesh, layered random medium read from
+    '=<' files, moment tensor, surface receivers) at a small size."""
+    import bench
+    return bench.wave_prm(shape, nt, nrec=6)
+
+
+def wave_inputs(path, shape=(40, 36, 30)):
+    import bench
+    inp = os.path.join(os.path.dirname(path), 'wave_inputs')
+    bench.make_inputs(shape, inp, use_torch=False)
+    for f in ('rho.bin', 'vp.bin', 'vs.bin', 'z.bin'):
+        dst = os.path.join(path, f)
+        if not os.path.exists(dst):
+            os.symlink(os.path.join(inp, f), dst)
+
+
 CASES = {
     'mpi': case_mpi,
     'pml': case_pml,
@@ -135,11 +171,17 @@ CASES = {
     'bc': case_bc,
     'rupture': case_rupture,
     'slipweak': case_slipweak,
+    'visc': case_visc,
+    'noise': case_noise,
+    'wave': case_wave,
 }
+INPUTS = {'wave': wave_inputs}
 
 
-def stage(prm, path, realsize=4):
+def stage(prm, path, realsize=4, inputs=None):
     os.makedirs(path, exist_ok=True)
+    if inputs:
+        inputs(path)
     cwd = os.getcwd()
     os.chdir(path)
     try:
@@ -155,9 +197,19 @@ def run_oracle(path, exe, threads=4):
     return json.loads(r.stdout.strip().splitlines()[-1])
 
 
-def run_gpu(path):
+def run_gpu(path, fused=True):
+    """Run the CUDA solver through the C ABI; SORD_FUSED (read when a handle
+    is created) selects the fused step kernel or the per-stage kernels."""
     from coseis_b200 import _lib
-    _lib.run_directory(path)
+    old = os.environ.get('SORD_FUSED')
+    os.environ['SORD_FUSED'] = '1' if fused else '0'
+    try:
+        _lib.run_directory(path)
+    finally:
+        if old is None:
+            del os.environ['SORD_FUSED']
+        else:
+            os.environ['SORD_FUSED'] = old
 
 
 def outputs(path):

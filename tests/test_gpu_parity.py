@@ -22,14 +22,16 @@ TOL_EXACT = 0.0
 TOL_LOOSE = 1e-4
 
 
+@pytest.mark.parametrize('fused', [True, False], ids=['fused', 'staged'])
 @pytest.mark.parametrize('name', sorted(sc.CASES))
-def test_parity(name, tmp_path, oracle_bins, gpu_lib):
+def test_parity(name, fused, tmp_path, oracle_bins, gpu_lib):
     prm = sc.CASES[name]()
+    inputs = sc.INPUTS.get(name)
     a, b = str(tmp_path / 'oracle'), str(tmp_path / 'gpu')
-    sc.stage(prm, a)
-    sc.stage(prm, b)
+    sc.stage(prm, a, inputs=inputs)
+    sc.stage(prm, b, inputs=inputs)
     sc.run_oracle(a, oracle_bins['f32'])
-    sc.run_gpu(b)
+    sc.run_gpu(b, fused=fused)
     res = sc.compare(a, b)
     assert res, 'no outputs'
     bad = {}
