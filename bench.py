@@ -84,7 +84,7 @@ def von_karman(shape, dx, a, hurst, std, seed, use_torch=True):
     return f.astype(np.float32)
 
 
-def make_inputs(shape, outdir, seed=SEED, use_torch=True):
+def make_inputs(shape, outdir, seed=SEED, use_torch=True, hill=500.0):
     """Write rho.bin, vp.bin, vs.bin (cells) and z.bin (nodes), j fastest."""
     os.makedirs(outdir, exist_ok=True)
     mark = os.path.join(outdir, 'ok.json')
@@ -96,7 +96,7 @@ def make_inputs(shape, outdir, seed=SEED, use_torch=True):
     y = DX * np.arange(ny, dtype=np.float32)
     xc, yc = x[-1] * 0.5, y[-1] * 0.5
     sig = 5000.0 * min(1.0, min(nx, ny) / 768.0)
-    h = 500.0 * np.exp(-((x[None, :] - xc) ** 2 + (y[:, None] - yc) ** 2) / (2 * sig * sig))
+    h = hill * np.exp(-((x[None, :] - xc) ** 2 + (y[:, None] - yc) ** 2) / (2 * sig * sig))
     h = h.astype(np.float32)
     with open(os.path.join(outdir, 'z.bin'), 'wb') as fh:
         for l in range(nz):
@@ -320,9 +320,9 @@ def run_ours(args):
     ws, rank, local, pg = dist_init()
     shape = tuple(args.shape)
     nodes = float(np.prod(shape))
-    inputs = os.path.join(args.cache, 'wave_%dx%dx%d_%d' % (shape + (SEED,)))
+    inputs = os.path.join(args.cache, 'wave_%dx%dx%d_%d_%g' % (shape + (SEED, args.hill)))
     if rank == 0:
-        make_inputs(shape, inputs)
+        make_inputs(shape, inputs, hill=args.hill)
     barrier(pg)
     prof_steps = 3
     nt = args.warmup + args.steps + prof_steps
@@ -450,6 +450,7 @@ def main():
     ap.add_argument('--cache', default=os.environ.get('SORD_BENCH_CACHE', os.path.join(tempfile.gettempdir(), 'sord_bench')))
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu', action='store_true')
+    ap.add_argument('--hill', type=float, default=500.0, help='topography peak (m); 0 gives a rectilinear mesh')
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)

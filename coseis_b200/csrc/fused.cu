@@ -25,6 +25,7 @@
 // general meshes compute all three.  Each cell's brackets are evaluated
 // once and shared by the cell's gradient and its eight corner nodes'
 // divergence (stencil.cuh: cell_cn_brackets).
+#include "inject.cuh"
 #include "sord.cuh"
 #include "stencil.cuh"
 
@@ -40,7 +41,9 @@ constexpr int NTH = FJ * FK;
 template <int GEOM>
 struct Lay {
     static constexpr int NCOORD = GEOM == GEOM_RECT ? 0 : GEOM == GEOM_TERRAIN ? 1 : 3;
-    static constexpr int NODEF = 7 + NCOORD;  // u(3) v(3) gam coords
+    static constexpr int PRE = 7 + NCOORD;    // prefetched: u(3) v(3) gam coords
+    static constexpr int NODEF = 9 + NCOORD;  // shared: u(3) v(3) w = u + gam v (3) coords
+    static constexpr int CO = 9;              // first coordinate field
     static constexpr int NDIR = GEOM == GEOM_RECT ? 0 : GEOM == GEOM_TERRAIN ? 2 : 3;
     static constexpr int CELLF = 6 + 12 + 8 * NDIR;  // stress, hourglass, divergence brackets
     static constexpr size_t bytes = sizeof(float) * (size_t)(3 * NPL * NODEF + 2 * NCL * CELLF);
@@ -93,8 +96,17 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
     const float h = g.h, dt = g.dt;
     float st_a = 0.f, st_v = 0.f, st_u = 0.f, st_w = 0.f;
 
+    // point injections that fall inside this block (cells / nodes it computes)
+    __shared__ Inject lpot[kLocalInject], lmom[kLocalInject], lfrc[kLocalInject];
+    __shared__ int lcnt[3];
+    gather_inject(A.pot, lpot, &lcnt[0], g, j0 - 1, j0 + FOJ - 1, k0 - 1, k0 + FOK - 1, L0 - 1, L1);
+    gather_inject(A.mom, lmom, &lcnt[1], g, j0 - 1, j0 + FOJ - 1, k0 - 1, k0 + FOK - 1, L0 - 1, L1);
+    gather_inject(A.force, lfrc, &lcnt[2], g, j0, j0 + FOJ - 1, k0, k0 + FOK - 1, L0, L1);
+    __syncthreads();
+    const int npot = lcnt[0], nmom = lcnt[1], nfrc = lcnt[2];
+
     // ---------------------------------------------------------------- loads
-    float pre[2][L::NODEF];
+    float pre[2][L::PRE];
     auto fetch = [&](int l) {
 #pragma unroll
         for (int r = 0; r < 2; r++) {
@@ -119,10 +131,30 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
 #pragma unroll
         for (int r = 0; r < 2; r++) {
             const int n = tid + r * NTH;
-            if (n < NPL)
+            if (n < NPL) {
 #pragma unroll
-                for (int f = 0; f < L::NODEF; f++) NODE(slot, f, n) = pre[r][f];
+                for (int f = 0; f < 6; f++) NODE(slot, f, n) = pre[r][f];
+                // w1 = u + gam * v (time_integration.f90:36)
+#pragma unroll
+                for (int c = 0; c < 3; c++) NODE(slot, 6 + c, n) = pre[r][c] + pre[r][6] * pre[r][3 + c];
+#pragma unroll
+                for (int f = 0; f < L::NCOORD; f++) NODE(slot, L::CO + f, n) = pre[r][7 + f];
+            }
         }
+    };
+
+    // per-plane statics of this thread's cell (lam, mu, 1/V, yy) and node
+    // (mass ratio), loaded one plane ahead of their use
+    float cur[5];
+    auto stat_load = [&](int l, float* o) {
+        const bool cv = cellcol && l >= g.i1cell[2] && l <= g.i2cell[2];
+        const long long qc = cv ? g.idx(J, K, l) : 0;
+        o[0] = cv ? A.lam[qc] : 0.f;
+        o[1] = cv ? A.mu[qc] : 0.f;
+        o[2] = cv ? A.vc[qc] : 0.f;
+        o[3] = cv ? A.yy[qc] : 0.f;
+        const bool nv = outcol && l >= g.i1node[2] && l <= g.i2node[2];
+        o[4] = nv ? A.mr[g.idx(jn, kn, l)] : 0.f;
     };
 
     // ---------------------------------------------------------------- cell phase
@@ -157,13 +189,13 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
                     for (int n = 0; n < 8; n++) {
                         X[0][n] = (n & 1) ? xb : xa;
                         X[1][n] = ((n >> 1) & 1) ? yb : ya;
-                        X[2][n] = NODE(ns[n], 7, ni[n]);
+                        X[2][n] = NODE(ns[n], L::CO, ni[n]);
                     }
                 } else {
 #pragma unroll
                     for (int c = 0; c < 3; c++)
 #pragma unroll
-                        for (int n = 0; n < 8; n++) X[c][n] = NODE(ns[n], 7 + c, ni[n]);
+                        for (int n = 0; n < 8; n++) X[c][n] = NODE(ns[n], L::CO + c, ni[n]);
                 }
 #pragma unroll
                 for (int a = 0; a < L::NDIR; a++) {
@@ -193,7 +225,7 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
                     const float uu = NODE(ns[n], ic, ni[n]), vv = NODE(ns[n], 3 + ic, ni[n]);
                     U[t] = uu;
                     V[t] = vv;
-                    W[t] = uu + NODE(ns[n], 6, ni[n]) * vv;
+                    W[t] = NODE(ns[n], 6 + ic, ni[n]);
                 }
 #pragma unroll
                 for (int iid = 0; iid < 3; iid++) {
@@ -225,26 +257,16 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
                     else eo[3 - ic - id] = eo[3 - ic - id] + 0.5f * s;
                 }
             }
-            for (int e = 0; e < A.pot.n; e++)
-                if (A.pot.e[e].idx == q) {
-                    const int c = A.pot.e[e].comp;
-                    if (c < 3) ed[c] = ed[c] + A.pot.e[e].inc;
-                    else eo[c - 3] = eo[c - 3] + A.pot.e[e].inc;
-                }
+            apply_inject(lpot, npot, A.pot, q, ed, eo);
             {
-                const float lm = A.lam[q], m2 = 2.0f * A.mu[q];
+                const float lm = cur[0], m2 = 2.0f * cur[1];
                 const float s1 = lm * (ed[0] + ed[1] + ed[2]);
 #pragma unroll
                 for (int i = 0; i < 3; i++) { ed[i] = m2 * ed[i] + s1; eo[i] = m2 * eo[i]; }
             }
-            for (int e = 0; e < A.mom.n; e++)
-                if (A.mom.e[e].idx == q) {
-                    const int c = A.mom.e[e].comp;
-                    if (c < 3) ed[c] = ed[c] + A.mom.e[e].inc;
-                    else eo[c - 3] = eo[c - 3] + A.mom.e[e].inc;
-                }
+            apply_inject(lmom, nmom, A.mom, q, ed, eo);
             {
-                const float r = A.vc[q];
+                const float r = cur[2];
 #pragma unroll
                 for (int i = 0; i < 3; i++) { ed[i] = ed[i] * r; eo[i] = eo[i] * r; }
             }
@@ -256,7 +278,7 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
 #pragma unroll
                 for (int d = 0; d < 3; d++) inE = inE && cc[d] >= g.i1pml[d] && cc[d] <= g.i2pml[d] - 1;
                 if (inE) {
-                    const float y = A.yy[q];
+                    const float y = cur[3];
 #pragma unroll
                     for (int ic = 0; ic < 3; ic++) {
                         float W2[8];
@@ -371,42 +393,50 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
                     yc[t] = okc[t] ? A.dh2 * A.yy[g.idx(Jc, Kc, Lc)] : 0.f;
                     cb[t] = o;
                 }
+                // each component's four modes share the cell corner loads; the
+                // updates of f[ic] keep the reference's mode order
+#pragma unroll 1
+                for (int ic = 0; ic < 3; ic++) {
+                    float Hq[4][8];
 #pragma unroll
-                for (int iq = 0; iq < 4; iq++)
+                    for (int t = 0; t < 8; t++) {
+                        if (okc[t]) {
+                            const int o = cb[t];
+                            float Vc[8];
 #pragma unroll
-                    for (int ic = 0; ic < 3; ic++) {
-                        float H[8];
-#pragma unroll
-                        for (int t = 0; t < 8; t++) {
-                            float hv = 0.f;
-                            if (okc[t]) {
-                                const int o = cb[t];
-                                float Vc[8];
-#pragma unroll
-                                for (int m = 0; m < 8; m++) {
-                                    const int n = hg_corner(m);
-                                    const int dj = (n & 1) - (o & 1), dk = ((n >> 1) & 1) - ((o >> 1) & 1), dl = (n >> 2) - (o >> 2);
-                                    Vc[m] = NODE((l + dl + 3) % 3, 3 + ic, (tx + 1 + dj) + FNJ * (ty + 1 + dk));
-                                }
-                                hv = yc[t] * hg_sum(Vc, iq);
+                            for (int m = 0; m < 8; m++) {
+                                const int n = hg_corner(m);
+                                const int dj = (n & 1) - (o & 1), dk = ((n >> 1) & 1) - ((o >> 1) & 1), dl = (n >> 2) - (o >> 2);
+                                Vc[m] = NODE((l + dl + 3) % 3, 3 + ic, (tx + 1 + dj) + FNJ * (ty + 1 + dk));
                             }
-                            H[t] = hv;
+#pragma unroll
+                            for (int iq = 0; iq < 4; iq++) Hq[iq][t] = yc[t] * hg_sum(Vc, iq);
+                        } else {
+#pragma unroll
+                            for (int iq = 0; iq < 4; iq++) Hq[iq][t] = 0.f;
                         }
-                        f[ic] = f[ic] - hg_sum(H, iq);
                     }
-            } else {
+                    float fi = f[0];
+                    if (ic == 1) fi = f[1];
+                    if (ic == 2) fi = f[2];
 #pragma unroll
-                for (int iq = 0; iq < 4; iq++)
-#pragma unroll
-                    for (int ic = 0; ic < 3; ic++) f[ic] = f[ic] - 0.f;
+                    for (int iq = 0; iq < 4; iq++) fi = fi - hg_sum(Hq[iq], iq);
+                    if (ic == 0) f[0] = fi;
+                    if (ic == 1) f[1] = fi;
+                    if (ic == 2) f[2] = fi;
+                }
             }
         }
-        for (int e = 0; e < A.force.n; e++)
-            if (A.force.e[e].idx == q) {
-                const int c = A.force.e[e].comp;
-                f[c] = f[c] + A.force.e[e].inc;
-            }
-        const float m = A.mr[q];
+        {
+            const Inject* E = nfrc >= 0 ? lfrc : A.force.e;
+            const int n = nfrc >= 0 ? nfrc : A.force.n;
+            for (int e = 0; e < n; e++)
+                if (E[e].idx == q) {
+                    const int c = E[e].comp;
+                    f[c] = f[c] + E[e].inc;
+                }
+        }
+        const float m = cur[4];
 #pragma unroll
         for (int i = 0; i < 3; i++) f[i] = f[i] * m;
         const float v0 = NODE(sn, 3, ni0), v1 = NODE(sn, 4, ni0), v2 = NODE(sn, 5, ni0);
@@ -435,17 +465,23 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
     store(L0 % 3);
     fetch(L0 + 1);
     store((L0 + 1) % 3);
+    stat_load(L0 - 1, cur);
     __syncthreads();
     cells(L0 - 1);
+    stat_load(L0, cur);
     fetch(L0 + 2);
     for (int l = L0; l <= L1; l++) {
         __syncthreads();
         cells(l);
+        float nxt[5];
+        stat_load(l + 1, nxt);
         __syncthreads();
         nodes(l);
         __syncthreads();
         store((l + 2) % 3);
         fetch(l + 3);
+#pragma unroll
+        for (int i = 0; i < 5; i++) cur[i] = nxt[i];
     }
     if (A.stats) {
         bmax(A.red + 0, st_a);

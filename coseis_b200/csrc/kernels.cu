@@ -10,6 +10,7 @@
 //                                     hook intervenes, :240-262 (f*mr, |a|)
 //   k_mass    acceleration.f90:240-251
 //   BC / injection helpers            boundary_cond.f90, field_io '.' ops
+#include "inject.cuh"
 #include "sord.cuh"
 #include "stencil.cuh"
 
@@ -114,6 +115,15 @@ __global__ void __launch_bounds__(256) k_stress(StressArgs A) {
     int k = g.i1cell[1] + blockIdx.y * blockDim.y + threadIdx.y;
     int l = g.i1cell[2] + blockIdx.z * blockDim.z + threadIdx.z;
     float wn = 0.f;
+    __shared__ Inject lpot[kLocalInject], lmom[kLocalInject];
+    __shared__ int lcnt[2];
+    {
+        const int bj = g.i1cell[0] + blockIdx.x * blockDim.x, bk = g.i1cell[1] + blockIdx.y * blockDim.y,
+                  bl = g.i1cell[2] + blockIdx.z * blockDim.z;
+        gather_inject(A.pot, lpot, &lcnt[0], g, bj, bj + blockDim.x - 1, bk, bk + blockDim.y - 1, bl, bl + blockDim.z - 1);
+        gather_inject(A.mom, lmom, &lcnt[1], g, bj, bj + blockDim.x - 1, bk, bk + blockDim.y - 1, bl, bl + blockDim.z - 1);
+        __syncthreads();
+    }
     bool active = j <= g.i2cell[0] && k <= g.i2cell[1] && l <= g.i2cell[2];
     if (active) {
         const long long q = g.idx(j, k, l);
@@ -191,24 +201,14 @@ __global__ void __launch_bounds__(256) k_stress(StressArgs A) {
             }
         }
         // potency ops / finite source (stress.f90:288-296)
-        for (int e = 0; e < A.pot.n; e++)
-            if (A.pot.e[e].idx == q) {
-                int c = A.pot.e[e].comp;
-                if (c < 3) ed[c] = ed[c] + A.pot.e[e].inc;
-                else eo[c - 3] = eo[c - 3] + A.pot.e[e].inc;
-            }
+        apply_inject(lpot, lcnt[0], A.pot, q, ed, eo);
         if (A.hooke) {
             // Hooke's law (stress.f90:310-330)
             const float lm = A.lam[q], m2 = 2.0f * A.mu[q];
             const float s1 = lm * (ed[0] + ed[1] + ed[2]);
 #pragma unroll
             for (int i = 0; i < 3; i++) { ed[i] = m2 * ed[i] + s1; eo[i] = m2 * eo[i]; }
-            for (int e = 0; e < A.mom.n; e++)
-                if (A.mom.e[e].idx == q) {
-                    int c = A.mom.e[e].comp;
-                    if (c < 3) ed[c] = ed[c] + A.mom.e[e].inc;
-                    else eo[c - 3] = eo[c - 3] + A.mom.e[e].inc;
-                }
+            apply_inject(lmom, lcnt[1], A.mom, q, ed, eo);
             // stress = moment / volume (stress.f90:344-355)
             const float r = A.vc[q];
 #pragma unroll
