@@ -236,7 +236,7 @@ bool Solver::fusable(int n) const {
     return true;
 }
 
-void Solver::step() {
+void Solver::step(bool last_in_call) {
     it++;
     for (auto& t : timers) t = 0;
     long long t_step = clock_us();
@@ -268,7 +268,9 @@ void Solver::step() {
     if (prm.source == "force") finite_source_entries(*this, frc);
     tensor_point_ops(*this, kPot, pot);
     tensor_point_ops(*this, kMom, mom);
-    const bool fold = it < nt && fusable(it + 1);
+    // never fold across the end of a sord_step call: the state it leaves is
+    // the state after its last step
+    const bool fold = !last_in_call && it < nt && fusable(it + 1);
     const bool write_a = any_pass(*this, kAcc, 3, '>') || field_active(*this, "am2", '>') || it == nt;
     InjectList lp = upload(*this, 0, pot), lm = upload(*this, 1, mom), lf = upload(*this, 2, frc);
     launch_fused(*this, lp, lm, lf, fold, write_a, st);
@@ -575,7 +577,7 @@ int sord_step(sord_handle* h, int nsteps) {
         SORD_CUDA(cudaSetDevice(s.device));
         if (nsteps < 0 || s.it + nsteps > s.nt) throw SordError(SORD_E_STATE, "step past nt");
         SORD_CUDA(cudaEventRecord(s.ev0, s.stream));
-        for (int i = 0; i < nsteps; i++) s.step();
+        for (int i = 0; i < nsteps; i++) s.step(i == nsteps - 1);
         SORD_CUDA(cudaEventRecord(s.ev1, s.stream));
         SORD_CUDA(cudaEventSynchronize(s.ev1));
         float ms = 0;

@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
 
     // per-plane statics of this thread's cell (lam, mu, 1/V, yy) and node
     // (mass ratio), loaded one plane ahead of their use
-    float cur[5];
+    float cur[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
     auto stat_load = [&](int l, float* o) {
         const bool cv = cellcol && l >= g.i1cell[2] && l <= g.i2cell[2];
         const long long qc = cv ? g.idx(J, K, l) : 0;

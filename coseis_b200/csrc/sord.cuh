@@ -276,7 +276,7 @@ struct Solver {
     long long clock_us() const;
     std::string path(const std::string& f) const;
 
-    void step();
+    void step(bool last_in_call = true);
     void step_general(bool st);
     bool fusable(int step) const;
     void stats();
