@@ -28,8 +28,7 @@
 //        [--nt-limit K]  -> writes the same output files as sord.x.
 //
 // Decisions where the reference is undefined or broken are the same ones the
-// CUDA solver makes; each is listed in DESIGN.md ("Reference defects").  In
-// short: the PML bounds from sord.in are converted so that exactly npml node
+// CUDA solver makes: the PML bounds from sord.in are converted so that exactly npml node
 // and cell layers are damped on PML faces and none elsewhere (the reference
 // reads its coefficient arrays one past the end and damps the boundary
 // layer of non-PML faces); fault normals and the hypocentral radius use the
