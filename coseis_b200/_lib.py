@@ -15,6 +15,7 @@ SYMBOLS = [
     'sord_get_field', 'sord_info', 'sord_stats', 'sord_last_step_ms',
     'sord_kernel_launches', 'sord_set_profiling', 'sord_kernel_times',
     'sord_last_error', 'sord_error_string', 'sord_destroy',
+    'sord_vector_max_noalloc',
 ]
 
 _lib = None
@@ -64,8 +65,22 @@ def load():
     lib.sord_error_string.restype = ctypes.c_char_p
     lib.sord_destroy.argtypes = [P]
     lib.sord_destroy.restype = None
+    IP = ctypes.POINTER(ctypes.c_int)
+    lib.sord_vector_max_noalloc.argtypes = [P, P, P, IP, IP, IP, P, P]
+    lib.sord_vector_max_noalloc.restype = ctypes.c_int
     _lib = lib
     return lib
+
+
+def vector_max_noalloc(w0, w1, w2, nm, i1, i2, out, stream=None):
+    """Max of w0^2 + w1^2 + w2^2 over [i1, i2] of device fields (raw device
+    pointers as ints, j fastest, extents nm) into the device float ``out``,
+    without allocating device memory (include/sordgpu.h)."""
+    lib = load()
+    a = (ctypes.c_int * 3)(*nm)
+    b = (ctypes.c_int * 3)(*i1)
+    c = (ctypes.c_int * 3)(*i2)
+    _check(lib.sord_vector_max_noalloc(w0, w1, w2, a, b, c, out, stream))
 
 
 def _check(rc, handle=None):

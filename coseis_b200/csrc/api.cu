@@ -530,6 +530,10 @@ struct sord_handle {
 
 static std::string g_create_error;
 
+namespace sordgpu {
+void set_global_error(const char* msg) { g_create_error = msg; }
+}  // namespace sordgpu
+
 static int fail(sord_handle* h, const std::exception& e) {
     const SordError* se = dynamic_cast<const SordError*>(&e);
     int code = se ? se->code : SORD_E_PARAM;

@@ -86,6 +86,26 @@ double sord_last_step_ms(const sord_handle* h);
 int sord_set_profiling(sord_handle* h, int on);
 int sord_kernel_times(sord_handle* h, double* ms, long long* count, int n);
 
+/* Maximum of w0^2 + w1^2 + w2^2 over the region [i1, i2] (1-based,
+ * inclusive) of a caller-owned FP32 device field of extents nm[3] (j
+ * fastest) -- the statistic behind the |v|, |u|, |a| maxima of
+ * sord_stats -- written to the device float `out`, enqueued on CUDA stream
+ * `stream` (NULL for the default stream) on the current device.
+ *
+ * No counterpart in the reference.  It allocates nothing (no cudaMalloc,
+ * cudaFree or allocating library call), for callers that cannot allocate
+ * device memory where they need the reduction (a frozen or exhausted memory
+ * pool, allocation-free sections of a host framework).  Its partial results
+ * live in a 4 KiB file-scope device array (1024 block maxima) that every GPU
+ * loading this library keeps until the process exits; regions of 2^31
+ * elements or more are rejected with SORD_E_PARAM.  All calls share that
+ * array, so calls that overlap on the GPU race and must be serialised by the
+ * caller.  The first call on each device looks up the array's address with
+ * that device current; make it before any stream capture.  On error,
+ * sord_last_error(NULL) gives the message. */
+int sord_vector_max_noalloc(const float* w0, const float* w1, const float* w2, const int* nm, const int* i1,
+                            const int* i2, float* out, void* stream);
+
 /* Number of kernels this library launched since the handle was created. */
 long long sord_kernel_launches(const sord_handle* h);
 
