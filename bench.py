@@ -300,12 +300,20 @@ def dist_init():
 
 
 def reduce_max(pg, v):
+    """Maximum of v over all ranks (the slowest rank's device time)."""
     if pg is None:
         return v
     import torch
-    t = torch.tensor([v], dtype=torch.float64, device='cuda')
+    dev = 'cuda' if pg.get_backend() == 'nccl' else 'cpu'
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_rate(ws, nodes, steps, ms_max):
+    """Whole-job node-updates/s: every rank advances its own replica of
+    `nodes` nodes by `steps` steps; the job takes the slowest rank's time."""
+    return ws * nodes * steps / (ms_max / 1e3)
 
 
 def barrier(pg):
@@ -357,7 +365,7 @@ def run_ours(args):
         shutil.rmtree(work, ignore_errors=True)
     if rank != 0:
         return
-    value = ws * nodes * args.steps / (ms_max / 1e3)
+    value = job_rate(ws, nodes, args.steps, ms_max)
     hbm, src = peaks()
     alg = algorithmic_bytes_per_node(shape)
     step_ms = sum(kt[k][0] for k in ('time', 'stress', 'accel', 'mass')) / prof_steps
