@@ -142,13 +142,14 @@ class Solver(object):
         _check(load().sord_set_profiling(self._h, 1 if on else 0), self._h)
 
     def kernel_times(self):
-        """{class: (ms, launches)} for time, stress, accel, mass, fault, io, other."""
-        ms = (ctypes.c_double * 7)()
-        cnt = (ctypes.c_longlong * 7)()
-        n = load().sord_kernel_times(self._h, ms, cnt, 7)
+        """{class: (ms, launches)} for time, stress, accel, mass, fault, io,
+        other and step (the fused whole-step kernel)."""
+        ms = (ctypes.c_double * 8)()
+        cnt = (ctypes.c_longlong * 8)()
+        n = load().sord_kernel_times(self._h, ms, cnt, 8)
         if n < 0:
             _check(n, self._h)
-        names = ['time', 'stress', 'accel', 'mass', 'fault', 'io', 'other']
+        names = ['time', 'stress', 'accel', 'mass', 'fault', 'io', 'other', 'step']
         return {names[i]: (ms[i], cnt[i]) for i in range(n)}
 
     def kernel_launches(self):

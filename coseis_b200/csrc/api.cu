@@ -687,7 +687,7 @@ int sord_kernel_times(sord_handle* h, double* ms, long long* count, int n) {
     } catch (const std::exception& e) {
         return fail(h, e);
     }
-    int m = n < 7 ? n : 7;
+    int m = n < 8 ? n : 8;
     for (int i = 0; i < m; i++) {
         if (ms) ms[i] = h->s.kernel_ms[i];
         if (count) count[i] = h->s.kernel_n[i];

@@ -540,13 +540,13 @@ void launch_fused(Solver& s, const InjectList& pot, const InjectList& mom, const
     nseg = (nl + A.segl - 1) / A.segl;
     dim3 grid(bx, by, nseg);
     cudaEvent_t e0 = nullptr;
-    s.prof_begin(KC_STRESS, &e0);
+    s.prof_begin(KC_FUSED, &e0);
     if (s.geom == GEOM_RECT) launch_geom<GEOM_RECT>(s, A, grid);
     else if (s.geom == GEOM_TERRAIN) launch_geom<GEOM_TERRAIN>(s, A, grid);
     else launch_geom<GEOM_GENERAL>(s, A, grid);
     s.launches++;
     SORD_CUDA(cudaGetLastError());
-    s.prof_end(KC_STRESS, e0);
+    s.prof_end(KC_FUSED, e0);
     if (fold) {
         for (int i = 0; i < 3; i++) {
             std::swap(d.v[i], d.vb[i]);

@@ -178,7 +178,7 @@ enum FaultArr {
 struct Solver;
 
 // kernel classes for sord_kernel_times
-enum { KC_TIME = 0, KC_STRESS = 1, KC_ACCEL = 2, KC_MASS = 3, KC_FAULT = 4, KC_IO = 5, KC_OTHER = 6 };
+enum { KC_TIME = 0, KC_STRESS = 1, KC_ACCEL = 2, KC_MASS = 3, KC_FAULT = 4, KC_IO = 5, KC_OTHER = 6, KC_FUSED = 7 };
 
 // kernels.cu entry points
 void launch_time_update(Solver& s, bool stats);

@@ -78,8 +78,9 @@ double sord_last_step_ms(const sord_handle* h);
 /* Per-kernel device timing for performance reports.  With profiling on,
  * CUDA events are recorded around each step kernel on the handle's stream
  * and accumulated per class: 0 time update, 1 stress, 2 acceleration,
- * 3 mass, 4 fault, 5 field I/O, 6 other.  Turning it on or off resets the
- * sums.  sord_kernel_times writes min(n, 7) totals (ms) and launch counts
+ * 3 mass, 4 fault, 5 field I/O, 6 other, 7 fused step kernel (one whole
+ * time step).  Turning it on or off resets the
+ * sums.  sord_kernel_times writes min(n, 8) totals (ms) and launch counts
  * and returns that number.  No reference counterpart (the reference writes
  * host timers to prof-*.bin, statistics.f90:116-129; those files are
  * written here too). */
