@@ -273,7 +273,7 @@ void Solver::step(bool last_in_call) {
     const bool fold = !last_in_call && it < nt && fusable(it + 1);
     const bool write_a = any_pass(*this, kAcc, 3, '>') || field_active(*this, "am2", '>') || it == nt;
     InjectList lp = upload(*this, 0, pot), lm = upload(*this, 1, mom), lf = upload(*this, 2, frc);
-    launch_fused(*this, lp, lm, lf, fold, write_a, st);
+    launch_fused(*this, lp, lm, lf, pot, mom, frc, fold, write_a, st);
     folded = fold;
     for (int i = 0; i < 3; i++) io("<>", kAcc[i], vol(*this, d.w1n[i]));
     io(">", "am2", vol(*this, d.s1));
@@ -509,6 +509,7 @@ void Solver::destroy() {
     fr(d.x1d); fr(d.y1d);
     for (auto& io : ops) fr(io.dbuf);
     probes_free(this);
+    fused_free(*this);
     for (auto& p : prof_ev) { cudaEventDestroy(p.second.first); cudaEventDestroy(p.second.second); }
     prof_ev.clear();
     if (hinj) cudaFreeHost(hinj);

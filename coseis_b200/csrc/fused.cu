@@ -11,13 +11,20 @@
 //                v' = v + dt a, u' = u + dt v' (time_integration.f90:27-41)
 //
 // Each block owns a 31 x 7 column of output nodes (32 x 8 cells including
-// the -1 halo) and streams along l: node planes sit in a 3-plane shared
-// ring (u, v, gam, coordinates), cell planes in a 2-plane ring (stress,
-// hourglass values, divergence brackets), and plane l+3 is prefetched into
-// registers while planes l-1..l+1 are being used.  Cells on tile borders are
-// computed by both neighbours (from identical inputs, so identically); the
-// owner writes the PML g memory, which is double-buffered like v and u so
-// no block reads a value another block has already advanced.
+// the -1 halo) and streams along l.  Node planes are staged raw (u, v, gam,
+// coordinates) by cp.async into shared memory one plane ahead, then turned
+// into a 3-plane ring of the per-node values the cells need: w = u + gam v,
+// the hourglass input hg1 u + dt hg2 v, and the coordinates.  Cell planes
+// (stress, hourglass values, divergence brackets) sit in a 2-plane ring.
+// Two barriers per plane.  Cells on tile borders are computed by both
+// neighbours (from identical inputs, so identically); the owner writes the
+// PML g memory, which is double-buffered like v and u so no block reads a
+// value another block has already advanced.
+//
+// Planes of blocks whose whole tile lies outside the PML, with no point
+// source in the block, run a fast path with the PML, boundary and injection
+// branches compiled out; the arithmetic of both paths is the same, so a
+// cell computed by either is bit-identical.
 //
 // Support-operator brackets: rectilinear meshes use the per-direction
 // constants verified at setup; terrain meshes (x = x(j), y = y(k)) compute
@@ -25,7 +32,14 @@
 // general meshes compute all three.  Each cell's brackets are evaluated
 // once and shared by the cell's gradient and its eight corner nodes'
 // divergence (stencil.cuh: cell_cn_brackets).
+#include <algorithm>
+#include <cstring>
+#include <type_traits>
+#include <utility>
+#include <vector>
+
 #include "inject.cuh"
+#include "pair.cuh"
 #include "sord.cuh"
 #include "stencil.cuh"
 
@@ -41,12 +55,13 @@ constexpr int NTH = FJ * FK;
 template <int GEOM>
 struct Lay {
     static constexpr int NCOORD = GEOM == GEOM_RECT ? 0 : GEOM == GEOM_TERRAIN ? 1 : 3;
-    static constexpr int PRE = 7 + NCOORD;    // prefetched: u(3) v(3) gam coords
-    static constexpr int NODEF = 9 + NCOORD;  // shared: u(3) v(3) w = u + gam v (3) coords
-    static constexpr int CO = 9;              // first coordinate field
+    static constexpr int RAWF = 7 + NCOORD;   // staged plane: u(3) v(3) gam coords
+    static constexpr int NODEF = 6 + NCOORD;  // ring: w = u + gam v (3), hg1 u + dt hg2 v (3), coords
+    static constexpr int HG = 3;              // first hourglass-input field
+    static constexpr int CO = 6;              // first coordinate field
     static constexpr int NDIR = GEOM == GEOM_RECT ? 0 : GEOM == GEOM_TERRAIN ? 2 : 3;
     static constexpr int CELLF = 6 + 12 + 8 * NDIR;  // stress, hourglass, divergence brackets
-    static constexpr size_t bytes = sizeof(float) * (size_t)(3 * NPL * NODEF + 2 * NCL * CELLF);
+    static constexpr size_t bytes = sizeof(float) * (size_t)(NPL * RAWF + 3 * NPL * NODEF + 2 * NCL * CELLF);
 };
 
 __device__ __forceinline__ void bmax(unsigned* dst, float v) {
@@ -75,19 +90,42 @@ __device__ __forceinline__ long long slab_idx(const Geom& g, int axis, int t, in
     return a0 + e0 * (a1 + e1 * a2) + (long long)ic * e0 * e1 * e2;
 }
 
-template <int GEOM>
+// 4-byte asynchronous global -> shared copy (no register staging).
+__device__ __forceinline__ void cp_async4(float* smem, const float* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// FASTK: interior tile columns and planes (A.bx0, A.by0, A.lf0..A.lf1), fast
+// path only; otherwise the work items A.items, general path only.
+template <int GEOM, bool FASTK>
 __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(StepArgs A) {
     using L = Lay<GEOM>;
     extern __shared__ float sm[];
-    float* sN = sm;                          // [3 slots][NODEF][NPL]
-    float* sC = sm + 3 * L::NODEF * NPL;     // [2 slots][CELLF][NCL]
+    float* sR = sm;                          // [RAWF][NPL] staged plane
+    float* sN = sR + L::RAWF * NPL;          // [3 slots][NODEF][NPL]
+    float* sC = sN + 3 * L::NODEF * NPL;     // [2 slots][CELLF][NCL]
+#define RAW(f, i) sR[(f) * NPL + (i)]
 #define NODE(slot, f, i) sN[((slot) * L::NODEF + (f)) * NPL + (i)]
 #define CELL(slot, f, i) sC[((slot) * L::CELLF + (f)) * NCL + (i)]
     const Geom& g = A.g;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + FJ * ty;
-    const int j0 = g.i1node[0] + blockIdx.x * FOJ, k0 = g.i1node[1] + blockIdx.y * FOK;
-    const int L0 = g.i1node[2] + blockIdx.z * A.segl;
-    const int L1 = min(L0 + A.segl - 1, g.i2node[2]);
+    int bx, by, L0, L1;
+    if (FASTK) {
+        bx = A.bx0 + blockIdx.x;
+        by = A.by0 + blockIdx.y;
+        L0 = A.lf0 + blockIdx.z * A.segl;
+        L1 = min(L0 + A.segl - 1, A.lf1);
+    } else {
+        const int4 it = A.items[blockIdx.x];
+        bx = it.x;
+        by = it.y;
+        L0 = it.z;
+        L1 = it.w;
+    }
+    const int j0 = g.i1node[0] + bx * FOJ, k0 = g.i1node[1] + by * FOK;
     const int J = j0 - 1 + tx, K = k0 - 1 + ty;      // this thread's cell column
     const int jn = j0 + tx, kn = k0 + ty;            // this thread's node column
     const bool outcol = tx < FOJ && ty < FOK && jn <= g.i2node[0] && kn <= g.i2node[1];
@@ -95,50 +133,74 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
     const bool owncol = J >= j0 && K >= k0;
     const float h = g.h, dt = g.dt;
     float st_a = 0.f, st_v = 0.f, st_u = 0.f, st_w = 0.f;
+    // terrain meshes: this thread's cell column's x (j, j+1) and y (k, k+1)
+    float txa = 0.f, txb = 0.f, tya = 0.f, tyb = 0.f;
+    if (GEOM == GEOM_TERRAIN && cellcol) {
+        txa = A.x1d[J - 1];
+        txb = A.x1d[J];
+        tya = A.y1d[K - 1];
+        tyb = A.y1d[K];
+    }
 
     // point injections that fall inside this block (cells / nodes it computes)
     __shared__ Inject lpot[kLocalInject], lmom[kLocalInject], lfrc[kLocalInject];
     __shared__ int lcnt[3];
-    gather_inject(A.pot, lpot, &lcnt[0], g, j0 - 1, j0 + FOJ - 1, k0 - 1, k0 + FOK - 1, L0 - 1, L1);
-    gather_inject(A.mom, lmom, &lcnt[1], g, j0 - 1, j0 + FOJ - 1, k0 - 1, k0 + FOK - 1, L0 - 1, L1);
-    gather_inject(A.force, lfrc, &lcnt[2], g, j0, j0 + FOJ - 1, k0, k0 + FOK - 1, L0, L1);
+    // A fast-kernel block whose (j, k) box holds a point source of this step
+    // leaves that column to the general kernel (the host lists it there).
+    const int gl1 = FASTK ? 0 : L0 - 1, gl2 = FASTK ? g.nm[2] + 1 : L1;
+    gather_inject(A.pot, lpot, &lcnt[0], g, j0 - 1, j0 + FOJ - 1, k0 - 1, k0 + FOK - 1, gl1, gl2);
+    gather_inject(A.mom, lmom, &lcnt[1], g, j0 - 1, j0 + FOJ - 1, k0 - 1, k0 + FOK - 1, gl1, gl2);
+    gather_inject(A.force, lfrc, &lcnt[2], g, j0, j0 + FOJ - 1, k0, k0 + FOK - 1, FASTK ? gl1 : L0, gl2);
     __syncthreads();
     const int npot = lcnt[0], nmom = lcnt[1], nfrc = lcnt[2];
+    if (FASTK && (npot != 0 || nmom != 0 || nfrc != 0)) return;
 
     // ---------------------------------------------------------------- loads
-    float pre[2][L::PRE];
+    // stage node plane l (u, v, gam, coordinates) into sR asynchronously
     auto fetch = [&](int l) {
 #pragma unroll
         for (int r = 0; r < 2; r++) {
             const int n = tid + r * NTH;
-            const int nj = n % FNJ, nk = n / FNJ;
-            const int j = j0 - 1 + nj, k = k0 - 1 + nk;
-            const bool ok = n < NPL && j <= g.nm[0] && k <= g.nm[1] && l >= 1 && l <= g.nm[2];
-            const long long q = ok ? g.idx(j, k, l) : 0;
+            if (n < NPL) {
+                const int nj = n % FNJ, nk = n / FNJ;
+                const int j = j0 - 1 + nj, k = k0 - 1 + nk;
+                const bool ok = j <= g.nm[0] && k <= g.nm[1] && l >= 1 && l <= g.nm[2];
+                if (ok) {
+                    const long long q = g.idx(j, k, l);
 #pragma unroll
-            for (int c = 0; c < 3; c++) {
-                pre[r][c] = ok ? A.uin[c][q] : 0.f;
-                pre[r][3 + c] = ok ? A.vin[c][q] : 0.f;
+                    for (int c = 0; c < 3; c++) {
+                        cp_async4(&RAW(c, n), A.uin[c] + q);
+                        cp_async4(&RAW(3 + c, n), A.vin[c] + q);
+                    }
+                    cp_async4(&RAW(6, n), A.gam + q);
+                    if (GEOM == GEOM_TERRAIN) cp_async4(&RAW(7, n), A.x[2] + q);
+                    if (GEOM == GEOM_GENERAL)
+#pragma unroll
+                        for (int c = 0; c < 3; c++) cp_async4(&RAW(7 + c, n), A.x[c] + q);
+                } else {
+#pragma unroll
+                    for (int f = 0; f < L::RAWF; f++) RAW(f, n) = 0.f;
+                }
             }
-            pre[r][6] = ok ? A.gam[q] : 0.f;
-            if (GEOM == GEOM_TERRAIN) pre[r][7] = ok ? A.x[2][q] : 0.f;
-            if (GEOM == GEOM_GENERAL)
-#pragma unroll
-                for (int c = 0; c < 3; c++) pre[r][7 + c] = ok ? A.x[c][q] : 0.f;
         }
+        cp_async_commit();
     };
+    // staged plane -> ring slot: w1 = u + gam * v (time_integration.f90:36)
+    // and the hourglass input hg1 u + dt hg2 v (acceleration.f90:141)
     auto store = [&](int slot) {
 #pragma unroll
         for (int r = 0; r < 2; r++) {
             const int n = tid + r * NTH;
             if (n < NPL) {
+                const float gm = RAW(6, n);
 #pragma unroll
-                for (int f = 0; f < 6; f++) NODE(slot, f, n) = pre[r][f];
-                // w1 = u + gam * v (time_integration.f90:36)
+                for (int c = 0; c < 3; c++) {
+                    const float u = RAW(c, n), v = RAW(3 + c, n);
+                    NODE(slot, c, n) = u + gm * v;
+                    NODE(slot, L::HG + c, n) = A.hg1 * u + A.dh2 * v;
+                }
 #pragma unroll
-                for (int c = 0; c < 3; c++) NODE(slot, 6 + c, n) = pre[r][c] + pre[r][6] * pre[r][3 + c];
-#pragma unroll
-                for (int f = 0; f < L::NCOORD; f++) NODE(slot, L::CO + f, n) = pre[r][7 + f];
+                for (int f = 0; f < L::NCOORD; f++) NODE(slot, L::CO + f, n) = RAW(7 + f, n);
             }
         }
     };
@@ -156,11 +218,23 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
         const bool nv = outcol && l >= g.i1node[2] && l <= g.i2node[2];
         o[4] = nv ? A.mr[g.idx(jn, kn, l)] : 0.f;
     };
+    // this thread's node u, v (for the update and statistics), one plane ahead
+    float uv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    auto uv_load = [&](int l, float* o) {
+        const bool nv = outcol && l >= g.i1node[2] && l <= g.i2node[2];
+        const long long q = nv ? g.idx(jn, kn, l) : 0;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            o[c] = nv ? A.uin[c][q] : 0.f;
+            o[3 + c] = nv ? A.vin[c][q] : 0.f;
+        }
+    };
 
     // ---------------------------------------------------------------- cell phase
-    auto cells = [&](int l) {
+    auto cells = [&](int l, auto fast_tag) {
+        constexpr bool F = decltype(fast_tag)::value;
         const int cs = l & 1;
-        const bool valid = cellcol && l >= g.i1cell[2] && l <= g.i2cell[2];
+        const bool valid = F || (cellcol && l >= g.i1cell[2] && l <= g.i2cell[2]);
         float ed[3] = {0.f, 0.f, 0.f}, eo[3] = {0.f, 0.f, 0.f};
         float he[12];
 #pragma unroll
@@ -184,7 +258,7 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
             } else {
                 float X[3][8];
                 if (GEOM == GEOM_TERRAIN) {
-                    const float xa = A.x1d[J - 1], xb = A.x1d[J], ya = A.y1d[K - 1], yb = A.y1d[K];
+                    const float xa = txa, xb = txb, ya = tya, yb = tyb;
 #pragma unroll
                     for (int n = 0; n < 8; n++) {
                         X[0][n] = (n & 1) ? xb : xa;
@@ -206,65 +280,111 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
 #pragma unroll
                     for (int t = 0; t < 8; t++) B[2][t] = A.br.bnc[2][t];
             }
-            // region of the cell (stress.f90:141-248)
-            bool nearS[3], farS[3], anyS = false;
-            const int cc[3] = {J, K, l};
-#pragma unroll
-            for (int d = 0; d < 3; d++) {
-                nearS[d] = cc[d] <= g.i1pml[d];
-                farS[d] = cc[d] >= g.i2pml[d] - 1;
-                anyS = anyS || nearS[d] || farS[d];
-            }
             const bool own = owncol && l >= L0;
+            if constexpr (F) {
+                // strain of an interior cell: gradients of w = u + gam v
 #pragma unroll
-            for (int ic = 0; ic < 3; ic++) {
-                float W[8], U[8], V[8];
+                for (int ic = 0; ic < 3; ic++) {
+                    float W[8];
 #pragma unroll
-                for (int t = 0; t < 8; t++) {
-                    const int n = term_corner(t);
-                    const float uu = NODE(ns[n], ic, ni[n]), vv = NODE(ns[n], 3 + ic, ni[n]);
-                    U[t] = uu;
-                    V[t] = vv;
-                    W[t] = NODE(ns[n], 6 + ic, ni[n]);
-                }
-#pragma unroll
-                for (int iid = 0; iid < 3; iid++) {
-                    const int id = (ic + iid + 1) % 3;
-                    float s;
-                    if (nearS[id] || farS[id]) {
-                        const float raw = stencil8(V, B[id], h);
-                        s = raw;
-                        const int c = cc[id];
-                        if (nearS[id]) {
-                            const int p = c + g.nnoff[id];
-                            const long long gi = slab_idx(g, id, A.sl.tg[id], c - g.i1cell[id], J, K, l, ic);
-                            s = A.pmlc[3 * g.npml + p - 1] * raw + A.pmlc[2 * g.npml + p - 1] * A.sl.g[id][gi];
-                            if (own) A.gout[id][gi] = s;
-                        }
-                        if (farS[id]) {
-                            const int p = g.nn[id] - c - g.nnoff[id];
-                            const long long gi = slab_idx(g, id, A.sl.tg[3 + id], g.i2cell[id] - c, J, K, l, ic);
-                            s = A.pmlc[3 * g.npml + p - 1] * raw + A.pmlc[2 * g.npml + p - 1] * A.sl.g[3 + id][gi];
-                            if (own) A.gout[3 + id][gi] = s;
-                        }
-                    } else if (anyS) {
-                        s = stencil8(U, B[id], h);
-                    } else {
-                        s = stencil8(W, B[id], h);
+                    for (int t = 0; t < 8; t++) {
+                        const int n = term_corner(t);
+                        W[t] = NODE(ns[n], ic, ni[n]);
                     }
-                    if (ic == id) ed[ic] = s;
-                    else if (ic < id) eo[3 - ic - id] = 0.5f * s;
-                    else eo[3 - ic - id] = eo[3 - ic - id] + 0.5f * s;
+#pragma unroll
+                    for (int iid = 0; iid < 3; iid++) {
+                        const int id = (ic + iid + 1) % 3;
+                        const float s = stencil8(W, B[id], h);
+                        if (ic == id) ed[ic] = s;
+                        else if (ic < id) eo[3 - ic - id] = 0.5f * s;
+                        else eo[3 - ic - id] = eo[3 - ic - id] + 0.5f * s;
+                    }
                 }
+            } else {
+                // region of the cell (stress.f90:141-248)
+                bool nearS[3], farS[3], anyS = false;
+                const int cc[3] = {J, K, l};
+#pragma unroll
+                for (int d = 0; d < 3; d++) {
+                    nearS[d] = cc[d] <= g.i1pml[d];
+                    farS[d] = cc[d] >= g.i2pml[d] - 1;
+                    anyS = anyS || nearS[d] || farS[d];
+                }
+                // PML cells that are not elastic-hourglass cells carry the
+                // viscous hourglass values dt hg2 yy hourglass_nc(v) in the
+                // hourglass slots (acceleration.f90:164-183)
+                bool inEc = true;
+#pragma unroll
+                for (int d = 0; d < 3; d++) inEc = inEc && cc[d] >= g.i1pml[d] && cc[d] <= g.i2pml[d] - 1;
+                const bool visc = A.hourglass && A.hgvisc && anyS && !inEc;
+                const float yv = A.dh2 * cur[3];
+#pragma unroll
+                for (int ic = 0; ic < 3; ic++) {
+                    float W[8], U[8], V[8];
+#pragma unroll
+                    for (int t = 0; t < 8; t++) {
+                        const int n = term_corner(t);
+                        W[t] = NODE(ns[n], ic, ni[n]);
+                        U[t] = 0.f;
+                        V[t] = 0.f;
+                    }
+                    if (anyS) {
+#pragma unroll
+                        for (int t = 0; t < 8; t++) {
+                            const int n = term_corner(t);
+                            const long long qn = g.idx(J + (n & 1), K + ((n >> 1) & 1), l + (n >> 2));
+                            U[t] = A.uin[ic][qn];
+                            V[t] = A.vin[ic][qn];
+                        }
+                    }
+                    if (visc) {
+                        float Vc[8], Vh[8];
+#pragma unroll
+                        for (int t = 0; t < 8; t++) Vc[term_corner(t)] = V[t];
+#pragma unroll
+                        for (int t = 0; t < 8; t++) Vh[t] = Vc[hg_corner(t)];
+#pragma unroll
+                        for (int iq = 0; iq < 4; iq++) he[3 * iq + ic] = yv * hg_sum(Vh, iq);
+                    }
+#pragma unroll
+                    for (int iid = 0; iid < 3; iid++) {
+                        const int id = (ic + iid + 1) % 3;
+                        float s;
+                        if (nearS[id] || farS[id]) {
+                            const float raw = stencil8(V, B[id], h);
+                            s = raw;
+                            const int c = cc[id];
+                            if (nearS[id]) {
+                                const int p = c + g.nnoff[id];
+                                const long long gi = slab_idx(g, id, A.sl.tg[id], c - g.i1cell[id], J, K, l, ic);
+                                s = A.pmlc[3 * g.npml + p - 1] * raw + A.pmlc[2 * g.npml + p - 1] * A.sl.g[id][gi];
+                                if (own) A.gout[id][gi] = s;
+                            }
+                            if (farS[id]) {
+                                const int p = g.nn[id] - c - g.nnoff[id];
+                                const long long gi = slab_idx(g, id, A.sl.tg[3 + id], g.i2cell[id] - c, J, K, l, ic);
+                                s = A.pmlc[3 * g.npml + p - 1] * raw + A.pmlc[2 * g.npml + p - 1] * A.sl.g[3 + id][gi];
+                                if (own) A.gout[3 + id][gi] = s;
+                            }
+                        } else if (anyS) {
+                            s = stencil8(U, B[id], h);
+                        } else {
+                            s = stencil8(W, B[id], h);
+                        }
+                        if (ic == id) ed[ic] = s;
+                        else if (ic < id) eo[3 - ic - id] = 0.5f * s;
+                        else eo[3 - ic - id] = eo[3 - ic - id] + 0.5f * s;
+                    }
+                }
+                apply_inject(lpot, npot, A.pot, q, ed, eo);
             }
-            apply_inject(lpot, npot, A.pot, q, ed, eo);
             {
                 const float lm = cur[0], m2 = 2.0f * cur[1];
-                const float s1 = lm * (ed[0] + ed[1] + ed[2]);
+                const float s1v = lm * (ed[0] + ed[1] + ed[2]);
 #pragma unroll
-                for (int i = 0; i < 3; i++) { ed[i] = m2 * ed[i] + s1; eo[i] = m2 * eo[i]; }
+                for (int i = 0; i < 3; i++) { ed[i] = m2 * ed[i] + s1v; eo[i] = m2 * eo[i]; }
             }
-            apply_inject(lmom, nmom, A.mom, q, ed, eo);
+            if constexpr (!F) apply_inject(lmom, nmom, A.mom, q, ed, eo);
             {
                 const float r = cur[2];
 #pragma unroll
@@ -275,8 +395,11 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
             // elastic hourglass cell values (acceleration.f90:141-156)
             if (A.hourglass) {
                 bool inE = true;
+                if constexpr (!F) {
+                    const int cc[3] = {J, K, l};
 #pragma unroll
-                for (int d = 0; d < 3; d++) inE = inE && cc[d] >= g.i1pml[d] && cc[d] <= g.i2pml[d] - 1;
+                    for (int d = 0; d < 3; d++) inE = inE && cc[d] >= g.i1pml[d] && cc[d] <= g.i2pml[d] - 1;
+                }
                 if (inE) {
                     const float y = cur[3];
 #pragma unroll
@@ -285,7 +408,7 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
 #pragma unroll
                         for (int t = 0; t < 8; t++) {
                             const int n = hg_corner(t);
-                            W2[t] = A.hg1 * NODE(ns[n], ic, ni[n]) + A.dh2 * NODE(ns[n], 3 + ic, ni[n]);
+                            W2[t] = NODE(ns[n], L::HG + ic, ni[n]);
                         }
 #pragma unroll
                         for (int iq = 0; iq < 4; iq++) he[3 * iq + ic] = hg_sum(W2, iq) * y;
@@ -308,12 +431,243 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
             for (int t = 0; t < 8; t++) CELL(cs, 18 + 8 * a + t, tid) = cnb[a][t];
     };
 
-    // ---------------------------------------------------------------- node phase
-    auto nodes = [&](int l) {
+    // ---------------------------------------------------------------- fast path
+    // Same arithmetic as cells() / nodes() for interior tiles, with the
+    // independent stencils evaluated two per packed instruction and every
+    // shared-memory operand at a constant offset from a per-plane base.
+    const float* const nbase = sN + (tx + FNJ * ty);
+    float* const cbase = sC + tid;
+    auto cells_fast = [&](int l) {
+        float* cw = cbase + (l & 1) * (L::CELLF * NCL);
+        if (l < g.i1cell[2] || l > g.i2cell[2]) {  // halo plane of a free surface
+#pragma unroll
+            for (int i = 0; i < L::CELLF; i++) cw[i * NCL] = 0.f;
+            return;
+        }
+        const float* p0 = nbase + (l % 3) * (L::NODEF * NPL);        // node plane l
+        const float* p1 = nbase + ((l + 1) % 3) * (L::NODEF * NPL);  // node plane l+1
+#define NC(n, f) (((n) >> 2) ? p1 : p0)[(f) * NPL + ((n) & 1) + FNJ * (((n) >> 1) & 1)]
+        const F2 h2 = f2(h);
+        float B[3][8];
+        float cnb[L::NDIR > 0 ? L::NDIR : 1][8];
+        if (GEOM == GEOM_RECT) {
+#pragma unroll
+            for (int a = 0; a < 3; a++)
+#pragma unroll
+                for (int t = 0; t < 8; t++) B[a][t] = A.br.bnc[a][t];
+        } else {
+            float X0[8], X1[8], X2[8];
+            if (GEOM == GEOM_TERRAIN) {
+                const float xa = txa, xb = txb, ya = tya, yb = tyb;
+#pragma unroll
+                for (int n = 0; n < 8; n++) {
+                    X0[n] = (n & 1) ? xb : xa;
+                    X1[n] = ((n >> 1) & 1) ? yb : ya;
+                    X2[n] = NC(n, L::CO);
+                }
+            } else {
+#pragma unroll
+                for (int n = 0; n < 8; n++) {
+                    X0[n] = NC(n, L::CO);
+                    X1[n] = NC(n, L::CO + 1);
+                    X2[n] = NC(n, L::CO + 2);
+                }
+            }
+            // directions 0 and 1 in the two lanes: (xb, xc) = (y, z) and (z, x)
+            F2 PB[8], PC[8], P[8], PN[8];
+#pragma unroll
+            for (int n = 0; n < 8; n++) {
+                PB[n] = f2(X1[n], X2[n]);
+                PC[n] = f2(X2[n], X0[n]);
+            }
+            brackets_nc_g<F2>(PB, PC, P);
+            cell_cn_brackets_g<F2>(PB, PC, P, PN, f2(0.0f));
+#pragma unroll
+            for (int t = 0; t < 8; t++) {
+                B[0][t] = P[t].x;
+                B[1][t] = P[t].y;
+                cnb[0][t] = PN[t].x;
+                cnb[1][t] = PN[t].y;
+            }
+            if (GEOM == GEOM_TERRAIN) {
+#pragma unroll
+                for (int t = 0; t < 8; t++) B[2][t] = A.br.bnc[2][t];
+            } else {
+                brackets_nc_g<float>(X0, X1, B[2]);
+                cell_cn_brackets_g<float>(X0, X1, B[2], cnb[L::NDIR - 1], 0.0f);
+            }
+        }
+        // strain: s[ic][id] = stencil8(w_ic, B[id]); (ic0, ic1) paired per
+        // iid, then ic2's first two directions paired and its last alone
+        float Wt[3][8];
+#pragma unroll
+        for (int ic = 0; ic < 3; ic++)
+#pragma unroll
+            for (int t = 0; t < 8; t++) Wt[ic][t] = NC(term_corner(t), ic);
+        float sg[3][3];
+        {
+            F2 W01[8];
+#pragma unroll
+            for (int t = 0; t < 8; t++) W01[t] = f2(Wt[0][t], Wt[1][t]);
+#pragma unroll
+            for (int iid = 0; iid < 3; iid++) {
+                const int ia = (0 + iid + 1) % 3, ib = (1 + iid + 1) % 3;
+                F2 Bp[8];
+#pragma unroll
+                for (int t = 0; t < 8; t++) Bp[t] = f2(B[ia][t], B[ib][t]);
+                const F2 r = stencil8<F2>(W01, Bp, h2);
+                sg[0][ia] = r.x;
+                sg[1][ib] = r.y;
+            }
+            F2 W22[8], Bp[8];
+#pragma unroll
+            for (int t = 0; t < 8; t++) {
+                W22[t] = f2(Wt[2][t]);
+                Bp[t] = f2(B[0][t], B[1][t]);
+            }
+            const F2 r = stencil8<F2>(W22, Bp, h2);
+            sg[2][0] = r.x;
+            sg[2][1] = r.y;
+            sg[2][2] = stencil8<float>(Wt[2], B[2], h);
+        }
+        float ed[3], eo[3];
+#pragma unroll
+        for (int i = 0; i < 3; i++) ed[i] = sg[i][i];
+        eo[0] = 0.5f * sg[1][2] + 0.5f * sg[2][1];
+        eo[1] = 0.5f * sg[0][2] + 0.5f * sg[2][0];
+        eo[2] = 0.5f * sg[0][1] + 0.5f * sg[1][0];
+        {
+            const float lm = cur[0], m2 = 2.0f * cur[1];
+            const float s1v = lm * (ed[0] + ed[1] + ed[2]);
+#pragma unroll
+            for (int i = 0; i < 3; i++) { ed[i] = m2 * ed[i] + s1v; eo[i] = m2 * eo[i]; }
+            const float r = cur[2];
+#pragma unroll
+            for (int i = 0; i < 3; i++) { ed[i] = ed[i] * r; eo[i] = eo[i] * r; }
+        }
+        if (A.stats && owncol && l >= L0)
+            st_w = fmaxn(st_w, (ed[0] * ed[0] + ed[1] * ed[1] + ed[2] * ed[2]) + 2.0f * (eo[0] * eo[0] + eo[1] * eo[1] + eo[2] * eo[2]));
+#pragma unroll
+        for (int i = 0; i < 3; i++) { cw[i * NCL] = ed[i]; cw[(3 + i) * NCL] = eo[i]; }
+        // elastic hourglass cell values, (ic0, ic1) paired
+        if (A.hourglass) {
+            const float y = cur[3];
+            F2 H01[8];
+            float H2[8];
+#pragma unroll
+            for (int t = 0; t < 8; t++) {
+                const int n = hg_corner(t);
+                H01[t] = f2(NC(n, L::HG), NC(n, L::HG + 1));
+                H2[t] = NC(n, L::HG + 2);
+            }
+#pragma unroll
+            for (int iq = 0; iq < 4; iq++) {
+                const F2 r = hg_sum<F2>(H01, iq) * f2(y);
+                cw[(6 + 3 * iq) * NCL] = r.x;
+                cw[(7 + 3 * iq) * NCL] = r.y;
+                cw[(8 + 3 * iq) * NCL] = hg_sum<float>(H2, iq) * y;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < 12; i++) cw[(6 + i) * NCL] = 0.f;
+        }
+#pragma unroll
+        for (int a = 0; a < L::NDIR; a++)
+#pragma unroll
+            for (int t = 0; t < 8; t++) cw[(18 + 8 * a + t) * NCL] = cnb[a][t];
+#undef NC
+    };
+
+    auto nodes_fast = [&](int l) {
         if (!outcol) return;
         const long long q = g.idx(jn, kn, l);
-        const int sn = l % 3;
-        const int ni0 = (tx + 1) + FNJ * (ty + 1);
+        const float* c0 = cbase + ((l - 1) & 1) * (L::CELLF * NCL);  // cell plane l-1
+        const float* c1 = cbase + (l & 1) * (L::CELLF * NCL);        // cell plane l
+        // cell of diff_cn term t: (j-1|j, k-1|k, l-1|l) = thread cell + (t&1, t>>2)
+#define CC(t, f) ((((t) >> 1) & 1) ? c1 : c0)[(f) * NCL + ((t) & 1) + FJ * ((t) >> 2)]
+        const F2 h2 = f2(h);
+        float Fc[6][8];
+#pragma unroll
+        for (int c = 0; c < 6; c++)
+#pragma unroll
+            for (int t = 0; t < 8; t++) Fc[c][t] = CC(t, c);
+        float Bc[3][8];
+#pragma unroll
+        for (int id = 0; id < 3; id++)
+#pragma unroll
+            for (int t = 0; t < 8; t++)
+                Bc[id][t] = (GEOM == GEOM_RECT || (GEOM == GEOM_TERRAIN && id == 2)) ? A.br.bcn[id][t]
+                                                                                     : CC(t, 18 + 8 * id + t);
+        // f[ic] = sum over iid of stencil8(sigma(ic, id), Bc[id]), id = (ic + iid) % 3
+        F2 f01;
+        float f2s;
+        {
+#pragma unroll
+            for (int iid = 0; iid < 3; iid++) {
+                const int ia = iid, ib = (1 + iid) % 3;
+                const int ca = 0 == ia ? 0 : 3 + (3 - 0 - ia), cb = 1 == ib ? 1 : 3 + (3 - 1 - ib);
+                F2 Fp[8], Bp[8];
+#pragma unroll
+                for (int t = 0; t < 8; t++) {
+                    Fp[t] = f2(Fc[ca][t], Fc[cb][t]);
+                    Bp[t] = f2(Bc[ia][t], Bc[ib][t]);
+                }
+                const F2 r = stencil8<F2>(Fp, Bp, h2);
+                f01 = iid == 0 ? r : f01 + r;
+            }
+            // ic 2: (id 2, id 0) paired, then id 1
+            F2 Fp[8], Bp[8];
+#pragma unroll
+            for (int t = 0; t < 8; t++) {
+                Fp[t] = f2(Fc[2][t], Fc[4][t]);
+                Bp[t] = f2(Bc[2][t], Bc[0][t]);
+            }
+            const F2 r = stencil8<F2>(Fp, Bp, h2);
+            f2s = r.x + r.y;
+            f2s = f2s + stencil8<float>(Fc[3], Bc[1], h);
+        }
+        if (A.hourglass) {
+#define CH(t, f) ((hg_corner(t) >> 2) ? c0 : c1)[(f) * NCL + (1 - (hg_corner(t) & 1)) + FJ * (1 - ((hg_corner(t) >> 1) & 1))]
+#pragma unroll
+            for (int iq = 0; iq < 4; iq++) {
+                F2 H01[8];
+                float H2[8];
+#pragma unroll
+                for (int t = 0; t < 8; t++) {
+                    H01[t] = f2(CH(t, 6 + 3 * iq), CH(t, 7 + 3 * iq));
+                    H2[t] = CH(t, 8 + 3 * iq);
+                }
+                f01 = f01 - hg_sum<F2>(H01, iq);
+                f2s = f2s - hg_sum<float>(H2, iq);
+            }
+#undef CH
+        }
+#undef CC
+        const float m = cur[4];
+        float f[3] = {f01.x * m, f01.y * m, f2s * m};
+        const float u0 = uv[0], u1 = uv[1], u2 = uv[2], v0 = uv[3], v1 = uv[4], v2 = uv[5];
+        if (A.stats) {
+            st_a = fmaxn(st_a, f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
+            st_v = fmaxn(st_v, v0 * v0 + v1 * v1 + v2 * v2);
+            st_u = fmaxn(st_u, u0 * u0 + u1 * u1 + u2 * u2);
+        }
+        if (A.aout[0])
+#pragma unroll
+            for (int i = 0; i < 3; i++) A.aout[i][q] = f[i];
+        if (A.fold) {
+            // leapfrog update of the next step (time_integration.f90:32-35)
+            float a, b;
+            a = v0 + dt * f[0]; b = u0 + dt * a; A.vout[0][q] = a; A.uout[0][q] = b;
+            a = v1 + dt * f[1]; b = u1 + dt * a; A.vout[1][q] = a; A.uout[1][q] = b;
+            a = v2 + dt * f[2]; b = u2 + dt * a; A.vout[2][q] = a; A.uout[2][q] = b;
+        }
+    };
+
+    // ---------------------------------------------------------------- node phase
+    auto nodes = [&](int l, auto fast_tag) {
+        constexpr bool F = decltype(fast_tag)::value;
+        if (!outcol) return;
+        const long long q = g.idx(jn, kn, l);
         // cells of diff_cn term t: (j-1|j, k-1|k, l-1|l)
         int ci[8], cs[8];
 #pragma unroll
@@ -329,35 +683,39 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
             for (int iid = 0; iid < 3; iid++) {
                 const int id = (ic + iid) % 3;
                 const int comp = ic == id ? ic : 3 + (3 - ic - id);
-                float F[8], B[8];
+                float Fv[8], B[8];
 #pragma unroll
                 for (int t = 0; t < 8; t++) {
-                    F[t] = CELL(cs[t], comp, ci[t]);
+                    Fv[t] = CELL(cs[t], comp, ci[t]);
                     if (GEOM == GEOM_RECT || (GEOM == GEOM_TERRAIN && id == 2)) B[t] = A.br.bcn[id][t];
                     else B[t] = CELL(cs[t], 18 + 8 * id + t, ci[t]);
                 }
-                float s = stencil8(F, B, h);
-                const int c = id == 0 ? jn : id == 1 ? kn : l;
-                if (c <= g.i1pml[id]) {
-                    const int p = c + g.nnoff[id];
-                    float* P = A.sl.p[id] + slab_idx(g, id, A.sl.tp[id], c - g.i1node[id], jn, kn, l, ic);
-                    s = A.pmlc[g.npml + p - 1] * s + A.pmlc[p - 1] * *P;
-                    *P = *P + dt * s;
-                }
-                if (c >= g.i2pml[id]) {
-                    const int p = g.nn[id] - c - g.nnoff[id] + 1;
-                    float* P = A.sl.p[3 + id] + slab_idx(g, id, A.sl.tp[3 + id], g.i2node[id] - c, jn, kn, l, ic);
-                    s = A.pmlc[g.npml + p - 1] * s + A.pmlc[p - 1] * *P;
-                    *P = *P + dt * s;
+                float s = stencil8(Fv, B, h);
+                if constexpr (!F) {
+                    const int c = id == 0 ? jn : id == 1 ? kn : l;
+                    if (c <= g.i1pml[id]) {
+                        const int p = c + g.nnoff[id];
+                        float* P = A.sl.p[id] + slab_idx(g, id, A.sl.tp[id], c - g.i1node[id], jn, kn, l, ic);
+                        s = A.pmlc[g.npml + p - 1] * s + A.pmlc[p - 1] * *P;
+                        *P = *P + dt * s;
+                    }
+                    if (c >= g.i2pml[id]) {
+                        const int p = g.nn[id] - c - g.nnoff[id] + 1;
+                        float* P = A.sl.p[3 + id] + slab_idx(g, id, A.sl.tp[3 + id], g.i2node[id] - c, jn, kn, l, ic);
+                        s = A.pmlc[g.npml + p - 1] * s + A.pmlc[p - 1] * *P;
+                        *P = *P + dt * s;
+                    }
                 }
                 f[ic] = iid == 0 ? s : f[ic] + s;
             }
         }
         if (A.hourglass) {
-            const int cn_[3] = {jn, kn, l};
             bool ne = true;
+            if constexpr (!F) {
+                const int cn_[3] = {jn, kn, l};
 #pragma unroll
-            for (int d = 0; d < 3; d++) ne = ne && cn_[d] >= g.i1pml[d] + 1 && cn_[d] <= g.i2pml[d] - 1;
+                for (int d = 0; d < 3; d++) ne = ne && cn_[d] >= g.i1pml[d] + 1 && cn_[d] <= g.i2pml[d] - 1;
+            }
             if (ne) {
                 int hi[8], hs[8];
 #pragma unroll
@@ -375,72 +733,83 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
                         for (int t = 0; t < 8; t++) H[t] = CELL(hs[t], 6 + 3 * iq + ic, hi[t]);
                         f[ic] = f[ic] - hg_sum(H, iq);
                     }
-            } else if (A.hgvisc) {
-                // viscous-only hourglass in the PML, cell values formed here from
-                // the node ring (acceleration.f90:164-199)
-                float yc[8];
-                bool okc[8];
-                int cb[8];
-#pragma unroll
-                for (int t = 0; t < 8; t++) {
-                    const int o = hg_corner(t);
-                    const int Jc = jn - (o & 1), Kc = kn - ((o >> 1) & 1), Lc = l - (o >> 2);
-                    const bool real = Jc >= g.i1cell[0] && Jc <= g.i2cell[0] && Kc >= g.i1cell[1] && Kc <= g.i2cell[1] &&
-                                      Lc >= g.i1cell[2] && Lc <= g.i2cell[2];
-                    const bool slab = Jc <= g.i1pml[0] || Jc >= g.i2pml[0] - 1 || Kc <= g.i1pml[1] || Kc >= g.i2pml[1] - 1 ||
-                                      Lc <= g.i1pml[2] || Lc >= g.i2pml[2] - 1;
-                    okc[t] = real && slab;
-                    yc[t] = okc[t] ? A.dh2 * A.yy[g.idx(Jc, Kc, Lc)] : 0.f;
-                    cb[t] = o;
-                }
-                // each component's four modes share the cell corner loads; the
-                // updates of f[ic] keep the reference's mode order
-#pragma unroll 1
-                for (int ic = 0; ic < 3; ic++) {
-                    float Hq[4][8];
+            } else if constexpr (!F) {
+                if (A.hgvisc) {
+                    // viscous-only hourglass in the PML (acceleration.f90:164-199):
+                    // every cell of a PML node is a PML cell; pure PML cells
+                    // hold their viscous values in the hourglass slots, cells
+                    // that are also elastic-hourglass cells (the layer next to
+                    // the elastic region) are evaluated here from v
+                    int hi[8], hs[8], kind[8];
+                    float yc[8];
 #pragma unroll
                     for (int t = 0; t < 8; t++) {
-                        if (okc[t]) {
-                            const int o = cb[t];
-                            float Vc[8];
-#pragma unroll
-                            for (int m = 0; m < 8; m++) {
-                                const int n = hg_corner(m);
-                                const int dj = (n & 1) - (o & 1), dk = ((n >> 1) & 1) - ((o >> 1) & 1), dl = (n >> 2) - (o >> 2);
-                                Vc[m] = NODE((l + dl + 3) % 3, 3 + ic, (tx + 1 + dj) + FNJ * (ty + 1 + dk));
-                            }
-#pragma unroll
-                            for (int iq = 0; iq < 4; iq++) Hq[iq][t] = yc[t] * hg_sum(Vc, iq);
-                        } else {
-#pragma unroll
-                            for (int iq = 0; iq < 4; iq++) Hq[iq][t] = 0.f;
-                        }
+                        const int o = hg_corner(t);
+                        hi[t] = (tx + 1 - (o & 1)) + FJ * (ty + 1 - ((o >> 1) & 1));
+                        hs[t] = (l - (o >> 2)) & 1;
+                        const int Jc = jn - (o & 1), Kc = kn - ((o >> 1) & 1), Lc = l - (o >> 2);
+                        const bool real = Jc >= g.i1cell[0] && Jc <= g.i2cell[0] && Kc >= g.i1cell[1] &&
+                                          Kc <= g.i2cell[1] && Lc >= g.i1cell[2] && Lc <= g.i2cell[2];
+                        const bool slab = Jc <= g.i1pml[0] || Jc >= g.i2pml[0] - 1 || Kc <= g.i1pml[1] ||
+                                          Kc >= g.i2pml[1] - 1 || Lc <= g.i1pml[2] || Lc >= g.i2pml[2] - 1;
+                        const bool inEc = Jc >= g.i1pml[0] && Jc <= g.i2pml[0] - 1 && Kc >= g.i1pml[1] &&
+                                          Kc <= g.i2pml[1] - 1 && Lc >= g.i1pml[2] && Lc <= g.i2pml[2] - 1;
+                        kind[t] = !(real && slab) ? 0 : inEc ? 2 : 1;
+                        yc[t] = kind[t] == 2 ? A.dh2 * A.yy[g.idx(Jc, Kc, Lc)] : 0.f;
                     }
-                    float fi = f[0];
-                    if (ic == 1) fi = f[1];
-                    if (ic == 2) fi = f[2];
+#pragma unroll 1
+                    for (int ic = 0; ic < 3; ic++) {
+                        float Hq[4][8];
 #pragma unroll
-                    for (int iq = 0; iq < 4; iq++) fi = fi - hg_sum(Hq[iq], iq);
-                    if (ic == 0) f[0] = fi;
-                    if (ic == 1) f[1] = fi;
-                    if (ic == 2) f[2] = fi;
+                        for (int t = 0; t < 8; t++) {
+                            if (kind[t] == 1) {
+#pragma unroll
+                                for (int iq = 0; iq < 4; iq++) Hq[iq][t] = CELL(hs[t], 6 + 3 * iq + ic, hi[t]);
+                            } else if (kind[t] == 2) {
+                                const int o = hg_corner(t);
+                                float Vc[8];
+#pragma unroll
+                                for (int m = 0; m < 8; m++) {
+                                    const int n = hg_corner(m);
+                                    const int dj = (n & 1) - (o & 1), dk = ((n >> 1) & 1) - ((o >> 1) & 1),
+                                              dl = (n >> 2) - (o >> 2);
+                                    Vc[m] = A.vin[ic][g.idx(jn + dj, kn + dk, l + dl)];
+                                }
+#pragma unroll
+                                for (int iq = 0; iq < 4; iq++) Hq[iq][t] = yc[t] * hg_sum(Vc, iq);
+                            } else {
+#pragma unroll
+                                for (int iq = 0; iq < 4; iq++) Hq[iq][t] = 0.f;
+                            }
+                        }
+                        float fi = f[0];
+                        if (ic == 1) fi = f[1];
+                        if (ic == 2) fi = f[2];
+#pragma unroll
+                        for (int iq = 0; iq < 4; iq++) fi = fi - hg_sum(Hq[iq], iq);
+                        if (ic == 0) f[0] = fi;
+                        if (ic == 1) f[1] = fi;
+                        if (ic == 2) f[2] = fi;
+                    }
                 }
             }
         }
-        {
+        if constexpr (!F) {
             const Inject* E = nfrc >= 0 ? lfrc : A.force.e;
             const int n = nfrc >= 0 ? nfrc : A.force.n;
             for (int e = 0; e < n; e++)
                 if (E[e].idx == q) {
                     const int c = E[e].comp;
-                    f[c] = f[c] + E[e].inc;
+                    const float inc = E[e].inc;
+                    if (c == 0) f[0] = f[0] + inc;
+                    else if (c == 1) f[1] = f[1] + inc;
+                    else f[2] = f[2] + inc;
                 }
         }
         const float m = cur[4];
 #pragma unroll
         for (int i = 0; i < 3; i++) f[i] = f[i] * m;
-        const float v0 = NODE(sn, 3, ni0), v1 = NODE(sn, 4, ni0), v2 = NODE(sn, 5, ni0);
-        const float u0 = NODE(sn, 0, ni0), u1 = NODE(sn, 1, ni0), u2 = NODE(sn, 2, ni0);
+        const float u0 = uv[0], u1 = uv[1], u2 = uv[2], v0 = uv[3], v1 = uv[4], v2 = uv[5];
         if (A.stats) {
             st_a = fmaxn(st_a, f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
             st_v = fmaxn(st_v, v0 * v0 + v1 * v1 + v2 * v2);
@@ -459,53 +828,175 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
     };
 
     // ---------------------------------------------------------------- stream
-    fetch(L0 - 1);
-    store((L0 - 1) % 3);
-    fetch(L0);
-    store(L0 % 3);
-    fetch(L0 + 1);
-    store((L0 + 1) % 3);
-    stat_load(L0 - 1, cur);
-    __syncthreads();
-    cells(L0 - 1);
-    stat_load(L0, cur);
+    // ring: planes L0-1, L0, L0+1; staged: L0+2 in flight
+#pragma unroll 1
+    for (int p = -1; p <= 1; p++) {
+        fetch(L0 + p);
+        cp_async_wait_all();
+        __syncthreads();
+        store((L0 + p + 3) % 3);
+        __syncthreads();
+    }
     fetch(L0 + 2);
+    stat_load(L0 - 1, cur);
+    uv_load(L0, uv);
+    if constexpr (FASTK) cells_fast(L0 - 1);
+    else cells(L0 - 1, std::false_type{});
+    stat_load(L0, cur);
+#pragma unroll 1
     for (int l = L0; l <= L1; l++) {
-        __syncthreads();
-        cells(l);
-        float nxt[5];
+        if constexpr (FASTK) cells_fast(l);
+        else cells(l, std::false_type{});
+        float nxt[5], nuv[6];
         stat_load(l + 1, nxt);
-        __syncthreads();
-        nodes(l);
-        __syncthreads();
+        cp_async_wait_all();
+        __syncthreads();  // cell plane l complete, staged plane l+2 landed
         store((l + 2) % 3);
+        if constexpr (FASTK) nodes_fast(l);
+        else nodes(l, std::false_type{});
+        uv_load(l + 1, nuv);
+        __syncthreads();  // ring slot l+2 complete, staging and cell slot l-1 free
         fetch(l + 3);
 #pragma unroll
         for (int i = 0; i < 5; i++) cur[i] = nxt[i];
+#pragma unroll
+        for (int i = 0; i < 6; i++) uv[i] = nuv[i];
     }
+    cp_async_wait_all();
     if (A.stats) {
         bmax(A.red + 0, st_a);
         bmax(A.red + 1, st_v);
         bmax(A.red + 2, st_u);
         bmax(A.red + 3, st_w);
     }
+#undef RAW
 #undef NODE
 #undef CELL
 }
 
-template <int GEOM>
-static void launch_geom(Solver& s, const StepArgs& A, dim3 grid) {
-    static bool set = false;
-    if (!set) {
-        SORD_CUDA(cudaFuncSetAttribute(k_step<GEOM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay<GEOM>::bytes));
-        set = true;
-    }
-    k_step<GEOM><<<grid, dim3(FJ, FK), Lay<GEOM>::bytes, s.stream>>>(A);
+// Work decomposition of a fused step, fixed by the mesh: interior tile
+// columns (bx, by) whose cells all lie strictly inside the non-PML region
+// run the fast kernel over the node planes lf0..lf1 whose cells are interior
+// (or halo planes of a free surface); everything else -- PML columns, the
+// PML planes of interior columns, and interior columns holding a point
+// source in the current step -- is a list of (bx, by, l1, l2) items for the
+// general kernel.
+struct FusedPlan {
+    int nbx = 0, nby = 0;
+    int fbx0 = 0, fbx1 = -1, fby0 = 0, fby1 = -1;  // fast tile columns (inclusive)
+    int lf0 = 0, lf1 = -1;                         // fast node planes (inclusive)
+    std::vector<int4> base;                        // general items without point sources
+    std::vector<int4> cur;                         // items of the last upload
+    int4* d_items = nullptr;
+    int4* h_items = nullptr;                       // pinned staging
+    int cap = 0;
+    cudaEvent_t done = nullptr;
+};
+
+void fused_free(Solver& s) {
+    FusedPlan* P = s.fplan;
+    if (!P) return;
+    if (P->done) cudaEventDestroy(P->done);
+    if (P->d_items) cudaFree(P->d_items);
+    if (P->h_items) cudaFreeHost(P->h_items);
+    delete P;
+    s.fplan = nullptr;
 }
 
-void launch_fused(Solver& s, const InjectList& pot, const InjectList& mom, const InjectList& force, bool fold, bool write_a,
-                  bool stats) {
+static constexpr int kItemPlanes = 96;  // longest general item, for load balance
+
+static void push_items(std::vector<int4>& v, int bx, int by, int l1, int l2) {
+    for (int a = l1; a <= l2; a += kItemPlanes) v.push_back(make_int4(bx, by, a, std::min(l2, a + kItemPlanes - 1)));
+}
+
+static FusedPlan& fused_plan(Solver& s) {
+    if (s.fplan) return *s.fplan;
+    FusedPlan* P = new FusedPlan();
+    s.fplan = P;
+    const Geom& g = s.g;
+    const int nj = g.i2node[0] - g.i1node[0] + 1, nk = g.i2node[1] - g.i1node[1] + 1;
+    P->nbx = (int)div_up(nj, FOJ);
+    P->nby = (int)div_up(nk, FOK);
+    auto colok = [&](int d, int b, int w) {  // tile b along axis d (w nodes) is interior
+        const int a0 = g.i1node[d] + b * w;
+        return a0 - 1 > g.i1pml[d] && a0 + w - 1 < g.i2pml[d] - 1 && a0 - 1 >= g.i1cell[d] &&
+               a0 + w - 1 <= g.i2cell[d] && a0 + w - 1 <= g.i2node[d];
+    };
+    for (int b = 0; b < P->nbx; b++)
+        if (colok(0, b, FOJ)) { if (P->fbx1 < P->fbx0) P->fbx0 = b; P->fbx1 = b; }
+    for (int b = 0; b < P->nby; b++)
+        if (colok(1, b, FOK)) { if (P->fby1 < P->fby0) P->fby0 = b; P->fby1 = b; }
+    auto cellok = [&](int c) {
+        return c < g.i1cell[2] || c > g.i2cell[2] || (c > g.i1pml[2] && c < g.i2pml[2] - 1);
+    };
+    for (int l = g.i1node[2]; l <= g.i2node[2]; l++) {
+        const bool f = l >= g.i1pml[2] + 1 && l <= g.i2pml[2] - 1 && cellok(l - 1) && cellok(l);
+        if (f && P->lf1 < P->lf0) P->lf0 = P->lf1 = l;
+        else if (f && P->lf1 == l - 1) P->lf1 = l;
+    }
+    const bool anyfast = P->fbx1 >= P->fbx0 && P->fby1 >= P->fby0 && P->lf1 >= P->lf0;
+    for (int by = 0; by < P->nby; by++)
+        for (int bx = 0; bx < P->nbx; bx++) {
+            const bool fc = anyfast && bx >= P->fbx0 && bx <= P->fbx1 && by >= P->fby0 && by <= P->fby1;
+            if (!fc) {
+                push_items(P->base, bx, by, g.i1node[2], g.i2node[2]);
+            } else {
+                if (P->lf0 > g.i1node[2]) push_items(P->base, bx, by, g.i1node[2], P->lf0 - 1);
+                if (P->lf1 < g.i2node[2]) push_items(P->base, bx, by, P->lf1 + 1, g.i2node[2]);
+            }
+        }
+    if (!anyfast) P->fbx1 = P->fbx0 - 1;
+    P->cap = (int)P->base.size() + 4096;
+    SORD_CUDA(cudaMalloc((void**)&P->d_items, sizeof(int4) * P->cap));
+    SORD_CUDA(cudaMallocHost((void**)&P->h_items, sizeof(int4) * P->cap));
+    SORD_CUDA(cudaEventCreateWithFlags(&P->done, cudaEventDisableTiming));
+    return *P;
+}
+
+// Interior columns whose (j, k) box holds a point source of this step; the
+// boxes are those the fast kernel tests (cells j0-1..j0+30 for potency /
+// moment entries, nodes j0..j0+30 for forces).
+static void source_columns(const Solver& s, const FusedPlan& P, const std::vector<Inject>& e, bool cell,
+                           std::vector<std::pair<int, int>>& out) {
+    const Geom& g = s.g;
+    for (const Inject& x : e) {
+        const int j = (int)(x.idx % g.sy) + 1, k = (int)((x.idx / g.sy) % g.nm[1]) + 1;
+        for (int bx = P.fbx0; bx <= P.fbx1; bx++) {
+            const int j0 = g.i1node[0] + bx * FOJ;
+            if (!(cell ? (j >= j0 - 1 && j <= j0 + FOJ - 1) : (j >= j0 && j <= j0 + FOJ - 1))) continue;
+            for (int by = P.fby0; by <= P.fby1; by++) {
+                const int k0 = g.i1node[1] + by * FOK;
+                if (cell ? (k >= k0 - 1 && k <= k0 + FOK - 1) : (k >= k0 && k <= k0 + FOK - 1)) out.push_back({bx, by});
+            }
+        }
+    }
+}
+
+template <int GEOM, bool FASTK>
+static void launch_mode(Solver& s, const StepArgs& A, dim3 grid) {
+    static bool set = false;
+    if (!set) {
+        SORD_CUDA(cudaFuncSetAttribute(k_step<GEOM, FASTK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)Lay<GEOM>::bytes));
+        set = true;
+    }
+    k_step<GEOM, FASTK><<<grid, dim3(FJ, FK), Lay<GEOM>::bytes, s.stream>>>(A);
+    s.launches++;
+    SORD_CUDA(cudaGetLastError());
+}
+
+template <bool FASTK>
+static void launch_geom(Solver& s, const StepArgs& A, dim3 grid) {
+    if (s.geom == GEOM_RECT) launch_mode<GEOM_RECT, FASTK>(s, A, grid);
+    else if (s.geom == GEOM_TERRAIN) launch_mode<GEOM_TERRAIN, FASTK>(s, A, grid);
+    else launch_mode<GEOM_GENERAL, FASTK>(s, A, grid);
+}
+
+void launch_fused(Solver& s, const InjectList& pot, const InjectList& mom, const InjectList& force,
+                  const std::vector<Inject>& hpot, const std::vector<Inject>& hmom, const std::vector<Inject>& hforce,
+                  bool fold, bool write_a, bool stats) {
     Device& d = s.d;
+    FusedPlan& P = fused_plan(s);
     StepArgs A;
     A.g = s.g;
     A.br = s.br;
@@ -531,21 +1022,45 @@ void launch_fused(Solver& s, const InjectList& pot, const InjectList& mom, const
     A.fold = fold ? 1 : 0;
     A.stats = stats ? 1 : 0;
     A.red = (unsigned*)d.red;
-    const Geom& g = s.g;
-    int nj = g.i2node[0] - g.i1node[0] + 1, nk = g.i2node[1] - g.i1node[1] + 1, nl = g.i2node[2] - g.i1node[2] + 1;
-    unsigned bx = div_up(nj, FOJ), by = div_up(nk, FOK);
-    long long bxy = (long long)bx * by;
-    int nseg = (int)std::min<long long>(std::max<long long>(1, (4LL * 148 + bxy - 1) / bxy), std::max(1, nl / 8));
-    A.segl = (nl + nseg - 1) / nseg;
-    nseg = (nl + A.segl - 1) / A.segl;
-    dim3 grid(bx, by, nseg);
+    A.bx0 = P.fbx0;
+    A.by0 = P.fby0;
+    A.lf0 = P.lf0;
+    A.lf1 = P.lf1;
+    A.segl = P.lf1 - P.lf0 + 1;
+    A.items = P.d_items;
+
+    // general items of this step: the fixed list, plus whole columns for
+    // interior columns holding a point source
+    std::vector<std::pair<int, int>> src;
+    if (P.fbx1 >= P.fbx0) {
+        source_columns(s, P, hpot, true, src);
+        source_columns(s, P, hmom, true, src);
+        source_columns(s, P, hforce, false, src);
+        std::sort(src.begin(), src.end());
+        src.erase(std::unique(src.begin(), src.end()), src.end());
+    }
+    std::vector<int4> items;
+    items.reserve(P.base.size() + src.size() * 4);
+    for (const int4& it : P.base)
+        if (src.empty() || !std::binary_search(src.begin(), src.end(), std::make_pair(it.x, it.y))) items.push_back(it);
+    for (auto& c : src) push_items(items, c.first, c.second, s.g.i1node[2], s.g.i2node[2]);
+    const bool same = items.size() == P.cur.size() &&
+                      std::equal(items.begin(), items.end(), P.cur.begin(), [](const int4& a, const int4& b) {
+                          return a.x == b.x && a.y == b.y && a.z == b.z && a.w == b.w;
+                      });
+    if (!same) {
+        if ((int)items.size() > P.cap) throw SordError(SORD_E_PARAM, "too many point-source columns in one step");
+        SORD_CUDA(cudaEventSynchronize(P.done));
+        std::memcpy(P.h_items, items.data(), sizeof(int4) * items.size());
+        SORD_CUDA(cudaMemcpyAsync(P.d_items, P.h_items, sizeof(int4) * items.size(), cudaMemcpyHostToDevice, s.stream));
+        SORD_CUDA(cudaEventRecord(P.done, s.stream));
+        P.cur = items;
+    }
+
     cudaEvent_t e0 = nullptr;
     s.prof_begin(KC_FUSED, &e0);
-    if (s.geom == GEOM_RECT) launch_geom<GEOM_RECT>(s, A, grid);
-    else if (s.geom == GEOM_TERRAIN) launch_geom<GEOM_TERRAIN>(s, A, grid);
-    else launch_geom<GEOM_GENERAL>(s, A, grid);
-    s.launches++;
-    SORD_CUDA(cudaGetLastError());
+    if (P.fbx1 >= P.fbx0) launch_geom<true>(s, A, dim3(P.fbx1 - P.fbx0 + 1, P.fby1 - P.fby0 + 1, 1));
+    if (!items.empty()) launch_geom<false>(s, A, dim3((unsigned)items.size(), 1, 1));
     s.prof_end(KC_FUSED, e0);
     if (fold) {
         for (int i = 0; i < 3; i++) {

@@ -46,9 +46,15 @@ __device__ __forceinline__ void apply_inject(const Inject* loc, int nloc, const 
     const int n = nloc >= 0 ? nloc : L.n;
     for (int e = 0; e < n; e++)
         if (E[e].idx == q) {
+            // constant indices only, so ed / eo stay in registers
             const int c = E[e].comp;
-            if (c < 3) ed[c] = ed[c] + E[e].inc;
-            else eo[c - 3] = eo[c - 3] + E[e].inc;
+            const float inc = E[e].inc;
+            if (c == 0) ed[0] = ed[0] + inc;
+            else if (c == 1) ed[1] = ed[1] + inc;
+            else if (c == 2) ed[2] = ed[2] + inc;
+            else if (c == 3) eo[0] = eo[0] + inc;
+            else if (c == 4) eo[1] = eo[1] + inc;
+            else eo[2] = eo[2] + inc;
         }
 }
 

@@ -143,6 +143,10 @@ struct StepArgs {
     int hourglass, hgvisc, fold, stats;
     unsigned* red;
     int segl;
+    // fast kernel: first tile (bx0, by0) and node planes lf0..lf1;
+    // general kernel: work items (bx, by, first plane, last plane)
+    int bx0, by0, lf0, lf1;
+    const int4* items;
 };
 
 // Device state of one handle.
@@ -190,7 +194,11 @@ void launch_mass(Solver& s, bool stats);
 void launch_vector_bc(Solver& s, float* const f[3], const int* bc1, const int* bc2, const int* i1, const int* i2);
 void launch_scalar_bc(Solver& s, float* f, const int* fn, const int* bc1, const int* bc2, const int* i1, const int* i2);
 void launch_inject(Solver& s, float* const f[6], const InjectList& l);
-void launch_fused(Solver& s, const InjectList& pot, const InjectList& mom, const InjectList& force, bool fold, bool write_a,
+struct FusedPlan;
+void fused_free(Solver& s);
+void launch_fused(Solver& s, const InjectList& pot, const InjectList& mom, const InjectList& force,
+                  const std::vector<Inject>& hpot, const std::vector<Inject>& hmom, const std::vector<Inject>& hforce,
+                  bool fold, bool write_a,
                   bool stats);
 
 // setup.cu
@@ -266,6 +274,8 @@ struct Solver {
     std::vector<float> src_xi[3], src_dt, src_t0, src_w1[3], src_w2[3], src_history;
     // injection staging (pinned): one slot per list
     Inject* hinj = nullptr;
+    // work decomposition of the fused step kernels (fused.cu)
+    FusedPlan* fplan = nullptr;
     cudaEvent_t inj_done[kInjectSlots] = {};
     // fault bookkeeping
     int fn3[3] = {0, 0, 0};

@@ -18,12 +18,12 @@ namespace sordgpu {
 // corner id = dj + 2*dk + 4*dl.
 SORD_HD int term_corner(int t) { return t < 6 ? t : 13 - t; }
 
-// Brackets of diff_nc for direction a (0-based) at one cell; X[c][n] is
-// coordinate c at corner n = dj + 2*dk + 4*dl.  B[t] multiplies term t.
-// sord/diff_nc_op.f90:19-70.
-SORD_HD void brackets_nc(const float (*X)[8], int a, float B[8]) {
-    const float* xb = X[(a + 1) % 3];
-    const float* xc = X[(a + 2) % 3];
+// Brackets of diff_nc for one direction at one cell, from the two other
+// coordinates xb, xc at the corners n = dj + 2*dk + 4*dl.  B[t] multiplies
+// term t.  sord/diff_nc_op.f90:19-70.  T is float, or a pair type whose
+// operators apply the same IEEE operation to two independent lanes.
+template <class T>
+SORD_HD void brackets_nc_g(const T* xb, const T* xc, T B[8]) {
 #define XB(j, k, l) xb[(j) + 2 * (k) + 4 * (l)]
 #define XC(j, k, l) xc[(j) + 2 * (k) + 4 * (l)]
     B[0] = (XB(0, 1, 1) - XB(1, 0, 0)) * (XC(0, 1, 0) - XC(0, 0, 1)) + XB(1, 0, 0) * (XC(1, 0, 1) - XC(1, 1, 0)) +
@@ -54,15 +54,19 @@ SORD_HD void brackets_nc(const float (*X)[8], int a, float B[8]) {
 #undef XC
 }
 
+// Direction a (0-based) with X[c][n] = coordinate c at corner n.
+SORD_HD void brackets_nc(const float (*X)[8], int a, float B[8]) {
+    brackets_nc_g<float>(X[(a + 1) % 3], X[(a + 2) % 3], B);
+}
+
 // Brackets of diff_cn for direction a at one node; X[c][m] is coordinate c
 // at neighbour m = (dj+1) + 3*(dk+1) + 9*(dl+1), dj,dk,dl in -1..1.
 // B[t] multiplies the cell of term t: (j-1,k-1,l-1) (j,k-1,l-1) (j-1,k-1,l)
 // (j,k-1,l) (j-1,k,l-1) (j,k,l-1) (j-1,k,l) (j,k,l).  sord/diff_cn_op.f90:19-70.
-template <class XA>
-SORD_HD void brackets_cn(const XA& X, int a, float B[8]) {
-    int b = (a + 1) % 3, c = (a + 2) % 3;
-#define XB(j, k, l) X(b, (j) + 1 + 3 * ((k) + 1) + 9 * ((l) + 1))
-#define XC(j, k, l) X(c, (j) + 1 + 3 * ((k) + 1) + 9 * ((l) + 1))
+template <class T, class XA>
+SORD_HD void brackets_cn_g(const XA& xb, const XA& xc, T B[8]) {
+#define XB(j, k, l) xb((j) + 1 + 3 * ((k) + 1) + 9 * ((l) + 1))
+#define XC(j, k, l) xc((j) + 1 + 3 * ((k) + 1) + 9 * ((l) + 1))
     B[0] = (XB(-1, 0, 0) - XB(0, -1, -1)) * (XC(0, 0, -1) - XC(0, -1, 0)) + XB(-1, 0, 0) * (XC(-1, 0, -1) - XC(-1, -1, 0)) +
            (XB(0, -1, 0) - XB(-1, 0, -1)) * (XC(-1, 0, 0) - XC(0, 0, -1)) + XB(0, -1, 0) * (XC(-1, -1, 0) - XC(0, -1, -1)) +
            (XB(0, 0, -1) - XB(-1, -1, 0)) * (XC(0, -1, 0) - XC(-1, 0, 0)) + XB(0, 0, -1) * (XC(0, -1, -1) - XC(-1, 0, -1));
@@ -91,9 +95,22 @@ SORD_HD void brackets_cn(const XA& X, int a, float B[8]) {
 #undef XC
 }
 
+template <class XA>
+struct CoordOf {
+    const XA& X;
+    int c;
+    SORD_HD float operator()(int m) const { return X(c, m); }
+};
+template <class XA>
+SORD_HD void brackets_cn(const XA& X, int a, float B[8]) {
+    CoordOf<XA> xb{X, (a + 1) % 3}, xc{X, (a + 2) % 3};
+    brackets_cn_g<float>(xb, xc, B);
+}
+
 // Weighted 8-term sum  d = h*F0*B0; d = d + h*Ft*Bt  (diff_nc / diff_cn).
-SORD_HD float stencil8(const float F[8], const float B[8], float h) {
-    float d = h * F[0] * B[0];
+template <class T>
+SORD_HD T stencil8(const T F[8], const T B[8], T h) {
+    T d = h * F[0] * B[0];
 #pragma unroll
     for (int t = 1; t < 8; t++) d = d + h * F[t] * B[t];
     return d;
@@ -106,8 +123,9 @@ SORD_HD float stencil8(const float F[8], const float B[8], float h) {
 SORD_HD int hg_corner(int t) { return (int)((0x43251670u >> (4 * t)) & 0xFu); }
 SORD_HD int hg_neg(int iq, int t) { return (int)(((0xAA3CCCF0u >> (8 * iq)) >> t) & 1u); }
 
-SORD_HD float hg_sum(const float A[8], int iq) {
-    float r = A[0];
+template <class T>
+SORD_HD T hg_sum(const T A[8], int iq) {
+    T r = A[0];
 #pragma unroll
     for (int t = 1; t < 8; t++) r = hg_neg(iq, t) ? r - A[t] : r + A[t];
     return r;
@@ -123,43 +141,47 @@ SORD_HD float hg_sum(const float A[8], int iq) {
 // bitwise by tests/stencil_identity.cpp); terms 1, 2, 5, 6 differ in operand
 // order and are evaluated with the diff_cn expression.  X[c][n]: cell corner
 // coordinates.
-SORD_HD void cell_cn_brackets(const float (*X)[8], int a, const float nc[8], float cn[8]) {
-    cn[0] = 0.0f - nc[6];
-    cn[3] = 0.0f - nc[2];
-    cn[4] = 0.0f - nc[5];
-    cn[7] = 0.0f - nc[0];
+template <class T>
+SORD_HD void cell_cn_brackets_g(const T* xb, const T* xc, const T nc[8], T cn[8], T zero) {
+    cn[0] = zero - nc[6];
+    cn[3] = zero - nc[2];
+    cn[4] = zero - nc[5];
+    cn[7] = zero - nc[0];
     // node-relative accessors for the four remaining terms; the node sits at
     // cell corner o = (oj, ok, ol) and neighbour d maps to corner o + d.
     struct Acc {
-        const float (*X)[8];
+        const T* x;
         int o;
-        SORD_HD float operator()(int c, int m) const {
+        SORD_HD T operator()(int m) const {
             int dj = m % 3 - 1, dk = (m / 3) % 3 - 1, dl = m / 9 - 1;
             int oj = o & 1, ok = (o >> 1) & 1, ol = (o >> 2) & 1;
-            return X[c][(oj + dj) + 2 * (ok + dk) + 4 * (ol + dl)];
+            return x[(oj + dj) + 2 * (ok + dk) + 4 * (ol + dl)];
         }
     };
-    float B[8];
+    T B[8];
     {  // term 1: cell (j, k-1, l-1) -> node at corner (0,1,1)
-        Acc A{X, 6};
-        brackets_cn(A, a, B);
+        Acc b{xb, 6}, c{xc, 6};
+        brackets_cn_g<T>(b, c, B);
         cn[1] = B[1];
     }
     {  // term 2: cell (j-1, k-1, l) -> node at corner (1,1,0)
-        Acc A{X, 3};
-        brackets_cn(A, a, B);
+        Acc b{xb, 3}, c{xc, 3};
+        brackets_cn_g<T>(b, c, B);
         cn[2] = B[2];
     }
     {  // term 5: cell (j, k, l-1) -> node at corner (0,0,1)
-        Acc A{X, 4};
-        brackets_cn(A, a, B);
+        Acc b{xb, 4}, c{xc, 4};
+        brackets_cn_g<T>(b, c, B);
         cn[5] = B[5];
     }
     {  // term 6: cell (j-1, k, l) -> node at corner (1,0,0)
-        Acc A{X, 1};
-        brackets_cn(A, a, B);
+        Acc b{xb, 1}, c{xc, 1};
+        brackets_cn_g<T>(b, c, B);
         cn[6] = B[6];
     }
+}
+SORD_HD void cell_cn_brackets(const float (*X)[8], int a, const float nc[8], float cn[8]) {
+    cell_cn_brackets_g<float>(X[(a + 1) % 3], X[(a + 2) % 3], nc, cn, 0.0f);
 }
 
 }  // namespace sordgpu
