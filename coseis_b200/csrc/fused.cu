@@ -52,17 +52,30 @@ constexpr int NPL = FNJ * FNK;                // 297 nodes per plane
 constexpr int NCL = FJ * FK;                  // 256 cells per plane
 constexpr int NTH = FJ * FK;
 
+// Shared-memory layout.  Node planes: float4 groups per node,
+//   group 0 = (w_x, w_y, w_z, coordinate 0), group 1 = (h_x, h_y, h_z,
+//   coordinate 1), group 2 = (coordinate 2, -, -, -) on general meshes,
+// with w = u + gam v and h = hg1 u + dt hg2 v; terrain meshes store z as
+// coordinate 0, general meshes x, y, z.  Cell planes: float4 groups per cell,
+//   0: s_xx s_yy s_zz s_yz   1: s_zx s_xy hA0   2: hA1 hA2   3: hA3 hB0 hB1
+//   4: hB2 hB3 - -   5..8: (b0, b1) divergence brackets of terms 2g, 2g+1
+//   9, 10: b2 of terms 0..7 (general meshes)
+// where hA_iq = hourglass values of mode iq for components (x, y) and
+// hB_iq the z component, so every packed pair is an aligned float2.
 template <int GEOM>
 struct Lay {
     static constexpr int NCOORD = GEOM == GEOM_RECT ? 0 : GEOM == GEOM_TERRAIN ? 1 : 3;
-    static constexpr int RAWF = 7 + NCOORD;   // staged plane: u(3) v(3) gam coords
-    static constexpr int NODEF = 6 + NCOORD;  // ring: w = u + gam v (3), hg1 u + dt hg2 v (3), coords
-    static constexpr int HG = 3;              // first hourglass-input field
-    static constexpr int CO = 6;              // first coordinate field
+    static constexpr int RAWF = 7 + NCOORD;                   // staged plane: u(3) v(3) gam coords
+    static constexpr int RAWSZ = (RAWF * NPL + 3) & ~3;        // floats, float4-aligned end
+    static constexpr int NGN = GEOM == GEOM_GENERAL ? 3 : 2;  // float4 groups per node
     static constexpr int NDIR = GEOM == GEOM_RECT ? 0 : GEOM == GEOM_TERRAIN ? 2 : 3;
-    static constexpr int CELLF = 6 + 12 + 8 * NDIR;  // stress, hourglass, divergence brackets
-    static constexpr size_t bytes = sizeof(float) * (size_t)(NPL * RAWF + 3 * NPL * NODEF + 2 * NCL * CELLF);
+    static constexpr int NGC = GEOM == GEOM_RECT ? 5 : GEOM == GEOM_TERRAIN ? 9 : 11;  // float4 groups per cell
+    static constexpr size_t bytes = sizeof(float) * (size_t)RAWSZ + sizeof(float4) * (size_t)(3 * NPL * NGN + 2 * NCL * NGC);
 };
+// scalar field numbers of the node and cell groups
+__host__ __device__ constexpr int nf_co(int c) { return c == 0 ? 3 : c == 1 ? 7 : 8; }
+__host__ __device__ constexpr int cf_hg(int iq, int ic) { return ic < 2 ? 6 + 2 * iq + ic : 14 + iq; }
+__host__ __device__ constexpr int cf_br(int a, int t) { return a < 2 ? 20 + 2 * t + a : 36 + t; }
 
 __device__ __forceinline__ void bmax(unsigned* dst, float v) {
     unsigned b = __float_as_uint(v);
@@ -103,13 +116,12 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 template <int GEOM, bool FASTK>
 __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(StepArgs A) {
     using L = Lay<GEOM>;
-    extern __shared__ float sm[];
-    float* sR = sm;                          // [RAWF][NPL] staged plane
-    float* sN = sR + L::RAWF * NPL;          // [3 slots][NODEF][NPL]
-    float* sC = sN + 3 * L::NODEF * NPL;     // [2 slots][CELLF][NCL]
+    constexpr int NGN = L::NGN, NGC = L::NGC, NDIR = L::NDIR;
+    extern __shared__ float4 sm4[];
+    float* sR = reinterpret_cast<float*>(sm4);  // [RAWF][NPL] staged plane
+    float4* sN = sm4 + L::RAWSZ / 4;            // [3 slots][NGN][NPL]
+    float4* sC = sN + 3 * NGN * NPL;            // [2 slots][NGC][NCL]
 #define RAW(f, i) sR[(f) * NPL + (i)]
-#define NODE(slot, f, i) sN[((slot) * L::NODEF + (f)) * NPL + (i)]
-#define CELL(slot, f, i) sC[((slot) * L::CELLF + (f)) * NCL + (i)]
     const Geom& g = A.g;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + FJ * ty;
     int bx, by, L0, L1;
@@ -132,6 +144,7 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
     const bool cellcol = J >= g.i1cell[0] && J <= g.i2cell[0] && K >= g.i1cell[1] && K <= g.i2cell[1];
     const bool owncol = J >= j0 && K >= k0;
     const float h = g.h, dt = g.dt;
+    const unsigned long long nz = f2_pack(A.negzero, A.negzero);  // (-0.0, -0.0) from the host (pair.cuh)
     float st_a = 0.f, st_v = 0.f, st_u = 0.f, st_w = 0.f;
     // terrain meshes: this thread's cell column's x (j, j+1) and y (k, k+1)
     float txa = 0.f, txb = 0.f, tya = 0.f, tyb = 0.f;
@@ -188,19 +201,24 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
     // staged plane -> ring slot: w1 = u + gam * v (time_integration.f90:36)
     // and the hourglass input hg1 u + dt hg2 v (acceleration.f90:141)
     auto store = [&](int slot) {
+        float4* dst = sN + slot * (NGN * NPL);
 #pragma unroll
         for (int r = 0; r < 2; r++) {
             const int n = tid + r * NTH;
             if (n < NPL) {
                 const float gm = RAW(6, n);
+                float w[3], hh[3];
 #pragma unroll
                 for (int c = 0; c < 3; c++) {
                     const float u = RAW(c, n), v = RAW(3 + c, n);
-                    NODE(slot, c, n) = u + gm * v;
-                    NODE(slot, L::HG + c, n) = A.hg1 * u + A.dh2 * v;
+                    w[c] = u + gm * v;
+                    hh[c] = A.hg1 * u + A.dh2 * v;
                 }
-#pragma unroll
-                for (int f = 0; f < L::NCOORD; f++) NODE(slot, L::CO + f, n) = RAW(7 + f, n);
+                const float c0 = L::NCOORD > 0 ? RAW(7, n) : 0.f;
+                const float c1 = L::NCOORD > 1 ? RAW(8, n) : 0.f;
+                dst[n] = make_float4(w[0], w[1], w[2], c0);
+                dst[NPL + n] = make_float4(hh[0], hh[1], hh[2], c1);
+                if (NGN > 2) dst[2 * NPL + n] = make_float4(L::NCOORD > 2 ? RAW(9, n) : 0.f, 0.f, 0.f, 0.f);
             }
         }
     };
@@ -230,378 +248,297 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
         }
     };
 
+    // one cell's results into cell slot cs (layout of Lay)
+#define WRITE_CELL(cs, ed, eo, he, cnb)                                                                   \
+    do {                                                                                                   \
+        float4* cw_ = sC + (cs) * (NGC * NCL) + tid;                                                       \
+        cw_[0] = make_float4(ed[0], ed[1], ed[2], eo[0]);                                                  \
+        cw_[NCL] = make_float4(eo[1], eo[2], he[0], he[1]);                                                \
+        cw_[2 * NCL] = make_float4(he[3], he[4], he[6], he[7]);                                            \
+        cw_[3 * NCL] = make_float4(he[9], he[10], he[2], he[5]);                                           \
+        cw_[4 * NCL] = make_float4(he[8], he[11], 0.f, 0.f);                                               \
+        if (NDIR >= 2)                                                                                     \
+            _Pragma("unroll") for (int q2 = 0; q2 < 4; q2++) cw_[(5 + q2) * NCL] =                         \
+                make_float4(cnb[0][2 * q2], cnb[1][2 * q2], cnb[0][2 * q2 + 1], cnb[1][2 * q2 + 1]);        \
+        if (NDIR == 3) {                                                                                   \
+            cw_[9 * NCL] = make_float4(cnb[NDIR - 1][0], cnb[NDIR - 1][1], cnb[NDIR - 1][2], cnb[NDIR - 1][3]); \
+            cw_[10 * NCL] = make_float4(cnb[NDIR - 1][4], cnb[NDIR - 1][5], cnb[NDIR - 1][6], cnb[NDIR - 1][7]); \
+        }                                                                                                  \
+    } while (0)
+
     // ---------------------------------------------------------------- cell phase
     auto cells = [&](int l, auto fast_tag) {
         constexpr bool F = decltype(fast_tag)::value;
         const int cs = l & 1;
-        const bool valid = F || (cellcol && l >= g.i1cell[2] && l <= g.i2cell[2]);
-        float ed[3] = {0.f, 0.f, 0.f}, eo[3] = {0.f, 0.f, 0.f};
-        float he[12];
+        const bool valid = (F || cellcol) && l >= g.i1cell[2] && l <= g.i2cell[2];
+        if (!valid) {
+            float4* cw = sC + cs * (NGC * NCL) + tid;
 #pragma unroll
-        for (int i = 0; i < 12; i++) he[i] = 0.f;
-        float cnb[L::NDIR > 0 ? L::NDIR : 1][8];
-        if (valid) {
-            const long long q = g.idx(J, K, l);
-            const int s0 = l % 3, s1 = (l + 1) % 3;
-            int ni[8], ns[8];
-#pragma unroll
-            for (int n = 0; n < 8; n++) {
-                ni[n] = (tx + (n & 1)) + FNJ * (ty + ((n >> 1) & 1));
-                ns[n] = (n >> 2) ? s1 : s0;
-            }
-            float B[3][8];
-            if (GEOM == GEOM_RECT) {
-#pragma unroll
-                for (int a = 0; a < 3; a++)
-#pragma unroll
-                    for (int t = 0; t < 8; t++) B[a][t] = A.br.bnc[a][t];
-            } else {
-                float X[3][8];
-                if (GEOM == GEOM_TERRAIN) {
-                    const float xa = txa, xb = txb, ya = tya, yb = tyb;
-#pragma unroll
-                    for (int n = 0; n < 8; n++) {
-                        X[0][n] = (n & 1) ? xb : xa;
-                        X[1][n] = ((n >> 1) & 1) ? yb : ya;
-                        X[2][n] = NODE(ns[n], L::CO, ni[n]);
-                    }
-                } else {
-#pragma unroll
-                    for (int c = 0; c < 3; c++)
-#pragma unroll
-                        for (int n = 0; n < 8; n++) X[c][n] = NODE(ns[n], L::CO + c, ni[n]);
-                }
-#pragma unroll
-                for (int a = 0; a < L::NDIR; a++) {
-                    brackets_nc(X, a, B[a]);
-                    cell_cn_brackets(X, a, B[a], cnb[a]);
-                }
-                if (GEOM == GEOM_TERRAIN)
-#pragma unroll
-                    for (int t = 0; t < 8; t++) B[2][t] = A.br.bnc[2][t];
-            }
-            const bool own = owncol && l >= L0;
-            if constexpr (F) {
-                // strain of an interior cell: gradients of w = u + gam v
-#pragma unroll
-                for (int ic = 0; ic < 3; ic++) {
-                    float W[8];
-#pragma unroll
-                    for (int t = 0; t < 8; t++) {
-                        const int n = term_corner(t);
-                        W[t] = NODE(ns[n], ic, ni[n]);
-                    }
-#pragma unroll
-                    for (int iid = 0; iid < 3; iid++) {
-                        const int id = (ic + iid + 1) % 3;
-                        const float s = stencil8(W, B[id], h);
-                        if (ic == id) ed[ic] = s;
-                        else if (ic < id) eo[3 - ic - id] = 0.5f * s;
-                        else eo[3 - ic - id] = eo[3 - ic - id] + 0.5f * s;
-                    }
-                }
-            } else {
-                // region of the cell (stress.f90:141-248)
-                bool nearS[3], farS[3], anyS = false;
-                const int cc[3] = {J, K, l};
-#pragma unroll
-                for (int d = 0; d < 3; d++) {
-                    nearS[d] = cc[d] <= g.i1pml[d];
-                    farS[d] = cc[d] >= g.i2pml[d] - 1;
-                    anyS = anyS || nearS[d] || farS[d];
-                }
-                // PML cells that are not elastic-hourglass cells carry the
-                // viscous hourglass values dt hg2 yy hourglass_nc(v) in the
-                // hourglass slots (acceleration.f90:164-183)
-                bool inEc = true;
-#pragma unroll
-                for (int d = 0; d < 3; d++) inEc = inEc && cc[d] >= g.i1pml[d] && cc[d] <= g.i2pml[d] - 1;
-                const bool visc = A.hourglass && A.hgvisc && anyS && !inEc;
-                const float yv = A.dh2 * cur[3];
-#pragma unroll
-                for (int ic = 0; ic < 3; ic++) {
-                    float W[8], U[8], V[8];
-#pragma unroll
-                    for (int t = 0; t < 8; t++) {
-                        const int n = term_corner(t);
-                        W[t] = NODE(ns[n], ic, ni[n]);
-                        U[t] = 0.f;
-                        V[t] = 0.f;
-                    }
-                    if (anyS) {
-#pragma unroll
-                        for (int t = 0; t < 8; t++) {
-                            const int n = term_corner(t);
-                            const long long qn = g.idx(J + (n & 1), K + ((n >> 1) & 1), l + (n >> 2));
-                            U[t] = A.uin[ic][qn];
-                            V[t] = A.vin[ic][qn];
-                        }
-                    }
-                    if (visc) {
-                        float Vc[8], Vh[8];
-#pragma unroll
-                        for (int t = 0; t < 8; t++) Vc[term_corner(t)] = V[t];
-#pragma unroll
-                        for (int t = 0; t < 8; t++) Vh[t] = Vc[hg_corner(t)];
-#pragma unroll
-                        for (int iq = 0; iq < 4; iq++) he[3 * iq + ic] = yv * hg_sum(Vh, iq);
-                    }
-#pragma unroll
-                    for (int iid = 0; iid < 3; iid++) {
-                        const int id = (ic + iid + 1) % 3;
-                        float s;
-                        if (nearS[id] || farS[id]) {
-                            const float raw = stencil8(V, B[id], h);
-                            s = raw;
-                            const int c = cc[id];
-                            if (nearS[id]) {
-                                const int p = c + g.nnoff[id];
-                                const long long gi = slab_idx(g, id, A.sl.tg[id], c - g.i1cell[id], J, K, l, ic);
-                                s = A.pmlc[3 * g.npml + p - 1] * raw + A.pmlc[2 * g.npml + p - 1] * A.sl.g[id][gi];
-                                if (own) A.gout[id][gi] = s;
-                            }
-                            if (farS[id]) {
-                                const int p = g.nn[id] - c - g.nnoff[id];
-                                const long long gi = slab_idx(g, id, A.sl.tg[3 + id], g.i2cell[id] - c, J, K, l, ic);
-                                s = A.pmlc[3 * g.npml + p - 1] * raw + A.pmlc[2 * g.npml + p - 1] * A.sl.g[3 + id][gi];
-                                if (own) A.gout[3 + id][gi] = s;
-                            }
-                        } else if (anyS) {
-                            s = stencil8(U, B[id], h);
-                        } else {
-                            s = stencil8(W, B[id], h);
-                        }
-                        if (ic == id) ed[ic] = s;
-                        else if (ic < id) eo[3 - ic - id] = 0.5f * s;
-                        else eo[3 - ic - id] = eo[3 - ic - id] + 0.5f * s;
-                    }
-                }
-                apply_inject(lpot, npot, A.pot, q, ed, eo);
-            }
-            {
-                const float lm = cur[0], m2 = 2.0f * cur[1];
-                const float s1v = lm * (ed[0] + ed[1] + ed[2]);
-#pragma unroll
-                for (int i = 0; i < 3; i++) { ed[i] = m2 * ed[i] + s1v; eo[i] = m2 * eo[i]; }
-            }
-            if constexpr (!F) apply_inject(lmom, nmom, A.mom, q, ed, eo);
-            {
-                const float r = cur[2];
-#pragma unroll
-                for (int i = 0; i < 3; i++) { ed[i] = ed[i] * r; eo[i] = eo[i] * r; }
-            }
-            if (A.stats && own)
-                st_w = fmaxn(st_w, (ed[0] * ed[0] + ed[1] * ed[1] + ed[2] * ed[2]) + 2.0f * (eo[0] * eo[0] + eo[1] * eo[1] + eo[2] * eo[2]));
-            // elastic hourglass cell values (acceleration.f90:141-156)
-            if (A.hourglass) {
-                bool inE = true;
-                if constexpr (!F) {
-                    const int cc[3] = {J, K, l};
-#pragma unroll
-                    for (int d = 0; d < 3; d++) inE = inE && cc[d] >= g.i1pml[d] && cc[d] <= g.i2pml[d] - 1;
-                }
-                if (inE) {
-                    const float y = cur[3];
-#pragma unroll
-                    for (int ic = 0; ic < 3; ic++) {
-                        float W2[8];
-#pragma unroll
-                        for (int t = 0; t < 8; t++) {
-                            const int n = hg_corner(t);
-                            W2[t] = NODE(ns[n], L::HG + ic, ni[n]);
-                        }
-#pragma unroll
-                        for (int iq = 0; iq < 4; iq++) he[3 * iq + ic] = hg_sum(W2, iq) * y;
-                    }
-                }
-            }
-        } else {
-#pragma unroll
-            for (int a = 0; a < L::NDIR; a++)
-#pragma unroll
-                for (int t = 0; t < 8; t++) cnb[a][t] = 0.f;
-        }
-#pragma unroll
-        for (int i = 0; i < 3; i++) { CELL(cs, i, tid) = ed[i]; CELL(cs, 3 + i, tid) = eo[i]; }
-#pragma unroll
-        for (int i = 0; i < 12; i++) CELL(cs, 6 + i, tid) = he[i];
-#pragma unroll
-        for (int a = 0; a < L::NDIR; a++)
-#pragma unroll
-            for (int t = 0; t < 8; t++) CELL(cs, 18 + 8 * a + t, tid) = cnb[a][t];
-    };
-
-    // ---------------------------------------------------------------- fast path
-    // Same arithmetic as cells() / nodes() for interior tiles, with the
-    // independent stencils evaluated two per packed instruction and every
-    // shared-memory operand at a constant offset from a per-plane base.
-    const float* const nbase = sN + (tx + FNJ * ty);
-    float* const cbase = sC + tid;
-    auto cells_fast = [&](int l) {
-        float* cw = cbase + (l & 1) * (L::CELLF * NCL);
-        if (l < g.i1cell[2] || l > g.i2cell[2]) {  // halo plane of a free surface
-#pragma unroll
-            for (int i = 0; i < L::CELLF; i++) cw[i * NCL] = 0.f;
+            for (int i = 0; i < NGC; i++) cw[i * NCL] = make_float4(0.f, 0.f, 0.f, 0.f);
             return;
         }
-        const float* p0 = nbase + (l % 3) * (L::NODEF * NPL);        // node plane l
-        const float* p1 = nbase + ((l + 1) % 3) * (L::NODEF * NPL);  // node plane l+1
-#define NC(n, f) (((n) >> 2) ? p1 : p0)[(f) * NPL + ((n) & 1) + FNJ * (((n) >> 1) & 1)]
-        const F2 h2 = f2(h);
+        const long long q = g.idx(J, K, l);
+        // corner values by corner id n = dj + 2 dk + 4 dl (node planes l, l+1)
+        float Wc[3][8], Hc[3][8], X0[8], X1[8], X2[8];
+        {
+            const float4* p0 = sN + (l % 3) * (NGN * NPL) + (tx + FNJ * ty);
+            const float4* p1 = sN + ((l + 1) % 3) * (NGN * NPL) + (tx + FNJ * ty);
+#pragma unroll
+            for (int n = 0; n < 8; n++) {
+                const float4* p = ((n >> 2) ? p1 : p0) + (n & 1) + FNJ * ((n >> 1) & 1);
+                const float4 a = p[0], b = p[NPL];
+                Wc[0][n] = a.x; Wc[1][n] = a.y; Wc[2][n] = a.z;
+                Hc[0][n] = b.x; Hc[1][n] = b.y; Hc[2][n] = b.z;
+                if (GEOM == GEOM_TERRAIN) {
+                    X0[n] = (n & 1) ? txb : txa;
+                    X1[n] = ((n >> 1) & 1) ? tyb : tya;
+                    X2[n] = a.w;
+                } else if (GEOM == GEOM_GENERAL) {
+                    X0[n] = a.w;
+                    X1[n] = b.w;
+                    X2[n] = p[2 * NPL].x;
+                }
+            }
+        }
+        // support-operator brackets; directions 0 and 1 in the two lanes
         float B[3][8];
-        float cnb[L::NDIR > 0 ? L::NDIR : 1][8];
+        float cnb[NDIR > 0 ? NDIR : 1][8];
         if (GEOM == GEOM_RECT) {
 #pragma unroll
             for (int a = 0; a < 3; a++)
 #pragma unroll
                 for (int t = 0; t < 8; t++) B[a][t] = A.br.bnc[a][t];
         } else {
-            float X0[8], X1[8], X2[8];
-            if (GEOM == GEOM_TERRAIN) {
-                const float xa = txa, xb = txb, ya = tya, yb = tyb;
-#pragma unroll
-                for (int n = 0; n < 8; n++) {
-                    X0[n] = (n & 1) ? xb : xa;
-                    X1[n] = ((n >> 1) & 1) ? yb : ya;
-                    X2[n] = NC(n, L::CO);
-                }
-            } else {
-#pragma unroll
-                for (int n = 0; n < 8; n++) {
-                    X0[n] = NC(n, L::CO);
-                    X1[n] = NC(n, L::CO + 1);
-                    X2[n] = NC(n, L::CO + 2);
-                }
-            }
-            // directions 0 and 1 in the two lanes: (xb, xc) = (y, z) and (z, x)
             F2 PB[8], PC[8], P[8], PN[8];
 #pragma unroll
             for (int n = 0; n < 8; n++) {
-                PB[n] = f2(X1[n], X2[n]);
-                PC[n] = f2(X2[n], X0[n]);
+                PB[n] = f2(X1[n], X2[n], nz);
+                PC[n] = f2(X2[n], X0[n], nz);
             }
             brackets_nc_g<F2>(PB, PC, P);
-            cell_cn_brackets_g<F2>(PB, PC, P, PN, f2(0.0f));
+            cell_cn_brackets_g<F2>(PB, PC, P, PN, f2(0.0f, nz));
 #pragma unroll
             for (int t = 0; t < 8; t++) {
-                B[0][t] = P[t].x;
-                B[1][t] = P[t].y;
-                cnb[0][t] = PN[t].x;
-                cnb[1][t] = PN[t].y;
+                B[0][t] = P[t].x();
+                B[1][t] = P[t].y();
+                cnb[0][t] = PN[t].x();
+                cnb[1][t] = PN[t].y();
             }
             if (GEOM == GEOM_TERRAIN) {
 #pragma unroll
                 for (int t = 0; t < 8; t++) B[2][t] = A.br.bnc[2][t];
             } else {
                 brackets_nc_g<float>(X0, X1, B[2]);
-                cell_cn_brackets_g<float>(X0, X1, B[2], cnb[L::NDIR - 1], 0.0f);
+                cell_cn_brackets_g<float>(X0, X1, B[2], cnb[NDIR - 1], 0.0f);
             }
         }
-        // strain: s[ic][id] = stencil8(w_ic, B[id]); (ic0, ic1) paired per
-        // iid, then ic2's first two directions paired and its last alone
-        float Wt[3][8];
+        float ed[3], eo[3], he[12];
 #pragma unroll
-        for (int ic = 0; ic < 3; ic++)
-#pragma unroll
-            for (int t = 0; t < 8; t++) Wt[ic][t] = NC(term_corner(t), ic);
-        float sg[3][3];
-        {
+        for (int i = 0; i < 12; i++) he[i] = 0.f;
+        const bool own = owncol && l >= L0;
+        if constexpr (F) {
+            // strain of an interior cell: s[ic][id] = stencil8(w_ic, B[id]);
+            // (ic0, ic1) paired per iid, ic2's first two directions paired
+            const F2 h2 = f2(h, nz);
+            float sg[3][3];
             F2 W01[8];
+            float W2v[8];
 #pragma unroll
-            for (int t = 0; t < 8; t++) W01[t] = f2(Wt[0][t], Wt[1][t]);
+            for (int t = 0; t < 8; t++) {
+                const int n = term_corner(t);
+                W01[t] = f2(Wc[0][n], Wc[1][n], nz);
+                W2v[t] = Wc[2][n];
+            }
 #pragma unroll
             for (int iid = 0; iid < 3; iid++) {
                 const int ia = (0 + iid + 1) % 3, ib = (1 + iid + 1) % 3;
                 F2 Bp[8];
 #pragma unroll
-                for (int t = 0; t < 8; t++) Bp[t] = f2(B[ia][t], B[ib][t]);
+                for (int t = 0; t < 8; t++) Bp[t] = f2(B[ia][t], B[ib][t], nz);
                 const F2 r = stencil8<F2>(W01, Bp, h2);
-                sg[0][ia] = r.x;
-                sg[1][ib] = r.y;
+                sg[0][ia] = r.x();
+                sg[1][ib] = r.y();
             }
-            F2 W22[8], Bp[8];
+            {
+                F2 W22[8], Bp[8];
 #pragma unroll
-            for (int t = 0; t < 8; t++) {
-                W22[t] = f2(Wt[2][t]);
-                Bp[t] = f2(B[0][t], B[1][t]);
+                for (int t = 0; t < 8; t++) {
+                    W22[t] = f2(W2v[t], nz);
+                    Bp[t] = f2(B[0][t], B[1][t], nz);
+                }
+                const F2 r = stencil8<F2>(W22, Bp, h2);
+                sg[2][0] = r.x();
+                sg[2][1] = r.y();
+                sg[2][2] = stencil8<float>(W2v, B[2], h);
             }
-            const F2 r = stencil8<F2>(W22, Bp, h2);
-            sg[2][0] = r.x;
-            sg[2][1] = r.y;
-            sg[2][2] = stencil8<float>(Wt[2], B[2], h);
+#pragma unroll
+            for (int i = 0; i < 3; i++) ed[i] = sg[i][i];
+            eo[0] = 0.5f * sg[1][2] + 0.5f * sg[2][1];
+            eo[1] = 0.5f * sg[0][2] + 0.5f * sg[2][0];
+            eo[2] = 0.5f * sg[0][1] + 0.5f * sg[1][0];
+        } else {
+            // region of the cell (stress.f90:141-248)
+            bool nearS[3], farS[3], anyS = false;
+            const int cc[3] = {J, K, l};
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                nearS[d] = cc[d] <= g.i1pml[d];
+                farS[d] = cc[d] >= g.i2pml[d] - 1;
+                anyS = anyS || nearS[d] || farS[d];
+            }
+            // PML cells that are not elastic-hourglass cells carry the viscous
+            // hourglass values dt hg2 yy hourglass_nc(v) in the hourglass
+            // slots (acceleration.f90:164-183)
+            bool inEc = true;
+#pragma unroll
+            for (int d = 0; d < 3; d++) inEc = inEc && cc[d] >= g.i1pml[d] && cc[d] <= g.i2pml[d] - 1;
+            const bool visc = A.hourglass && A.hgvisc && anyS && !inEc;
+            const float yv = A.dh2 * cur[3];
+#pragma unroll
+            for (int i = 0; i < 3; i++) { ed[i] = 0.f; eo[i] = 0.f; }
+#pragma unroll
+            for (int ic = 0; ic < 3; ic++) {
+                float W[8], U[8], V[8];
+#pragma unroll
+                for (int t = 0; t < 8; t++) {
+                    W[t] = Wc[ic][term_corner(t)];
+                    U[t] = 0.f;
+                    V[t] = 0.f;
+                }
+                if (anyS) {
+#pragma unroll
+                    for (int t = 0; t < 8; t++) {
+                        const int n = term_corner(t);
+                        const long long qn = g.idx(J + (n & 1), K + ((n >> 1) & 1), l + (n >> 2));
+                        U[t] = A.uin[ic][qn];
+                        V[t] = A.vin[ic][qn];
+                    }
+                }
+                if (visc) {
+                    float Vc[8], Vh[8];
+#pragma unroll
+                    for (int t = 0; t < 8; t++) Vc[term_corner(t)] = V[t];
+#pragma unroll
+                    for (int t = 0; t < 8; t++) Vh[t] = Vc[hg_corner(t)];
+#pragma unroll
+                    for (int iq = 0; iq < 4; iq++) he[3 * iq + ic] = yv * hg_sum(Vh, iq);
+                }
+#pragma unroll
+                for (int iid = 0; iid < 3; iid++) {
+                    const int id = (ic + iid + 1) % 3;
+                    float s;
+                    if (nearS[id] || farS[id]) {
+                        const float raw = stencil8(V, B[id], h);
+                        s = raw;
+                        const int c = cc[id];
+                        if (nearS[id]) {
+                            const int p = c + g.nnoff[id];
+                            const long long gi = slab_idx(g, id, A.sl.tg[id], c - g.i1cell[id], J, K, l, ic);
+                            s = A.pmlc[3 * g.npml + p - 1] * raw + A.pmlc[2 * g.npml + p - 1] * A.sl.g[id][gi];
+                            if (own) A.gout[id][gi] = s;
+                        }
+                        if (farS[id]) {
+                            const int p = g.nn[id] - c - g.nnoff[id];
+                            const long long gi = slab_idx(g, id, A.sl.tg[3 + id], g.i2cell[id] - c, J, K, l, ic);
+                            s = A.pmlc[3 * g.npml + p - 1] * raw + A.pmlc[2 * g.npml + p - 1] * A.sl.g[3 + id][gi];
+                            if (own) A.gout[3 + id][gi] = s;
+                        }
+                    } else if (anyS) {
+                        s = stencil8(U, B[id], h);
+                    } else {
+                        s = stencil8(W, B[id], h);
+                    }
+                    if (ic == id) ed[ic] = s;
+                    else if (ic < id) eo[3 - ic - id] = 0.5f * s;
+                    else eo[3 - ic - id] = eo[3 - ic - id] + 0.5f * s;
+                }
+            }
+            apply_inject(lpot, npot, A.pot, q, ed, eo);
         }
-        float ed[3], eo[3];
-#pragma unroll
-        for (int i = 0; i < 3; i++) ed[i] = sg[i][i];
-        eo[0] = 0.5f * sg[1][2] + 0.5f * sg[2][1];
-        eo[1] = 0.5f * sg[0][2] + 0.5f * sg[2][0];
-        eo[2] = 0.5f * sg[0][1] + 0.5f * sg[1][0];
         {
             const float lm = cur[0], m2 = 2.0f * cur[1];
             const float s1v = lm * (ed[0] + ed[1] + ed[2]);
 #pragma unroll
             for (int i = 0; i < 3; i++) { ed[i] = m2 * ed[i] + s1v; eo[i] = m2 * eo[i]; }
+        }
+        if constexpr (!F) apply_inject(lmom, nmom, A.mom, q, ed, eo);
+        {
             const float r = cur[2];
 #pragma unroll
             for (int i = 0; i < 3; i++) { ed[i] = ed[i] * r; eo[i] = eo[i] * r; }
         }
-        if (A.stats && owncol && l >= L0)
+        if (A.stats && own)
             st_w = fmaxn(st_w, (ed[0] * ed[0] + ed[1] * ed[1] + ed[2] * ed[2]) + 2.0f * (eo[0] * eo[0] + eo[1] * eo[1] + eo[2] * eo[2]));
-#pragma unroll
-        for (int i = 0; i < 3; i++) { cw[i * NCL] = ed[i]; cw[(3 + i) * NCL] = eo[i]; }
-        // elastic hourglass cell values, (ic0, ic1) paired
+        // elastic hourglass cell values (acceleration.f90:141-156)
         if (A.hourglass) {
-            const float y = cur[3];
-            F2 H01[8];
-            float H2[8];
+            bool inE = true;
+            if constexpr (!F) {
+                const int cc[3] = {J, K, l};
 #pragma unroll
-            for (int t = 0; t < 8; t++) {
-                const int n = hg_corner(t);
-                H01[t] = f2(NC(n, L::HG), NC(n, L::HG + 1));
-                H2[t] = NC(n, L::HG + 2);
+                for (int d = 0; d < 3; d++) inE = inE && cc[d] >= g.i1pml[d] && cc[d] <= g.i2pml[d] - 1;
             }
+            if (inE) {
+                const float y = cur[3];
+                F2 H01[8];
+                float H2v[8];
 #pragma unroll
-            for (int iq = 0; iq < 4; iq++) {
-                const F2 r = hg_sum<F2>(H01, iq) * f2(y);
-                cw[(6 + 3 * iq) * NCL] = r.x;
-                cw[(7 + 3 * iq) * NCL] = r.y;
-                cw[(8 + 3 * iq) * NCL] = hg_sum<float>(H2, iq) * y;
+                for (int t = 0; t < 8; t++) {
+                    const int n = hg_corner(t);
+                    H01[t] = f2(Hc[0][n], Hc[1][n], nz);
+                    H2v[t] = Hc[2][n];
+                }
+#pragma unroll
+                for (int iq = 0; iq < 4; iq++) {
+                    const F2 r = hg_sum<F2>(H01, iq) * f2(y, nz);
+                    he[3 * iq] = r.x();
+                    he[3 * iq + 1] = r.y();
+                    he[3 * iq + 2] = hg_sum<float>(H2v, iq) * y;
+                }
             }
-        } else {
-#pragma unroll
-            for (int i = 0; i < 12; i++) cw[(6 + i) * NCL] = 0.f;
         }
-#pragma unroll
-        for (int a = 0; a < L::NDIR; a++)
-#pragma unroll
-            for (int t = 0; t < 8; t++) cw[(18 + 8 * a + t) * NCL] = cnb[a][t];
-#undef NC
+        WRITE_CELL(cs, ed, eo, he, cnb);
     };
 
-    auto nodes_fast = [&](int l) {
+    // ---------------------------------------------------------------- node phase
+    // The eight cells of node (jn, kn, l) are cell positions p = cj + 2 ck + 4 cl
+    // at (J + cj, K + ck, l - 1 + cl); diff_cn term t sits at position
+    // pt(t), hourglass_cn term t at position ph(t).
+    auto nodes = [&](int l, auto fast_tag) {
+        constexpr bool F = decltype(fast_tag)::value;
         if (!outcol) return;
         const long long q = g.idx(jn, kn, l);
-        const float* c0 = cbase + ((l - 1) & 1) * (L::CELLF * NCL);  // cell plane l-1
-        const float* c1 = cbase + (l & 1) * (L::CELLF * NCL);        // cell plane l
-        // cell of diff_cn term t: (j-1|j, k-1|k, l-1|l) = thread cell + (t&1, t>>2)
-#define CC(t, f) ((((t) >> 1) & 1) ? c1 : c0)[(f) * NCL + ((t) & 1) + FJ * ((t) >> 2)]
-        const F2 h2 = f2(h);
-        float Fc[6][8];
+        const float4* c0 = sC + ((l - 1) & 1) * (NGC * NCL) + tid;  // cell plane l-1
+        const float4* c1 = sC + (l & 1) * (NGC * NCL) + tid;        // cell plane l
+        auto cpos = [&](int p) { return ((p >> 2) ? c1 : c0) + (p & 1) + FJ * ((p >> 1) & 1); };
+        auto pt = [](int t) { return (t & 1) + 2 * (t >> 2) + 4 * ((t >> 1) & 1); };
+        auto ph = [](int t) {
+            const int o = hg_corner(t);
+            return (1 - (o & 1)) + 2 * (1 - ((o >> 1) & 1)) + 4 * (1 - (o >> 2));
+        };
+        // stress (6) and divergence brackets by diff_cn term
+        float S[6][8], Bc[3][8];
 #pragma unroll
-        for (int c = 0; c < 6; c++)
+        for (int t = 0; t < 8; t++) {
+            const float4* cp = cpos(pt(t));
+            const float4 a = cp[0], b = cp[NCL];
+            S[0][t] = a.x; S[1][t] = a.y; S[2][t] = a.z; S[3][t] = a.w; S[4][t] = b.x; S[5][t] = b.y;
+            if (NDIR >= 2) {
+                const float2 bb = reinterpret_cast<const float2*>(cp + (5 + t / 2) * NCL)[t % 2];
+                Bc[0][t] = bb.x;
+                Bc[1][t] = bb.y;
+            }
+            if (NDIR == 3) Bc[2][t] = reinterpret_cast<const float*>(cp + (9 + t / 4) * NCL)[t % 4];
+            if (GEOM == GEOM_RECT)
 #pragma unroll
-            for (int t = 0; t < 8; t++) Fc[c][t] = CC(t, c);
-        float Bc[3][8];
-#pragma unroll
-        for (int id = 0; id < 3; id++)
-#pragma unroll
-            for (int t = 0; t < 8; t++)
-                Bc[id][t] = (GEOM == GEOM_RECT || (GEOM == GEOM_TERRAIN && id == 2)) ? A.br.bcn[id][t]
-                                                                                     : CC(t, 18 + 8 * id + t);
-        // f[ic] = sum over iid of stencil8(sigma(ic, id), Bc[id]), id = (ic + iid) % 3
-        F2 f01;
-        float f2s;
-        {
+                for (int id = 0; id < 3; id++) Bc[id][t] = A.br.bcn[id][t];
+            if (GEOM == GEOM_TERRAIN) Bc[2][t] = A.br.bcn[2][t];
+        }
+        float f[3];
+        if constexpr (F) {
+            // f[ic] = sum over iid of stencil8(sigma(ic, id), Bc[id]), id = (ic + iid) % 3;
+            // (ic0, ic1) paired per iid, ic2's first two terms paired
+            const F2 h2 = f2(h, nz);
+            F2 f01;
 #pragma unroll
             for (int iid = 0; iid < 3; iid++) {
                 const int ia = iid, ib = (1 + iid) % 3;
@@ -609,89 +546,31 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
                 F2 Fp[8], Bp[8];
 #pragma unroll
                 for (int t = 0; t < 8; t++) {
-                    Fp[t] = f2(Fc[ca][t], Fc[cb][t]);
-                    Bp[t] = f2(Bc[ia][t], Bc[ib][t]);
+                    Fp[t] = f2(S[ca][t], S[cb][t], nz);
+                    Bp[t] = f2(Bc[ia][t], Bc[ib][t], nz);
                 }
                 const F2 r = stencil8<F2>(Fp, Bp, h2);
                 f01 = iid == 0 ? r : f01 + r;
             }
-            // ic 2: (id 2, id 0) paired, then id 1
             F2 Fp[8], Bp[8];
 #pragma unroll
             for (int t = 0; t < 8; t++) {
-                Fp[t] = f2(Fc[2][t], Fc[4][t]);
-                Bp[t] = f2(Bc[2][t], Bc[0][t]);
+                Fp[t] = f2(S[2][t], S[4][t], nz);
+                Bp[t] = f2(Bc[2][t], Bc[0][t], nz);
             }
             const F2 r = stencil8<F2>(Fp, Bp, h2);
-            f2s = r.x + r.y;
-            f2s = f2s + stencil8<float>(Fc[3], Bc[1], h);
-        }
-        if (A.hourglass) {
-#define CH(t, f) ((hg_corner(t) >> 2) ? c0 : c1)[(f) * NCL + (1 - (hg_corner(t) & 1)) + FJ * (1 - ((hg_corner(t) >> 1) & 1))]
+            f[2] = r.x() + r.y();
+            f[2] = f[2] + stencil8<float>(S[3], Bc[1], h);
+            f[0] = f01.x();
+            f[1] = f01.y();
+        } else {
 #pragma unroll
-            for (int iq = 0; iq < 4; iq++) {
-                F2 H01[8];
-                float H2[8];
+            for (int ic = 0; ic < 3; ic++) {
 #pragma unroll
-                for (int t = 0; t < 8; t++) {
-                    H01[t] = f2(CH(t, 6 + 3 * iq), CH(t, 7 + 3 * iq));
-                    H2[t] = CH(t, 8 + 3 * iq);
-                }
-                f01 = f01 - hg_sum<F2>(H01, iq);
-                f2s = f2s - hg_sum<float>(H2, iq);
-            }
-#undef CH
-        }
-#undef CC
-        const float m = cur[4];
-        float f[3] = {f01.x * m, f01.y * m, f2s * m};
-        const float u0 = uv[0], u1 = uv[1], u2 = uv[2], v0 = uv[3], v1 = uv[4], v2 = uv[5];
-        if (A.stats) {
-            st_a = fmaxn(st_a, f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
-            st_v = fmaxn(st_v, v0 * v0 + v1 * v1 + v2 * v2);
-            st_u = fmaxn(st_u, u0 * u0 + u1 * u1 + u2 * u2);
-        }
-        if (A.aout[0])
-#pragma unroll
-            for (int i = 0; i < 3; i++) A.aout[i][q] = f[i];
-        if (A.fold) {
-            // leapfrog update of the next step (time_integration.f90:32-35)
-            float a, b;
-            a = v0 + dt * f[0]; b = u0 + dt * a; A.vout[0][q] = a; A.uout[0][q] = b;
-            a = v1 + dt * f[1]; b = u1 + dt * a; A.vout[1][q] = a; A.uout[1][q] = b;
-            a = v2 + dt * f[2]; b = u2 + dt * a; A.vout[2][q] = a; A.uout[2][q] = b;
-        }
-    };
-
-    // ---------------------------------------------------------------- node phase
-    auto nodes = [&](int l, auto fast_tag) {
-        constexpr bool F = decltype(fast_tag)::value;
-        if (!outcol) return;
-        const long long q = g.idx(jn, kn, l);
-        // cells of diff_cn term t: (j-1|j, k-1|k, l-1|l)
-        int ci[8], cs[8];
-#pragma unroll
-        for (int t = 0; t < 8; t++) {
-            const int oj = (t & 1) ? 0 : -1, ok = (t >> 2) ? 0 : -1, ol = ((t >> 1) & 1) ? 0 : -1;
-            ci[t] = (tx + 1 + oj) + FJ * (ty + 1 + ok);
-            cs[t] = (l + ol) & 1;
-        }
-        float f[3];
-#pragma unroll
-        for (int ic = 0; ic < 3; ic++) {
-#pragma unroll
-            for (int iid = 0; iid < 3; iid++) {
-                const int id = (ic + iid) % 3;
-                const int comp = ic == id ? ic : 3 + (3 - ic - id);
-                float Fv[8], B[8];
-#pragma unroll
-                for (int t = 0; t < 8; t++) {
-                    Fv[t] = CELL(cs[t], comp, ci[t]);
-                    if (GEOM == GEOM_RECT || (GEOM == GEOM_TERRAIN && id == 2)) B[t] = A.br.bcn[id][t];
-                    else B[t] = CELL(cs[t], 18 + 8 * id + t, ci[t]);
-                }
-                float s = stencil8(Fv, B, h);
-                if constexpr (!F) {
+                for (int iid = 0; iid < 3; iid++) {
+                    const int id = (ic + iid) % 3;
+                    const int comp = ic == id ? ic : 3 + (3 - ic - id);
+                    float s = stencil8(S[comp], Bc[id], h);
                     const int c = id == 0 ? jn : id == 1 ? kn : l;
                     if (c <= g.i1pml[id]) {
                         const int p = c + g.nnoff[id];
@@ -705,8 +584,8 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
                         s = A.pmlc[g.npml + p - 1] * s + A.pmlc[p - 1] * *P;
                         *P = *P + dt * s;
                     }
+                    f[ic] = iid == 0 ? s : f[ic] + s;
                 }
-                f[ic] = iid == 0 ? s : f[ic] + s;
             }
         }
         if (A.hourglass) {
@@ -716,23 +595,40 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
 #pragma unroll
                 for (int d = 0; d < 3; d++) ne = ne && cn_[d] >= g.i1pml[d] + 1 && cn_[d] <= g.i2pml[d] - 1;
             }
+            // hourglass values of mode iq by hourglass_cn term: (x, y) pair and z
+#define HVALS(iq, hA, hB)                                                      \
+    _Pragma("unroll") for (int t = 0; t < 8; t++) {                            \
+        const float4* cp_ = cpos(ph(t));                                       \
+        if ((iq) == 0) {                                                       \
+            const float4 b_ = cp_[NCL];                                        \
+            hA[t] = f2(b_.z, b_.w, nz);                                        \
+            hB[t] = cp_[3 * NCL].z;                                            \
+        } else if ((iq) == 1) {                                                \
+            const float4 b_ = cp_[2 * NCL];                                    \
+            hA[t] = f2(b_.x, b_.y, nz);                                        \
+            hB[t] = cp_[3 * NCL].w;                                            \
+        } else if ((iq) == 2) {                                                \
+            const float4 b_ = cp_[2 * NCL];                                    \
+            hA[t] = f2(b_.z, b_.w, nz);                                        \
+            hB[t] = cp_[4 * NCL].x;                                            \
+        } else {                                                               \
+            const float4 b_ = cp_[3 * NCL];                                    \
+            hA[t] = f2(b_.x, b_.y, nz);                                        \
+            hB[t] = cp_[4 * NCL].y;                                            \
+        }                                                                      \
+    }
             if (ne) {
-                int hi[8], hs[8];
+                F2 f01 = f2(f[0], f[1], nz);
 #pragma unroll
-                for (int t = 0; t < 8; t++) {
-                    const int o = hg_corner(t);
-                    hi[t] = (tx + 1 - (o & 1)) + FJ * (ty + 1 - ((o >> 1) & 1));
-                    hs[t] = (l - (o >> 2)) & 1;
+                for (int iq = 0; iq < 4; iq++) {
+                    F2 hA[8];
+                    float hB[8];
+                    HVALS(iq, hA, hB);
+                    f01 = f01 - hg_sum<F2>(hA, iq);
+                    f[2] = f[2] - hg_sum<float>(hB, iq);
                 }
-#pragma unroll
-                for (int iq = 0; iq < 4; iq++)
-#pragma unroll
-                    for (int ic = 0; ic < 3; ic++) {
-                        float H[8];
-#pragma unroll
-                        for (int t = 0; t < 8; t++) H[t] = CELL(hs[t], 6 + 3 * iq + ic, hi[t]);
-                        f[ic] = f[ic] - hg_sum(H, iq);
-                    }
+                f[0] = f01.x();
+                f[1] = f01.y();
             } else if constexpr (!F) {
                 if (A.hgvisc) {
                     // viscous-only hourglass in the PML (acceleration.f90:164-199):
@@ -740,13 +636,11 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
                     // hold their viscous values in the hourglass slots, cells
                     // that are also elastic-hourglass cells (the layer next to
                     // the elastic region) are evaluated here from v
-                    int hi[8], hs[8], kind[8];
+                    int kind[8];
                     float yc[8];
 #pragma unroll
                     for (int t = 0; t < 8; t++) {
                         const int o = hg_corner(t);
-                        hi[t] = (tx + 1 - (o & 1)) + FJ * (ty + 1 - ((o >> 1) & 1));
-                        hs[t] = (l - (o >> 2)) & 1;
                         const int Jc = jn - (o & 1), Kc = kn - ((o >> 1) & 1), Lc = l - (o >> 2);
                         const bool real = Jc >= g.i1cell[0] && Jc <= g.i2cell[0] && Kc >= g.i1cell[1] &&
                                           Kc <= g.i2cell[1] && Lc >= g.i1cell[2] && Lc <= g.i2cell[2];
@@ -757,39 +651,42 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
                         kind[t] = !(real && slab) ? 0 : inEc ? 2 : 1;
                         yc[t] = kind[t] == 2 ? A.dh2 * A.yy[g.idx(Jc, Kc, Lc)] : 0.f;
                     }
-#pragma unroll 1
-                    for (int ic = 0; ic < 3; ic++) {
-                        float Hq[4][8];
+#pragma unroll
+                    for (int iq = 0; iq < 4; iq++) {
+                        F2 hA[8];
+                        float hB[8];
+                        HVALS(iq, hA, hB);
+                        float Hq[3][8];
 #pragma unroll
                         for (int t = 0; t < 8; t++) {
-                            if (kind[t] == 1) {
+                            Hq[0][t] = kind[t] == 1 ? hA[t].x() : 0.f;
+                            Hq[1][t] = kind[t] == 1 ? hA[t].y() : 0.f;
+                            Hq[2][t] = kind[t] == 1 ? hB[t] : 0.f;
+                        }
 #pragma unroll
-                                for (int iq = 0; iq < 4; iq++) Hq[iq][t] = CELL(hs[t], 6 + 3 * iq + ic, hi[t]);
-                            } else if (kind[t] == 2) {
+                        for (int t = 0; t < 8; t++) {
+                            if (kind[t] == 2) {
                                 const int o = hg_corner(t);
-                                float Vc[8];
 #pragma unroll
-                                for (int m = 0; m < 8; m++) {
-                                    const int n = hg_corner(m);
-                                    const int dj = (n & 1) - (o & 1), dk = ((n >> 1) & 1) - ((o >> 1) & 1),
-                                              dl = (n >> 2) - (o >> 2);
-                                    Vc[m] = A.vin[ic][g.idx(jn + dj, kn + dk, l + dl)];
+                                for (int ic = 0; ic < 3; ic++) {
+                                    float Vc[8];
+#pragma unroll
+                                    for (int m = 0; m < 8; m++) {
+                                        const int n = hg_corner(m);
+                                        const int dj = (n & 1) - (o & 1), dk = ((n >> 1) & 1) - ((o >> 1) & 1),
+                                                  dl = (n >> 2) - (o >> 2);
+                                        const float* vp = ic == 0 ? A.vin[0] : ic == 1 ? A.vin[1] : A.vin[2];
+                                        Vc[m] = vp[g.idx(jn + dj, kn + dk, l + dl)];
+                                    }
+                                    const float hv = yc[t] * hg_sum(Vc, iq);
+                                    if (ic == 0) Hq[0][t] = hv;
+                                    else if (ic == 1) Hq[1][t] = hv;
+                                    else Hq[2][t] = hv;
                                 }
-#pragma unroll
-                                for (int iq = 0; iq < 4; iq++) Hq[iq][t] = yc[t] * hg_sum(Vc, iq);
-                            } else {
-#pragma unroll
-                                for (int iq = 0; iq < 4; iq++) Hq[iq][t] = 0.f;
                             }
                         }
-                        float fi = f[0];
-                        if (ic == 1) fi = f[1];
-                        if (ic == 2) fi = f[2];
 #pragma unroll
-                        for (int iq = 0; iq < 4; iq++) fi = fi - hg_sum(Hq[iq], iq);
-                        if (ic == 0) f[0] = fi;
-                        if (ic == 1) f[1] = fi;
-                        if (ic == 2) f[2] = fi;
+                        for (int ic = 0; ic < 3; ic++) f[ic] = f[ic] - hg_sum(Hq[ic], iq);
                     }
                 }
             }
@@ -829,6 +726,7 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
 
     // ---------------------------------------------------------------- stream
     // ring: planes L0-1, L0, L0+1; staged: L0+2 in flight
+    constexpr std::integral_constant<bool, FASTK> path{};
 #pragma unroll 1
     for (int p = -1; p <= 1; p++) {
         fetch(L0 + p);
@@ -840,20 +738,17 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
     fetch(L0 + 2);
     stat_load(L0 - 1, cur);
     uv_load(L0, uv);
-    if constexpr (FASTK) cells_fast(L0 - 1);
-    else cells(L0 - 1, std::false_type{});
+    cells(L0 - 1, path);
     stat_load(L0, cur);
 #pragma unroll 1
     for (int l = L0; l <= L1; l++) {
-        if constexpr (FASTK) cells_fast(l);
-        else cells(l, std::false_type{});
+        cells(l, path);
         float nxt[5], nuv[6];
         stat_load(l + 1, nxt);
         cp_async_wait_all();
         __syncthreads();  // cell plane l complete, staged plane l+2 landed
         store((l + 2) % 3);
-        if constexpr (FASTK) nodes_fast(l);
-        else nodes(l, std::false_type{});
+        nodes(l, path);
         uv_load(l + 1, nuv);
         __syncthreads();  // ring slot l+2 complete, staging and cell slot l-1 free
         fetch(l + 3);
@@ -870,8 +765,8 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
         bmax(A.red + 3, st_w);
     }
 #undef RAW
-#undef NODE
-#undef CELL
+#undef WRITE_CELL
+#undef HVALS
 }
 
 // Work decomposition of a fused step, fixed by the mesh: interior tile
@@ -1028,6 +923,7 @@ void launch_fused(Solver& s, const InjectList& pot, const InjectList& mom, const
     A.lf1 = P.lf1;
     A.segl = P.lf1 - P.lf0 + 1;
     A.items = P.d_items;
+    A.negzero = -0.0f;
 
     // general items of this step: the fixed list, plus whole columns for
     // interior columns holding a point source

@@ -147,6 +147,7 @@ struct StepArgs {
     // general kernel: work items (bx, by, first plane, last plane)
     int bx0, by0, lf0, lf1;
     const int4* items;
+    float negzero;  // -0.0, the addend of packed products (pair.cuh)
 };
 
 // Device state of one handle.

@@ -155,12 +155,50 @@ def case_wave(shape=(40, 36, 30), nt=24):
 
 def wave_inputs(path, shape=(40, 36, 30)):
     import bench
-    inp = os.path.join(os.path.dirname(path), 'wave_inputs')
+    inp = os.path.join(os.path.dirname(path), 'wave_inputs_%dx%dx%d' % tuple(shape))
     bench.make_inputs(shape, inp, use_torch=False)
     for f in ('rho.bin', 'vp.bin', 'vs.bin', 'z.bin'):
         dst = os.path.join(path, f)
         if not os.path.exists(dst):
             os.symlink(os.path.join(inp, f), dst)
+
+
+def case_interior(shape=(72, 40, 28), nt=14, gridnoise=0.0):
+    """A mesh large enough to hold interior tiles, so the fused interior
+    kernel runs next to the PML kernel; one moment source inside an interior
+    tile column and one inside the PML, viscous hourglass, every step fused."""
+    nx, ny, nz = shape
+    prm = {
+        'shape': [nx, ny, nz, nt], 'delta': [100.0, 100.0, 100.0, 0.008],
+        'rho': [2670.0], 'vp': [6000.0], 'vs': [3464.0], 'gam': [0.2],
+        'hourglass': [1.0, 2.0], 'bc1': ['pml', 'pml', 'free'], 'bc2': ['pml'] * 3, 'npml': 4,
+        'itstats': 3, 'itio': 10, 'gridnoise': gridnoise,
+    }
+    for f, v in (('mxx', 1e16), ('myy', 8e15), ('mzz', 1.2e16), ('mxy', -3e15)):
+        prm[f] = [([45.3, 21.6, 13.2, []], '.', v, 'brune', 0.1),
+                  ([2.5, 20.5, 6.5, []], '.', 0.5 * v, 'brune', 0.1)]
+    for f in 'vx', 'vy', 'vz':
+        prm[f] = [([[], 20, [], [None, None, 4]], '=>', 'snap-%s.bin' % f)]
+        for r, (x, y, z) in enumerate([(40.0, 18.0, 0.0), (50.5, 25.25, 10.0), (3.0, 5.0, 20.0)]):
+            prm[f] += [([x, y, z, []], '.>', 'rec%d-%s.bin' % (r, f))]
+    return prm
+
+
+def case_interior_noise():
+    """The interior-tile case on a random (general) mesh."""
+    return case_interior(gridnoise=0.1)
+
+
+WAVE_INTERIOR = (80, 48, 32)
+
+
+def case_interior_wave():
+    """The benchmark workload (terrain mesh) at a size with interior tiles."""
+    return case_wave(WAVE_INTERIOR, nt=16)
+
+
+def interior_wave_inputs(path):
+    wave_inputs(path, WAVE_INTERIOR)
 
 
 CASES = {
@@ -174,8 +212,11 @@ CASES = {
     'visc': case_visc,
     'noise': case_noise,
     'wave': case_wave,
+    'interior': case_interior,
+    'interior_noise': case_interior_noise,
+    'interior_wave': case_interior_wave,
 }
-INPUTS = {'wave': wave_inputs}
+INPUTS = {'wave': wave_inputs, 'interior_wave': interior_wave_inputs}
 
 
 def stage(prm, path, realsize=4, inputs=None):
