@@ -43,8 +43,16 @@
 #include "sord.cuh"
 #include "stencil.cuh"
 
+// SORD_FAST_PAIRED selects packed f32x2 evaluation (pair.cuh) of the
+// interior kernel's independent stencils; 0 evaluates them one at a time.
+// Both give bit-identical results.
+#ifndef SORD_FAST_PAIRED
+#define SORD_FAST_PAIRED 0
+#endif
+
 namespace sordgpu {
 
+constexpr bool kPaired = SORD_FAST_PAIRED != 0;
 constexpr int FJ = 32, FK = 8;                // cell tile = threads
 constexpr int FNJ = FJ + 1, FNK = FK + 1;     // node region of a plane
 constexpr int FOJ = FJ - 1, FOK = FK - 1;     // output nodes of a tile
@@ -111,10 +119,568 @@ __device__ __forceinline__ void cp_async4(float* smem, const float* gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-// FASTK: interior tile columns and planes (A.bx0, A.by0, A.lf0..A.lf1), fast
-// path only; otherwise the work items A.items, general path only.
+// Shared-memory layout of the PML-shell kernel: plain per-field planes
+// (node ring: w(3), hourglass input(3), coordinates; cell ring: stress(6),
+// hourglass(12), divergence brackets(8 per direction)).
+template <int GEOM>
+struct LayS {
+    static constexpr int NCOORD = GEOM == GEOM_RECT ? 0 : GEOM == GEOM_TERRAIN ? 1 : 3;
+    static constexpr int RAWF = 7 + NCOORD;   // staged plane: u(3) v(3) gam coords
+    static constexpr int NODEF = 6 + NCOORD;  // ring: w = u + gam v (3), hg1 u + dt hg2 v (3), coords
+    static constexpr int HG = 3;              // first hourglass-input field
+    static constexpr int CO = 6;              // first coordinate field
+    static constexpr int NDIR = GEOM == GEOM_RECT ? 0 : GEOM == GEOM_TERRAIN ? 2 : 3;
+    static constexpr int CELLF = 6 + 12 + 8 * NDIR;  // stress, hourglass, divergence brackets
+    static constexpr size_t bytes = sizeof(float) * (size_t)(NPL * RAWF + 3 * NPL * NODEF + 2 * NCL * CELLF);
+};
+
+
+// PML-shell kernel: the work items A.items (tile column, first and last node
+// plane), with every PML, boundary and point-source term of the step.
+template <int GEOM>
+__global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_shell(StepArgs A) {
+    constexpr bool FASTK = false;
+    using L = LayS<GEOM>;
+    extern __shared__ float sm[];
+    float* sR = sm;                          // [RAWF][NPL] staged plane
+    float* sN = sR + L::RAWF * NPL;          // [3 slots][NODEF][NPL]
+    float* sC = sN + 3 * L::NODEF * NPL;     // [2 slots][CELLF][NCL]
+#define RAW(f, i) sR[(f) * NPL + (i)]
+#define NODE(slot, f, i) sN[((slot) * L::NODEF + (f)) * NPL + (i)]
+#define CELL(slot, f, i) sC[((slot) * L::CELLF + (f)) * NCL + (i)]
+    const Geom& g = A.g;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + FJ * ty;
+    int bx, by, L0, L1;
+    if (FASTK) {
+        bx = A.bx0 + blockIdx.x;
+        by = A.by0 + blockIdx.y;
+        L0 = A.lf0 + blockIdx.z * A.segl;
+        L1 = min(L0 + A.segl - 1, A.lf1);
+    } else {
+        const int4 it = A.items[blockIdx.x];
+        bx = it.x;
+        by = it.y;
+        L0 = it.z;
+        L1 = it.w;
+    }
+    const int j0 = g.i1node[0] + bx * FOJ, k0 = g.i1node[1] + by * FOK;
+    const int J = j0 - 1 + tx, K = k0 - 1 + ty;      // this thread's cell column
+    const int jn = j0 + tx, kn = k0 + ty;            // this thread's node column
+    const bool outcol = tx < FOJ && ty < FOK && jn <= g.i2node[0] && kn <= g.i2node[1];
+    const bool cellcol = J >= g.i1cell[0] && J <= g.i2cell[0] && K >= g.i1cell[1] && K <= g.i2cell[1];
+    const bool owncol = J >= j0 && K >= k0;
+    const float h = g.h, dt = g.dt;
+    float st_a = 0.f, st_v = 0.f, st_u = 0.f, st_w = 0.f;
+    // terrain meshes: this thread's cell column's x (j, j+1) and y (k, k+1)
+    float txa = 0.f, txb = 0.f, tya = 0.f, tyb = 0.f;
+    if (GEOM == GEOM_TERRAIN && cellcol) {
+        txa = A.x1d[J - 1];
+        txb = A.x1d[J];
+        tya = A.y1d[K - 1];
+        tyb = A.y1d[K];
+    }
+
+    // point injections that fall inside this block (cells / nodes it computes)
+    __shared__ Inject lpot[kLocalInject], lmom[kLocalInject], lfrc[kLocalInject];
+    __shared__ int lcnt[3];
+    // A fast-kernel block whose (j, k) box holds a point source of this step
+    // leaves that column to the general kernel (the host lists it there).
+    const int gl1 = FASTK ? 0 : L0 - 1, gl2 = FASTK ? g.nm[2] + 1 : L1;
+    gather_inject(A.pot, lpot, &lcnt[0], g, j0 - 1, j0 + FOJ - 1, k0 - 1, k0 + FOK - 1, gl1, gl2);
+    gather_inject(A.mom, lmom, &lcnt[1], g, j0 - 1, j0 + FOJ - 1, k0 - 1, k0 + FOK - 1, gl1, gl2);
+    gather_inject(A.force, lfrc, &lcnt[2], g, j0, j0 + FOJ - 1, k0, k0 + FOK - 1, FASTK ? gl1 : L0, gl2);
+    __syncthreads();
+    const int npot = lcnt[0], nmom = lcnt[1], nfrc = lcnt[2];
+    if (FASTK && (npot != 0 || nmom != 0 || nfrc != 0)) return;
+
+    // ---------------------------------------------------------------- loads
+    // stage node plane l (u, v, gam, coordinates) into sR asynchronously
+    auto fetch = [&](int l) {
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+            const int n = tid + r * NTH;
+            if (n < NPL) {
+                const int nj = n % FNJ, nk = n / FNJ;
+                const int j = j0 - 1 + nj, k = k0 - 1 + nk;
+                const bool ok = j <= g.nm[0] && k <= g.nm[1] && l >= 1 && l <= g.nm[2];
+                if (ok) {
+                    const long long q = g.idx(j, k, l);
+#pragma unroll
+                    for (int c = 0; c < 3; c++) {
+                        cp_async4(&RAW(c, n), A.uin[c] + q);
+                        cp_async4(&RAW(3 + c, n), A.vin[c] + q);
+                    }
+                    cp_async4(&RAW(6, n), A.gam + q);
+                    if (GEOM == GEOM_TERRAIN) cp_async4(&RAW(7, n), A.x[2] + q);
+                    if (GEOM == GEOM_GENERAL)
+#pragma unroll
+                        for (int c = 0; c < 3; c++) cp_async4(&RAW(7 + c, n), A.x[c] + q);
+                } else {
+#pragma unroll
+                    for (int f = 0; f < L::RAWF; f++) RAW(f, n) = 0.f;
+                }
+            }
+        }
+        cp_async_commit();
+    };
+    // staged plane -> ring slot: w1 = u + gam * v (time_integration.f90:36)
+    // and the hourglass input hg1 u + dt hg2 v (acceleration.f90:141)
+    auto store = [&](int slot) {
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+            const int n = tid + r * NTH;
+            if (n < NPL) {
+                const float gm = RAW(6, n);
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const float u = RAW(c, n), v = RAW(3 + c, n);
+                    NODE(slot, c, n) = u + gm * v;
+                    NODE(slot, L::HG + c, n) = A.hg1 * u + A.dh2 * v;
+                }
+#pragma unroll
+                for (int f = 0; f < L::NCOORD; f++) NODE(slot, L::CO + f, n) = RAW(7 + f, n);
+            }
+        }
+    };
+
+    // per-plane statics of this thread's cell (lam, mu, 1/V, yy) and node
+    // (mass ratio), loaded one plane ahead of their use
+    float cur[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+    auto stat_load = [&](int l, float* o) {
+        const bool cv = cellcol && l >= g.i1cell[2] && l <= g.i2cell[2];
+        const long long qc = cv ? g.idx(J, K, l) : 0;
+        o[0] = cv ? A.lam[qc] : 0.f;
+        o[1] = cv ? A.mu[qc] : 0.f;
+        o[2] = cv ? A.vc[qc] : 0.f;
+        o[3] = cv ? A.yy[qc] : 0.f;
+        const bool nv = outcol && l >= g.i1node[2] && l <= g.i2node[2];
+        o[4] = nv ? A.mr[g.idx(jn, kn, l)] : 0.f;
+    };
+    // this thread's node u, v (for the update and statistics), one plane ahead
+    float uv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    auto uv_load = [&](int l, float* o) {
+        const bool nv = outcol && l >= g.i1node[2] && l <= g.i2node[2];
+        const long long q = nv ? g.idx(jn, kn, l) : 0;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            o[c] = nv ? A.uin[c][q] : 0.f;
+            o[3 + c] = nv ? A.vin[c][q] : 0.f;
+        }
+    };
+
+    // ---------------------------------------------------------------- cell phase
+    auto cells = [&](int l, auto fast_tag) {
+        constexpr bool F = decltype(fast_tag)::value;
+        const int cs = l & 1;
+        const bool valid = F || (cellcol && l >= g.i1cell[2] && l <= g.i2cell[2]);
+        float ed[3] = {0.f, 0.f, 0.f}, eo[3] = {0.f, 0.f, 0.f};
+        float he[12];
+#pragma unroll
+        for (int i = 0; i < 12; i++) he[i] = 0.f;
+        float cnb[L::NDIR > 0 ? L::NDIR : 1][8];
+        if (valid) {
+            const long long q = g.idx(J, K, l);
+            const int s0 = l % 3, s1 = (l + 1) % 3;
+            int ni[8], ns[8];
+#pragma unroll
+            for (int n = 0; n < 8; n++) {
+                ni[n] = (tx + (n & 1)) + FNJ * (ty + ((n >> 1) & 1));
+                ns[n] = (n >> 2) ? s1 : s0;
+            }
+            float B[3][8];
+            if (GEOM == GEOM_RECT) {
+#pragma unroll
+                for (int a = 0; a < 3; a++)
+#pragma unroll
+                    for (int t = 0; t < 8; t++) B[a][t] = A.br.bnc[a][t];
+            } else {
+                float X[3][8];
+                if (GEOM == GEOM_TERRAIN) {
+                    const float xa = txa, xb = txb, ya = tya, yb = tyb;
+#pragma unroll
+                    for (int n = 0; n < 8; n++) {
+                        X[0][n] = (n & 1) ? xb : xa;
+                        X[1][n] = ((n >> 1) & 1) ? yb : ya;
+                        X[2][n] = NODE(ns[n], L::CO, ni[n]);
+                    }
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 3; c++)
+#pragma unroll
+                        for (int n = 0; n < 8; n++) X[c][n] = NODE(ns[n], L::CO + c, ni[n]);
+                }
+#pragma unroll
+                for (int a = 0; a < L::NDIR; a++) {
+                    brackets_nc(X, a, B[a]);
+                    cell_cn_brackets(X, a, B[a], cnb[a]);
+                }
+                if (GEOM == GEOM_TERRAIN)
+#pragma unroll
+                    for (int t = 0; t < 8; t++) B[2][t] = A.br.bnc[2][t];
+            }
+            const bool own = owncol && l >= L0;
+            if constexpr (F) {
+                // strain of an interior cell: gradients of w = u + gam v
+#pragma unroll
+                for (int ic = 0; ic < 3; ic++) {
+                    float W[8];
+#pragma unroll
+                    for (int t = 0; t < 8; t++) {
+                        const int n = term_corner(t);
+                        W[t] = NODE(ns[n], ic, ni[n]);
+                    }
+#pragma unroll
+                    for (int iid = 0; iid < 3; iid++) {
+                        const int id = (ic + iid + 1) % 3;
+                        const float s = stencil8(W, B[id], h);
+                        if (ic == id) ed[ic] = s;
+                        else if (ic < id) eo[3 - ic - id] = 0.5f * s;
+                        else eo[3 - ic - id] = eo[3 - ic - id] + 0.5f * s;
+                    }
+                }
+            } else {
+                // region of the cell (stress.f90:141-248)
+                bool nearS[3], farS[3], anyS = false;
+                const int cc[3] = {J, K, l};
+#pragma unroll
+                for (int d = 0; d < 3; d++) {
+                    nearS[d] = cc[d] <= g.i1pml[d];
+                    farS[d] = cc[d] >= g.i2pml[d] - 1;
+                    anyS = anyS || nearS[d] || farS[d];
+                }
+                // PML cells that are not elastic-hourglass cells carry the
+                // viscous hourglass values dt hg2 yy hourglass_nc(v) in the
+                // hourglass slots (acceleration.f90:164-183)
+                bool inEc = true;
+#pragma unroll
+                for (int d = 0; d < 3; d++) inEc = inEc && cc[d] >= g.i1pml[d] && cc[d] <= g.i2pml[d] - 1;
+                const bool visc = A.hourglass && A.hgvisc && anyS && !inEc;
+                const float yv = A.dh2 * cur[3];
+#pragma unroll
+                for (int ic = 0; ic < 3; ic++) {
+                    float W[8], U[8], V[8];
+#pragma unroll
+                    for (int t = 0; t < 8; t++) {
+                        const int n = term_corner(t);
+                        W[t] = NODE(ns[n], ic, ni[n]);
+                        U[t] = 0.f;
+                        V[t] = 0.f;
+                    }
+                    if (anyS) {
+#pragma unroll
+                        for (int t = 0; t < 8; t++) {
+                            const int n = term_corner(t);
+                            const long long qn = g.idx(J + (n & 1), K + ((n >> 1) & 1), l + (n >> 2));
+                            U[t] = A.uin[ic][qn];
+                            V[t] = A.vin[ic][qn];
+                        }
+                    }
+                    if (visc) {
+                        float Vc[8], Vh[8];
+#pragma unroll
+                        for (int t = 0; t < 8; t++) Vc[term_corner(t)] = V[t];
+#pragma unroll
+                        for (int t = 0; t < 8; t++) Vh[t] = Vc[hg_corner(t)];
+#pragma unroll
+                        for (int iq = 0; iq < 4; iq++) he[3 * iq + ic] = yv * hg_sum(Vh, iq);
+                    }
+#pragma unroll
+                    for (int iid = 0; iid < 3; iid++) {
+                        const int id = (ic + iid + 1) % 3;
+                        float s;
+                        if (nearS[id] || farS[id]) {
+                            const float raw = stencil8(V, B[id], h);
+                            s = raw;
+                            const int c = cc[id];
+                            if (nearS[id]) {
+                                const int p = c + g.nnoff[id];
+                                const long long gi = slab_idx(g, id, A.sl.tg[id], c - g.i1cell[id], J, K, l, ic);
+                                s = A.pmlc[3 * g.npml + p - 1] * raw + A.pmlc[2 * g.npml + p - 1] * A.sl.g[id][gi];
+                                if (own) A.gout[id][gi] = s;
+                            }
+                            if (farS[id]) {
+                                const int p = g.nn[id] - c - g.nnoff[id];
+                                const long long gi = slab_idx(g, id, A.sl.tg[3 + id], g.i2cell[id] - c, J, K, l, ic);
+                                s = A.pmlc[3 * g.npml + p - 1] * raw + A.pmlc[2 * g.npml + p - 1] * A.sl.g[3 + id][gi];
+                                if (own) A.gout[3 + id][gi] = s;
+                            }
+                        } else if (anyS) {
+                            s = stencil8(U, B[id], h);
+                        } else {
+                            s = stencil8(W, B[id], h);
+                        }
+                        if (ic == id) ed[ic] = s;
+                        else if (ic < id) eo[3 - ic - id] = 0.5f * s;
+                        else eo[3 - ic - id] = eo[3 - ic - id] + 0.5f * s;
+                    }
+                }
+                apply_inject(lpot, npot, A.pot, q, ed, eo);
+            }
+            {
+                const float lm = cur[0], m2 = 2.0f * cur[1];
+                const float s1v = lm * (ed[0] + ed[1] + ed[2]);
+#pragma unroll
+                for (int i = 0; i < 3; i++) { ed[i] = m2 * ed[i] + s1v; eo[i] = m2 * eo[i]; }
+            }
+            if constexpr (!F) apply_inject(lmom, nmom, A.mom, q, ed, eo);
+            {
+                const float r = cur[2];
+#pragma unroll
+                for (int i = 0; i < 3; i++) { ed[i] = ed[i] * r; eo[i] = eo[i] * r; }
+            }
+            if (A.stats && own)
+                st_w = fmaxn(st_w, (ed[0] * ed[0] + ed[1] * ed[1] + ed[2] * ed[2]) + 2.0f * (eo[0] * eo[0] + eo[1] * eo[1] + eo[2] * eo[2]));
+            // elastic hourglass cell values (acceleration.f90:141-156)
+            if (A.hourglass) {
+                bool inE = true;
+                if constexpr (!F) {
+                    const int cc[3] = {J, K, l};
+#pragma unroll
+                    for (int d = 0; d < 3; d++) inE = inE && cc[d] >= g.i1pml[d] && cc[d] <= g.i2pml[d] - 1;
+                }
+                if (inE) {
+                    const float y = cur[3];
+#pragma unroll
+                    for (int ic = 0; ic < 3; ic++) {
+                        float W2[8];
+#pragma unroll
+                        for (int t = 0; t < 8; t++) {
+                            const int n = hg_corner(t);
+                            W2[t] = NODE(ns[n], L::HG + ic, ni[n]);
+                        }
+#pragma unroll
+                        for (int iq = 0; iq < 4; iq++) he[3 * iq + ic] = hg_sum(W2, iq) * y;
+                    }
+                }
+            }
+        } else {
+#pragma unroll
+            for (int a = 0; a < L::NDIR; a++)
+#pragma unroll
+                for (int t = 0; t < 8; t++) cnb[a][t] = 0.f;
+        }
+#pragma unroll
+        for (int i = 0; i < 3; i++) { CELL(cs, i, tid) = ed[i]; CELL(cs, 3 + i, tid) = eo[i]; }
+#pragma unroll
+        for (int i = 0; i < 12; i++) CELL(cs, 6 + i, tid) = he[i];
+#pragma unroll
+        for (int a = 0; a < L::NDIR; a++)
+#pragma unroll
+            for (int t = 0; t < 8; t++) CELL(cs, 18 + 8 * a + t, tid) = cnb[a][t];
+    };
+
+    // ---------------------------------------------------------------- node phase
+    auto nodes = [&](int l, auto fast_tag) {
+        constexpr bool F = decltype(fast_tag)::value;
+        if (!outcol) return;
+        const long long q = g.idx(jn, kn, l);
+        // cells of diff_cn term t: (j-1|j, k-1|k, l-1|l)
+        int ci[8], cs[8];
+#pragma unroll
+        for (int t = 0; t < 8; t++) {
+            const int oj = (t & 1) ? 0 : -1, ok = (t >> 2) ? 0 : -1, ol = ((t >> 1) & 1) ? 0 : -1;
+            ci[t] = (tx + 1 + oj) + FJ * (ty + 1 + ok);
+            cs[t] = (l + ol) & 1;
+        }
+        float f[3];
+#pragma unroll
+        for (int ic = 0; ic < 3; ic++) {
+#pragma unroll
+            for (int iid = 0; iid < 3; iid++) {
+                const int id = (ic + iid) % 3;
+                const int comp = ic == id ? ic : 3 + (3 - ic - id);
+                float Fv[8], B[8];
+#pragma unroll
+                for (int t = 0; t < 8; t++) {
+                    Fv[t] = CELL(cs[t], comp, ci[t]);
+                    if (GEOM == GEOM_RECT || (GEOM == GEOM_TERRAIN && id == 2)) B[t] = A.br.bcn[id][t];
+                    else B[t] = CELL(cs[t], 18 + 8 * id + t, ci[t]);
+                }
+                float s = stencil8(Fv, B, h);
+                if constexpr (!F) {
+                    const int c = id == 0 ? jn : id == 1 ? kn : l;
+                    if (c <= g.i1pml[id]) {
+                        const int p = c + g.nnoff[id];
+                        float* P = A.sl.p[id] + slab_idx(g, id, A.sl.tp[id], c - g.i1node[id], jn, kn, l, ic);
+                        s = A.pmlc[g.npml + p - 1] * s + A.pmlc[p - 1] * *P;
+                        *P = *P + dt * s;
+                    }
+                    if (c >= g.i2pml[id]) {
+                        const int p = g.nn[id] - c - g.nnoff[id] + 1;
+                        float* P = A.sl.p[3 + id] + slab_idx(g, id, A.sl.tp[3 + id], g.i2node[id] - c, jn, kn, l, ic);
+                        s = A.pmlc[g.npml + p - 1] * s + A.pmlc[p - 1] * *P;
+                        *P = *P + dt * s;
+                    }
+                }
+                f[ic] = iid == 0 ? s : f[ic] + s;
+            }
+        }
+        if (A.hourglass) {
+            bool ne = true;
+            if constexpr (!F) {
+                const int cn_[3] = {jn, kn, l};
+#pragma unroll
+                for (int d = 0; d < 3; d++) ne = ne && cn_[d] >= g.i1pml[d] + 1 && cn_[d] <= g.i2pml[d] - 1;
+            }
+            if (ne) {
+                int hi[8], hs[8];
+#pragma unroll
+                for (int t = 0; t < 8; t++) {
+                    const int o = hg_corner(t);
+                    hi[t] = (tx + 1 - (o & 1)) + FJ * (ty + 1 - ((o >> 1) & 1));
+                    hs[t] = (l - (o >> 2)) & 1;
+                }
+#pragma unroll
+                for (int iq = 0; iq < 4; iq++)
+#pragma unroll
+                    for (int ic = 0; ic < 3; ic++) {
+                        float H[8];
+#pragma unroll
+                        for (int t = 0; t < 8; t++) H[t] = CELL(hs[t], 6 + 3 * iq + ic, hi[t]);
+                        f[ic] = f[ic] - hg_sum(H, iq);
+                    }
+            } else if constexpr (!F) {
+                if (A.hgvisc) {
+                    // viscous-only hourglass in the PML (acceleration.f90:164-199):
+                    // every cell of a PML node is a PML cell; pure PML cells
+                    // hold their viscous values in the hourglass slots, cells
+                    // that are also elastic-hourglass cells (the layer next to
+                    // the elastic region) are evaluated here from v
+                    int hi[8], hs[8], kind[8];
+                    float yc[8];
+#pragma unroll
+                    for (int t = 0; t < 8; t++) {
+                        const int o = hg_corner(t);
+                        hi[t] = (tx + 1 - (o & 1)) + FJ * (ty + 1 - ((o >> 1) & 1));
+                        hs[t] = (l - (o >> 2)) & 1;
+                        const int Jc = jn - (o & 1), Kc = kn - ((o >> 1) & 1), Lc = l - (o >> 2);
+                        const bool real = Jc >= g.i1cell[0] && Jc <= g.i2cell[0] && Kc >= g.i1cell[1] &&
+                                          Kc <= g.i2cell[1] && Lc >= g.i1cell[2] && Lc <= g.i2cell[2];
+                        const bool slab = Jc <= g.i1pml[0] || Jc >= g.i2pml[0] - 1 || Kc <= g.i1pml[1] ||
+                                          Kc >= g.i2pml[1] - 1 || Lc <= g.i1pml[2] || Lc >= g.i2pml[2] - 1;
+                        const bool inEc = Jc >= g.i1pml[0] && Jc <= g.i2pml[0] - 1 && Kc >= g.i1pml[1] &&
+                                          Kc <= g.i2pml[1] - 1 && Lc >= g.i1pml[2] && Lc <= g.i2pml[2] - 1;
+                        kind[t] = !(real && slab) ? 0 : inEc ? 2 : 1;
+                        yc[t] = kind[t] == 2 ? A.dh2 * A.yy[g.idx(Jc, Kc, Lc)] : 0.f;
+                    }
+#pragma unroll 1
+                    for (int ic = 0; ic < 3; ic++) {
+                        float Hq[4][8];
+#pragma unroll
+                        for (int t = 0; t < 8; t++) {
+                            if (kind[t] == 1) {
+#pragma unroll
+                                for (int iq = 0; iq < 4; iq++) Hq[iq][t] = CELL(hs[t], 6 + 3 * iq + ic, hi[t]);
+                            } else if (kind[t] == 2) {
+                                const int o = hg_corner(t);
+                                float Vc[8];
+#pragma unroll
+                                for (int m = 0; m < 8; m++) {
+                                    const int n = hg_corner(m);
+                                    const int dj = (n & 1) - (o & 1), dk = ((n >> 1) & 1) - ((o >> 1) & 1),
+                                              dl = (n >> 2) - (o >> 2);
+                                    Vc[m] = A.vin[ic][g.idx(jn + dj, kn + dk, l + dl)];
+                                }
+#pragma unroll
+                                for (int iq = 0; iq < 4; iq++) Hq[iq][t] = yc[t] * hg_sum(Vc, iq);
+                            } else {
+#pragma unroll
+                                for (int iq = 0; iq < 4; iq++) Hq[iq][t] = 0.f;
+                            }
+                        }
+                        float fi = f[0];
+                        if (ic == 1) fi = f[1];
+                        if (ic == 2) fi = f[2];
+#pragma unroll
+                        for (int iq = 0; iq < 4; iq++) fi = fi - hg_sum(Hq[iq], iq);
+                        if (ic == 0) f[0] = fi;
+                        if (ic == 1) f[1] = fi;
+                        if (ic == 2) f[2] = fi;
+                    }
+                }
+            }
+        }
+        if constexpr (!F) {
+            const Inject* E = nfrc >= 0 ? lfrc : A.force.e;
+            const int n = nfrc >= 0 ? nfrc : A.force.n;
+            for (int e = 0; e < n; e++)
+                if (E[e].idx == q) {
+                    const int c = E[e].comp;
+                    const float inc = E[e].inc;
+                    if (c == 0) f[0] = f[0] + inc;
+                    else if (c == 1) f[1] = f[1] + inc;
+                    else f[2] = f[2] + inc;
+                }
+        }
+        const float m = cur[4];
+#pragma unroll
+        for (int i = 0; i < 3; i++) f[i] = f[i] * m;
+        const float u0 = uv[0], u1 = uv[1], u2 = uv[2], v0 = uv[3], v1 = uv[4], v2 = uv[5];
+        if (A.stats) {
+            st_a = fmaxn(st_a, f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
+            st_v = fmaxn(st_v, v0 * v0 + v1 * v1 + v2 * v2);
+            st_u = fmaxn(st_u, u0 * u0 + u1 * u1 + u2 * u2);
+        }
+        if (A.aout[0])
+#pragma unroll
+            for (int i = 0; i < 3; i++) A.aout[i][q] = f[i];
+        if (A.fold) {
+            // leapfrog update of the next step (time_integration.f90:32-35)
+            float a, b;
+            a = v0 + dt * f[0]; b = u0 + dt * a; A.vout[0][q] = a; A.uout[0][q] = b;
+            a = v1 + dt * f[1]; b = u1 + dt * a; A.vout[1][q] = a; A.uout[1][q] = b;
+            a = v2 + dt * f[2]; b = u2 + dt * a; A.vout[2][q] = a; A.uout[2][q] = b;
+        }
+    };
+
+    // ---------------------------------------------------------------- stream
+    // ring: planes L0-1, L0, L0+1; staged: L0+2 in flight
+#pragma unroll 1
+    for (int p = -1; p <= 1; p++) {
+        fetch(L0 + p);
+        cp_async_wait_all();
+        __syncthreads();
+        store((L0 + p + 3) % 3);
+        __syncthreads();
+    }
+    fetch(L0 + 2);
+    stat_load(L0 - 1, cur);
+    uv_load(L0, uv);
+    cells(L0 - 1, std::false_type{});
+    stat_load(L0, cur);
+#pragma unroll 1
+    for (int l = L0; l <= L1; l++) {
+        cells(l, std::false_type{});
+        float nxt[5], nuv[6];
+        stat_load(l + 1, nxt);
+        cp_async_wait_all();
+        __syncthreads();  // cell plane l complete, staged plane l+2 landed
+        store((l + 2) % 3);
+        nodes(l, std::false_type{});
+        uv_load(l + 1, nuv);
+        __syncthreads();  // ring slot l+2 complete, staging and cell slot l-1 free
+        fetch(l + 3);
+#pragma unroll
+        for (int i = 0; i < 5; i++) cur[i] = nxt[i];
+#pragma unroll
+        for (int i = 0; i < 6; i++) uv[i] = nuv[i];
+    }
+    cp_async_wait_all();
+    if (A.stats) {
+        bmax(A.red + 0, st_a);
+        bmax(A.red + 1, st_v);
+        bmax(A.red + 2, st_u);
+        bmax(A.red + 3, st_w);
+    }
+#undef RAW
+#undef NODE
+#undef CELL
+}
+
+// Interior kernel: tile columns and planes (A.bx0, A.by0, A.lf0..A.lf1)
+// strictly inside the non-PML region, with no PML or boundary terms.
 template <int GEOM, bool FASTK>
-__global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(StepArgs A) {
+__global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(StepArgs A) {
     using L = Lay<GEOM>;
     constexpr int NGN = L::NGN, NGC = L::NGC, NDIR = L::NDIR;
     extern __shared__ float4 sm4[];
@@ -308,7 +874,7 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
             for (int a = 0; a < 3; a++)
 #pragma unroll
                 for (int t = 0; t < 8; t++) B[a][t] = A.br.bnc[a][t];
-        } else {
+        } else if (kPaired) {
             F2 PB[8], PC[8], P[8], PN[8];
 #pragma unroll
             for (int n = 0; n < 8; n++) {
@@ -331,12 +897,39 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
                 brackets_nc_g<float>(X0, X1, B[2]);
                 cell_cn_brackets_g<float>(X0, X1, B[2], cnb[NDIR - 1], 0.0f);
             }
+        } else {
+            brackets_nc_g<float>(X1, X2, B[0]);
+            cell_cn_brackets_g<float>(X1, X2, B[0], cnb[0], 0.0f);
+            brackets_nc_g<float>(X2, X0, B[1]);
+            cell_cn_brackets_g<float>(X2, X0, B[1], cnb[1], 0.0f);
+            if (GEOM == GEOM_TERRAIN) {
+#pragma unroll
+                for (int t = 0; t < 8; t++) B[2][t] = A.br.bnc[2][t];
+            } else {
+                brackets_nc_g<float>(X0, X1, B[2]);
+                cell_cn_brackets_g<float>(X0, X1, B[2], cnb[NDIR - 1], 0.0f);
+            }
         }
         float ed[3], eo[3], he[12];
 #pragma unroll
         for (int i = 0; i < 12; i++) he[i] = 0.f;
         const bool own = owncol && l >= L0;
-        if constexpr (F) {
+        if constexpr (F && !kPaired) {
+#pragma unroll
+            for (int ic = 0; ic < 3; ic++) {
+                float W[8];
+#pragma unroll
+                for (int t = 0; t < 8; t++) W[t] = Wc[ic][term_corner(t)];
+#pragma unroll
+                for (int iid = 0; iid < 3; iid++) {
+                    const int id = (ic + iid + 1) % 3;
+                    const float s = stencil8(W, B[id], h);
+                    if (ic == id) ed[ic] = s;
+                    else if (ic < id) eo[3 - ic - id] = 0.5f * s;
+                    else eo[3 - ic - id] = eo[3 - ic - id] + 0.5f * s;
+                }
+            }
+        } else if constexpr (F) {
             // strain of an interior cell: s[ic][id] = stencil8(w_ic, B[id]);
             // (ic0, ic1) paired per iid, ic2's first two directions paired
             const F2 h2 = f2(h, nz);
@@ -477,7 +1070,17 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
 #pragma unroll
                 for (int d = 0; d < 3; d++) inE = inE && cc[d] >= g.i1pml[d] && cc[d] <= g.i2pml[d] - 1;
             }
-            if (inE) {
+            if (inE && (!F || !kPaired)) {
+                const float y = cur[3];
+#pragma unroll
+                for (int ic = 0; ic < 3; ic++) {
+                    float W2[8];
+#pragma unroll
+                    for (int t = 0; t < 8; t++) W2[t] = Hc[ic][hg_corner(t)];
+#pragma unroll
+                    for (int iq = 0; iq < 4; iq++) he[3 * iq + ic] = hg_sum(W2, iq) * y;
+                }
+            } else if (inE) {
                 const float y = cur[3];
                 F2 H01[8];
                 float H2v[8];
@@ -534,7 +1137,17 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
             if (GEOM == GEOM_TERRAIN) Bc[2][t] = A.br.bcn[2][t];
         }
         float f[3];
-        if constexpr (F) {
+        if constexpr (F && !kPaired) {
+#pragma unroll
+            for (int ic = 0; ic < 3; ic++)
+#pragma unroll
+                for (int iid = 0; iid < 3; iid++) {
+                    const int id = (ic + iid) % 3;
+                    const int comp = ic == id ? ic : 3 + (3 - ic - id);
+                    const float s = stencil8(S[comp], Bc[id], h);
+                    f[ic] = iid == 0 ? s : f[ic] + s;
+                }
+        } else if constexpr (F) {
             // f[ic] = sum over iid of stencil8(sigma(ic, id), Bc[id]), id = (ic + iid) % 3;
             // (ic0, ic1) paired per iid, ic2's first two terms paired
             const F2 h2 = f2(h, nz);
@@ -617,7 +1230,20 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_step(Step
             hB[t] = cp_[4 * NCL].y;                                            \
         }                                                                      \
     }
-            if (ne) {
+            if (ne && (!F || !kPaired)) {
+#pragma unroll
+                for (int iq = 0; iq < 4; iq++) {
+                    F2 hA[8];
+                    float hB[8];
+                    HVALS(iq, hA, hB);
+                    float Hx[8], Hy[8];
+#pragma unroll
+                    for (int t = 0; t < 8; t++) { Hx[t] = hA[t].x(); Hy[t] = hA[t].y(); }
+                    f[0] = f[0] - hg_sum(Hx, iq);
+                    f[1] = f[1] - hg_sum(Hy, iq);
+                    f[2] = f[2] - hg_sum(hB, iq);
+                }
+            } else if (ne) {
                 F2 f01 = f2(f[0], f[1], nz);
 #pragma unroll
                 for (int iq = 0; iq < 4; iq++) {
@@ -870,12 +1496,16 @@ static void source_columns(const Solver& s, const FusedPlan& P, const std::vecto
 template <int GEOM, bool FASTK>
 static void launch_mode(Solver& s, const StepArgs& A, dim3 grid) {
     static bool set = false;
+    const size_t bytes = FASTK ? Lay<GEOM>::bytes : LayS<GEOM>::bytes;
     if (!set) {
-        SORD_CUDA(cudaFuncSetAttribute(k_step<GEOM, FASTK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)Lay<GEOM>::bytes));
+        if (FASTK)
+            SORD_CUDA(cudaFuncSetAttribute(k_interior<GEOM, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+        else
+            SORD_CUDA(cudaFuncSetAttribute(k_shell<GEOM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
         set = true;
     }
-    k_step<GEOM, FASTK><<<grid, dim3(FJ, FK), Lay<GEOM>::bytes, s.stream>>>(A);
+    if (FASTK) k_interior<GEOM, true><<<grid, dim3(FJ, FK), bytes, s.stream>>>(A);
+    else k_shell<GEOM><<<grid, dim3(FJ, FK), bytes, s.stream>>>(A);
     s.launches++;
     SORD_CUDA(cudaGetLastError());
 }

@@ -29,13 +29,13 @@ struct F2 {
     unsigned long long v;   // lanes (x, y)
     unsigned long long nz;  // (-0.0, -0.0), unknown to the compiler
     __device__ __forceinline__ float x() const {
-        float a, b;
-        asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+        float a;
+        asm("{\n\t.reg .f32 hi;\n\tmov.b64 {%0, hi}, %1;\n\t}" : "=f"(a) : "l"(v));
         return a;
     }
     __device__ __forceinline__ float y() const {
-        float a, b;
-        asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+        float b;
+        asm("{\n\t.reg .f32 lo;\n\tmov.b64 {lo, %0}, %1;\n\t}" : "=f"(b) : "l"(v));
         return b;
     }
 };
