@@ -1412,12 +1412,19 @@ struct FusedPlan {
     int4* h_items = nullptr;                       // pinned staging
     int cap = 0;
     cudaEvent_t done = nullptr;
+    // the PML-shell kernel runs on a second stream, concurrently with the
+    // interior kernel (they write disjoint nodes and read the same inputs)
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
 };
 
 void fused_free(Solver& s) {
     FusedPlan* P = s.fplan;
     if (!P) return;
     if (P->done) cudaEventDestroy(P->done);
+    if (P->fork) cudaEventDestroy(P->fork);
+    if (P->join) cudaEventDestroy(P->join);
+    if (P->side) cudaStreamDestroy(P->side);
     if (P->d_items) cudaFree(P->d_items);
     if (P->h_items) cudaFreeHost(P->h_items);
     delete P;
@@ -1471,6 +1478,9 @@ static FusedPlan& fused_plan(Solver& s) {
     SORD_CUDA(cudaMalloc((void**)&P->d_items, sizeof(int4) * P->cap));
     SORD_CUDA(cudaMallocHost((void**)&P->h_items, sizeof(int4) * P->cap));
     SORD_CUDA(cudaEventCreateWithFlags(&P->done, cudaEventDisableTiming));
+    SORD_CUDA(cudaEventCreateWithFlags(&P->fork, cudaEventDisableTiming));
+    SORD_CUDA(cudaEventCreateWithFlags(&P->join, cudaEventDisableTiming));
+    SORD_CUDA(cudaStreamCreateWithFlags(&P->side, cudaStreamNonBlocking));
     return *P;
 }
 
@@ -1494,7 +1504,7 @@ static void source_columns(const Solver& s, const FusedPlan& P, const std::vecto
 }
 
 template <int GEOM, bool FASTK>
-static void launch_mode(Solver& s, const StepArgs& A, dim3 grid) {
+static void launch_mode(Solver& s, const StepArgs& A, dim3 grid, cudaStream_t st) {
     static bool set = false;
     const size_t bytes = FASTK ? Lay<GEOM>::bytes : LayS<GEOM>::bytes;
     if (!set) {
@@ -1504,17 +1514,17 @@ static void launch_mode(Solver& s, const StepArgs& A, dim3 grid) {
             SORD_CUDA(cudaFuncSetAttribute(k_shell<GEOM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
         set = true;
     }
-    if (FASTK) k_interior<GEOM, true><<<grid, dim3(FJ, FK), bytes, s.stream>>>(A);
-    else k_shell<GEOM><<<grid, dim3(FJ, FK), bytes, s.stream>>>(A);
+    if (FASTK) k_interior<GEOM, true><<<grid, dim3(FJ, FK), bytes, st>>>(A);
+    else k_shell<GEOM><<<grid, dim3(FJ, FK), bytes, st>>>(A);
     s.launches++;
     SORD_CUDA(cudaGetLastError());
 }
 
 template <bool FASTK>
-static void launch_geom(Solver& s, const StepArgs& A, dim3 grid) {
-    if (s.geom == GEOM_RECT) launch_mode<GEOM_RECT, FASTK>(s, A, grid);
-    else if (s.geom == GEOM_TERRAIN) launch_mode<GEOM_TERRAIN, FASTK>(s, A, grid);
-    else launch_mode<GEOM_GENERAL, FASTK>(s, A, grid);
+static void launch_geom(Solver& s, const StepArgs& A, dim3 grid, cudaStream_t st) {
+    if (s.geom == GEOM_RECT) launch_mode<GEOM_RECT, FASTK>(s, A, grid, st);
+    else if (s.geom == GEOM_TERRAIN) launch_mode<GEOM_TERRAIN, FASTK>(s, A, grid, st);
+    else launch_mode<GEOM_GENERAL, FASTK>(s, A, grid, st);
 }
 
 void launch_fused(Solver& s, const InjectList& pot, const InjectList& mom, const InjectList& force,
@@ -1585,8 +1595,19 @@ void launch_fused(Solver& s, const InjectList& pot, const InjectList& mom, const
 
     cudaEvent_t e0 = nullptr;
     s.prof_begin(KC_FUSED, &e0);
-    if (P.fbx1 >= P.fbx0) launch_geom<true>(s, A, dim3(P.fbx1 - P.fbx0 + 1, P.fby1 - P.fby0 + 1, 1));
-    if (!items.empty()) launch_geom<false>(s, A, dim3((unsigned)items.size(), 1, 1));
+    const bool inner = P.fbx1 >= P.fbx0;
+    if (inner && !items.empty()) {
+        SORD_CUDA(cudaEventRecord(P.fork, s.stream));
+        SORD_CUDA(cudaStreamWaitEvent(P.side, P.fork, 0));
+        launch_geom<false>(s, A, dim3((unsigned)items.size(), 1, 1), P.side);
+        launch_geom<true>(s, A, dim3(P.fbx1 - P.fbx0 + 1, P.fby1 - P.fby0 + 1, 1), s.stream);
+        SORD_CUDA(cudaEventRecord(P.join, P.side));
+        SORD_CUDA(cudaStreamWaitEvent(s.stream, P.join, 0));
+    } else if (inner) {
+        launch_geom<true>(s, A, dim3(P.fbx1 - P.fbx0 + 1, P.fby1 - P.fby0 + 1, 1), s.stream);
+    } else if (!items.empty()) {
+        launch_geom<false>(s, A, dim3((unsigned)items.size(), 1, 1), s.stream);
+    }
     s.prof_end(KC_FUSED, e0);
     if (fold) {
         for (int i = 0; i < 3; i++) {
