@@ -371,7 +371,7 @@ def run_ours(args):
     # dominant kernel: the fused whole-step kernel, average launch duration
     k_ms, k_n = kt.get('step', (0.0, 0))
     if k_n:
-        kernel, launch_ms = 'k_step (fused whole step)', k_ms / k_n
+        kernel, launch_ms = 'k_interior + k_shell (one fused step, concurrent)', k_ms / k_n
     else:
         kernel = 'k_time + k_stress + k_accel (separate-kernel step)'
         launch_ms = sum(kt[k][0] for k in ('time', 'stress', 'accel', 'mass')) / prof_steps
