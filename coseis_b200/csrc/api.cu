@@ -513,6 +513,11 @@ void Solver::destroy() {
     for (auto& p : prof_ev) { cudaEventDestroy(p.second.first); cudaEventDestroy(p.second.second); }
     prof_ev.clear();
     if (hinj) cudaFreeHost(hinj);
+    if (d_stage) cudaFree(d_stage);
+    for (int i = 0; i < 2; i++) {
+        if (pin_io[i]) cudaFreeHost(pin_io[i]);
+        if (pin_ev[i]) cudaEventDestroy(pin_ev[i]);
+    }
     for (auto& e : inj_done) if (e) cudaEventDestroy(e);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);

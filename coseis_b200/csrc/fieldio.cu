@@ -7,10 +7,16 @@
 //                 launch per hook serves every firing probe; records are
 //                 copied to the host and appended to the file every nb
 //                 samples, at it2 and every itio steps
-//   disk input    host-side: the field is copied down, the op applied with
+//   disk input    whole-volume records with unit stride (the setup inputs:
+//                 material, coordinates) are read in chunks through pinned
+//                 buffers straight into a device record, checked for
+//                 NaN / Inf, staged into the volume scratch s1 and applied
+//                 on the device; other inputs (sub-cell '.<', strided or
+//                 half-dimension records, time-varying inputs) take the
+//                 host path: the field is copied down, the op applied with
 //                 the reference's buffer / interpolation / half-dimension
-//                 fill rules, and copied back (setup inputs and rare
-//                 time-varying inputs only)
+//                 fill rules, and copied back
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -120,6 +126,35 @@ __global__ void k_probe(const float* f, ProbeBatch b) {
     float acc = 0.f;
     for (int t = 0; t < P.n; t++) acc = acc + f[P.idx[t]] * P.r[t];
     *b.dst[i] = acc;
+}
+
+// Whole-volume input record (unit stride): s1 region = record, and any NaN
+// or +Inf flagged (input_output.f90:333-337, 359-369).
+__global__ void k_stage_in(float* s1, const float* rec, Region R, unsigned* bad) {
+    const long long c0 = R.i2[0] - R.i1[0] + 1, c1 = R.i2[1] - R.i1[1] + 1, c2 = R.i2[2] - R.i1[2] + 1;
+    const long long n = c0 * c1 * c2;
+    unsigned b = 0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int j = R.i1[0] + (int)(t % c0), k = R.i1[1] + (int)((t / c0) % c1), l = R.i1[2] + (int)(t / (c0 * c1));
+        const float v = rec[t];
+        if (v != v || v > 3.402823466e38f) b = 1;
+        s1[(j - 1) + (long long)R.n[0] * ((k - 1) + (long long)R.n[1] * (l - 1))] = v;
+    }
+    if (b) atomicOr(bad, 1u);
+}
+
+// f region (op) s1 region: 0 '=<', 1 '+<', 2 '*<' (input_output.f90:392-419)
+__global__ void k_apply_in(float* f, const float* s1, Region R, int op) {
+    const long long c0 = R.i2[0] - R.i1[0] + 1, c1 = R.i2[1] - R.i1[1] + 1, c2 = R.i2[2] - R.i1[2] + 1;
+    const long long n = c0 * c1 * c2;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int j = R.i1[0] + (int)(t % c0), k = R.i1[1] + (int)((t / c0) % c1), l = R.i1[2] + (int)(t / (c0 * c1));
+        const long long q = (j - 1) + (long long)R.n[0] * ((k - 1) + (long long)R.n[1] * (l - 1));
+        const float a = s1[q];
+        if (op == 0) f[q] = a;
+        else if (op == 1) f[q] = f[q] + a;
+        else f[q] = f[q] * a;
+    }
 }
 
 // ------------------------------------------------------------ host
@@ -320,6 +355,82 @@ static void magnitude(Solver& s, const std::string& fl) {
     else if (fl == "wm2") dev_tensor_norm(s, s.d.s1, s.d.sd, s.d.so, g.i1core, g.i2core, one);
 }
 
+// Read `count` floats of file `fn` from float offset `off` into device
+// memory `dst`: chunks of 16 M floats alternate between two pinned buffers,
+// so the file read of one chunk overlaps the copy of the previous one.
+static void read_to_device(Solver& s, const std::string& fn, size_t off, size_t count, float* dst) {
+    constexpr size_t kChunk = (size_t)16 << 20;
+    for (int i = 0; i < 2; i++)
+        if (!s.pin_io[i]) {
+            SORD_CUDA(cudaMallocHost((void**)&s.pin_io[i], sizeof(float) * kChunk));
+            SORD_CUDA(cudaEventCreateWithFlags(&s.pin_ev[i], cudaEventDisableTiming));
+        }
+    FILE* fp = fopen(s.path(fn).c_str(), "rb");
+    if (!fp) throw SordError(SORD_E_IO, "cannot open " + fn);
+    if (fseeko(fp, (off_t)(off * sizeof(float)), SEEK_SET) != 0) {
+        fclose(fp);
+        throw SordError(SORD_E_IO, "short read " + fn);
+    }
+    size_t done = 0;
+    for (int b = 0; done < count; b ^= 1) {
+        const size_t want = std::min(kChunk, count - done);
+        SORD_CUDA(cudaEventSynchronize(s.pin_ev[b]));  // the copy that last used this buffer
+        const size_t got = fread(s.pin_io[b], sizeof(float), want, fp);
+        if (got != want) {
+            fclose(fp);
+            SORD_CUDA(cudaStreamSynchronize(s.stream));
+            throw SordError(SORD_E_IO, "short read " + fn);
+        }
+        SORD_CUDA(cudaMemcpyAsync(dst + done, s.pin_io[b], sizeof(float) * want, cudaMemcpyHostToDevice, s.stream));
+        SORD_CUDA(cudaEventRecord(s.pin_ev[b], s.stream));
+        done += want;
+    }
+    fclose(fp);
+}
+
+// Device path of disk input for one whole-volume record with unit stride
+// and no half-dimension fill, read once (static inputs).  Same semantics as
+// the host path below: s1 keeps the staged record, f gets the op.
+static bool device_volume_input(Solver& s, IoOp& io, FieldView f, const int* i1, const int* i2, const int* di,
+                                const int* m, const int* n) {
+    const Geom& g = s.g;
+    const int it1 = io.ii[3][0], it2 = io.ii[3][1], dit = io.ii[3][2];
+    const int code = io.op == "=<" ? 0 : io.op == "+<" ? 1 : io.op == "*<" ? 2 : -1;
+    if (code < 0 || io.ib >= 0 || s.it != it2) return false;
+    if (code != 0 && f.p == s.d.s1) return false;  // f aliases the staging scratch: host path order
+    for (int i = 0; i < 3; i++)
+        if (f.n[i] != g.nm[i] || di[i] != 1 || m[i] != n[i] || m[i] == 1 || n[i] < 1) return false;
+    const size_t nsp = (size_t)n[0] * n[1] * n[2];
+    if (nsp == 0) return false;
+    if (s.stage_cap < nsp) {
+        if (s.d_stage) SORD_CUDA(cudaFree(s.d_stage));
+        s.d_stage = nullptr;
+        s.stage_cap = 0;
+        if (cudaMalloc((void**)&s.d_stage, sizeof(float) * (nsp + 1)) != cudaSuccess) {
+            cudaGetLastError();
+            throw SordError(SORD_E_NOMEM, "cannot allocate the input staging record");
+        }
+        s.stage_cap = nsp;
+    }
+    unsigned* bad = reinterpret_cast<unsigned*>(s.d_stage + nsp);
+    SORD_CUDA(cudaMemsetAsync(bad, 0, sizeof(unsigned), s.stream));
+    const int o4 = (s.it - it1) / dit;
+    read_to_device(s, io.fname, nsp * (size_t)o4, nsp, s.d_stage);
+    Region R;
+    for (int i = 0; i < 3; i++) { R.n[i] = f.n[i]; R.i1[i] = i1[i]; R.i2[i] = i2[i]; R.di[i] = 1; }
+    R.vsy = g.sy;
+    R.vsz = g.sz;
+    k_stage_in<<<gf((long long)nsp), 256, 0, s.stream>>>(s.d.s1, s.d_stage, R, bad);
+    FCHK(s);
+    unsigned hbad = 0;
+    SORD_CUDA(cudaMemcpyAsync(&hbad, bad, sizeof(unsigned), cudaMemcpyDeviceToHost, s.stream));
+    SORD_CUDA(cudaStreamSynchronize(s.stream));
+    if (hbad) throw SordError(SORD_E_NANINF, "NaN/Inf in " + io.fname);
+    k_apply_in<<<gf((long long)nsp), 256, 0, s.stream>>>(f.p, s.d.s1, R, code);
+    FCHK(s);
+    return true;
+}
+
 // host-side disk input (input_output.f90:296-437)
 static void disk_input(Solver& s, IoOp& io, FieldView f, int* i1, int* i2, int* di, int* m, int* n, int* o, const PointGeom* P) {
     const Geom& g = s.g;
@@ -327,6 +438,11 @@ static void disk_input(Solver& s, IoOp& io, FieldView f, int* i1, int* i2, int* 
     if (io.op != ".<")
         for (int i = 0; i < 3; i++)
             if (m[i] == 1) { i1[i] = 1; i2[i] = 1; n[i] = 1; o[i] = 0; }
+    if (io.op != ".<" && device_volume_input(s, io, f, i1, i2, di, m, n)) {
+        region_scalar_bc(s, io, f);
+        io.op = "#";
+        return;
+    }
     int nsp = n[0] * n[1] * n[2];
     if (io.ib < 0) {
         io.bufn = std::max(nsp, 0);

@@ -275,6 +275,12 @@ struct Solver {
     std::vector<float> src_xi[3], src_dt, src_t0, src_w1[3], src_w2[3], src_history;
     // injection staging (pinned): one slot per list
     Inject* hinj = nullptr;
+    // volume file input on the device (fieldio.cu): staging record and two
+    // pinned chunk buffers for the file reads
+    float* d_stage = nullptr;
+    size_t stage_cap = 0;
+    float* pin_io[2] = {nullptr, nullptr};
+    cudaEvent_t pin_ev[2] = {nullptr, nullptr};
     // work decomposition of the fused step kernels (fused.cu)
     FusedPlan* fplan = nullptr;
     cudaEvent_t inj_done[kInjectSlots] = {};
