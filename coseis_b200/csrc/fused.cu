@@ -122,7 +122,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // Shared-memory layout of the PML-shell kernel: plain per-field planes
 // (node ring: w(3), hourglass input(3), coordinates; cell ring: stress(6),
 // hourglass(12), divergence brackets(8 per direction)).
-template <int GEOM>
+template <int GEOM, int NPLS, int NCLS>
 struct LayS {
     static constexpr int NCOORD = GEOM == GEOM_RECT ? 0 : GEOM == GEOM_TERRAIN ? 1 : 3;
     static constexpr int RAWF = 7 + NCOORD;   // staged plane: u(3) v(3) gam coords
@@ -131,16 +131,22 @@ struct LayS {
     static constexpr int CO = 6;              // first coordinate field
     static constexpr int NDIR = GEOM == GEOM_RECT ? 0 : GEOM == GEOM_TERRAIN ? 2 : 3;
     static constexpr int CELLF = 6 + 12 + 8 * NDIR;  // stress, hourglass, divergence brackets
-    static constexpr size_t bytes = sizeof(float) * (size_t)(NPL * RAWF + 3 * NPL * NODEF + 2 * NCL * CELLF);
+    static constexpr size_t bytes = sizeof(float) * (size_t)(NPLS * RAWF + 3 * NPLS * NODEF + 2 * NCLS * CELLF);
 };
 
 
-// PML-shell kernel: the work items A.items (tile column, first and last node
-// plane), with every PML, boundary and point-source term of the step.
+// PML-shell kernel: 16 x 16 threads per block, each block the node box of
+// one work item of A.items (j0, k0, last j, last k, first and last plane,
+// at most 15 x 15 nodes), with every PML, boundary and point-source term of
+// the step.
+constexpr int SJ = 16, SK = 16;  // shell tile (cells = threads)
 template <int GEOM>
-__global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_shell(StepArgs A) {
+__global__ void __launch_bounds__(SJ * SK, GEOM == GEOM_GENERAL ? 1 : 2) k_shell(StepArgs A) {
+    constexpr int FJ = SJ, FK = SK, FNJ = FJ + 1, FNK = FK + 1, FOJ = FJ - 1, FOK = FK - 1;
+    constexpr int NPL = FNJ * FNK, NCL = FJ * FK, NTH = FJ * FK;
+    (void)FNK;
     constexpr bool FASTK = false;
-    using L = LayS<GEOM>;
+    using L = LayS<GEOM, NPL, NCL>;
     extern __shared__ float sm[];
     float* sR = sm;                          // [RAWF][NPL] staged plane
     float* sN = sR + L::RAWF * NPL;          // [3 slots][NODEF][NPL]
@@ -150,25 +156,14 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_shell(Ste
 #define CELL(slot, f, i) sC[((slot) * L::CELLF + (f)) * NCL + (i)]
     const Geom& g = A.g;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + FJ * ty;
-    int bx, by, L0, L1;
-    if (FASTK) {
-        bx = A.bx0 + blockIdx.x;
-        by = A.by0 + blockIdx.y;
-        L0 = A.lf0 + blockIdx.z * A.segl;
-        L1 = min(L0 + A.segl - 1, A.lf1);
-    } else {
-        const int4 it = A.items[blockIdx.x];
-        bx = it.x;
-        by = it.y;
-        L0 = it.z;
-        L1 = it.w;
-    }
-    const int j0 = g.i1node[0] + bx * FOJ, k0 = g.i1node[1] + by * FOK;
+    const int* it = A.items + 6 * blockIdx.x;
+    const int j0 = it[0], k0 = it[1], jm = it[2], km = it[3], L0 = it[4], L1 = it[5];
     const int J = j0 - 1 + tx, K = k0 - 1 + ty;      // this thread's cell column
     const int jn = j0 + tx, kn = k0 + ty;            // this thread's node column
-    const bool outcol = tx < FOJ && ty < FOK && jn <= g.i2node[0] && kn <= g.i2node[1];
+    const bool outcol = tx < FOJ && ty < FOK && jn <= jm && kn <= km;
     const bool cellcol = J >= g.i1cell[0] && J <= g.i2cell[0] && K >= g.i1cell[1] && K <= g.i2cell[1];
-    const bool owncol = J >= j0 && K >= k0;
+    // the cell of node column (J, K) belongs to the block that owns that node
+    const bool owncol = J >= j0 && J <= jm && K >= k0 && K <= km;
     const float h = g.h, dt = g.dt;
     float st_a = 0.f, st_v = 0.f, st_u = 0.f, st_w = 0.f;
     // terrain meshes: this thread's cell column's x (j, j+1) and y (k, k+1)
@@ -677,7 +672,7 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_shell(Ste
 #undef CELL
 }
 
-// Interior kernel: tile columns and planes (A.bx0, A.by0, A.lf0..A.lf1)
+// Interior kernel: tiles of 31 x 7 nodes from (A.jf, A.kf), planes A.lf0..A.lf1,
 // strictly inside the non-PML region, with no PML or boundary terms.
 template <int GEOM, bool FASTK>
 __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(StepArgs A) {
@@ -690,25 +685,16 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
 #define RAW(f, i) sR[(f) * NPL + (i)]
     const Geom& g = A.g;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + FJ * ty;
-    int bx, by, L0, L1;
-    if (FASTK) {
-        bx = A.bx0 + blockIdx.x;
-        by = A.by0 + blockIdx.y;
-        L0 = A.lf0 + blockIdx.z * A.segl;
-        L1 = min(L0 + A.segl - 1, A.lf1);
-    } else {
-        const int4 it = A.items[blockIdx.x];
-        bx = it.x;
-        by = it.y;
-        L0 = it.z;
-        L1 = it.w;
-    }
-    const int j0 = g.i1node[0] + bx * FOJ, k0 = g.i1node[1] + by * FOK;
+    const int L0 = A.lf0 + blockIdx.z * A.segl;
+    const int L1 = min(L0 + A.segl - 1, A.lf1);
+    const int j0 = A.jf + blockIdx.x * FOJ, k0 = A.kf + blockIdx.y * FOK;
     const int J = j0 - 1 + tx, K = k0 - 1 + ty;      // this thread's cell column
     const int jn = j0 + tx, kn = k0 + ty;            // this thread's node column
-    const bool outcol = tx < FOJ && ty < FOK && jn <= g.i2node[0] && kn <= g.i2node[1];
+    // the last tile of each row may be partial: its cells past (jend, kend)
+    // are computed but feed no output node
+    const bool outcol = tx < FOJ && ty < FOK && jn <= A.jend && kn <= A.kend;
     const bool cellcol = J >= g.i1cell[0] && J <= g.i2cell[0] && K >= g.i1cell[1] && K <= g.i2cell[1];
-    const bool owncol = J >= j0 && K >= k0;
+    const bool owncol = J >= j0 && J <= A.jend && K >= k0 && K <= A.kend;
     const float h = g.h, dt = g.dt;
     const unsigned long long nz = f2_pack(A.negzero, A.negzero);  // (-0.0, -0.0) from the host (pair.cuh)
     float st_a = 0.f, st_v = 0.f, st_u = 0.f, st_w = 0.f;
@@ -1395,22 +1381,25 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
 #undef HVALS
 }
 
-// Work decomposition of a fused step, fixed by the mesh: interior tile
-// columns (bx, by) whose cells all lie strictly inside the non-PML region
-// run the fast kernel over the node planes lf0..lf1 whose cells are interior
-// (or halo planes of a free surface); everything else -- PML columns, the
-// PML planes of interior columns, and interior columns holding a point
-// source in the current step -- is a list of (bx, by, l1, l2) items for the
-// general kernel.
+// Work decomposition of a fused step, fixed by the mesh.  The interior
+// rectangle holds the node columns (j, k) whose adjacent cells all lie
+// strictly inside the non-PML region, jf..jend x kf..kend; it is tiled by
+// 31 x 7 node tiles from (jf, kf) (the last tile of a row may be partial)
+// and runs the interior kernel over the node planes lf0..lf1 whose cells are
+// interior (or the halo plane of a free surface).  Everything else -- the
+// PML faces at full depth, the PML planes of the interior rectangle, and in
+// each step the interior tiles holding a point source -- is covered by
+// masked 15 x 15 node boxes for the shell kernel.  Boxes and tiles partition
+// the nodes, so every node, and every PML memory, is updated once.
 struct FusedPlan {
-    int nbx = 0, nby = 0;
-    int fbx0 = 0, fbx1 = -1, fby0 = 0, fby1 = -1;  // fast tile columns (inclusive)
-    int lf0 = 0, lf1 = -1;                         // fast node planes (inclusive)
-    std::vector<int4> base;                        // general items without point sources
-    std::vector<int4> cur;                         // items of the last upload
-    int4* d_items = nullptr;
-    int4* h_items = nullptr;                       // pinned staging
-    int cap = 0;
+    int jf = 0, jend = -1, kf = 0, kend = -1;   // interior rectangle (inclusive)
+    int nbx = 0, nby = 0;                       // interior tiles
+    int lf0 = 0, lf1 = -1;                      // interior node planes (inclusive)
+    std::vector<int> base;                      // shell items without point sources (6 ints each)
+    std::vector<int> cur;                       // items of the last upload
+    int* d_items = nullptr;
+    int* h_items = nullptr;                     // pinned staging
+    int cap = 0;                                // items
     cudaEvent_t done = nullptr;
     // the PML-shell kernel runs on a second stream, concurrently with the
     // interior kernel (they write disjoint nodes and read the same inputs)
@@ -1431,10 +1420,18 @@ void fused_free(Solver& s) {
     s.fplan = nullptr;
 }
 
-static constexpr int kItemPlanes = 96;  // longest general item, for load balance
+static constexpr int kItemPlanes = 96;  // deepest shell item, for load balance
 
-static void push_items(std::vector<int4>& v, int bx, int by, int l1, int l2) {
-    for (int a = l1; a <= l2; a += kItemPlanes) v.push_back(make_int4(bx, by, a, std::min(l2, a + kItemPlanes - 1)));
+// shell items covering node box [j1, j2] x [k1, k2] x [l1, l2]
+static void push_box(std::vector<int>& v, int j1, int j2, int k1, int k2, int l1, int l2) {
+    if (j1 > j2 || k1 > k2 || l1 > l2) return;
+    for (int a = l1; a <= l2; a += kItemPlanes)
+        for (int k = k1; k <= k2; k += SK - 1)
+            for (int j = j1; j <= j2; j += SJ - 1) {
+                const int it[6] = {j, k, std::min(j2, j + SJ - 2), std::min(k2, k + SK - 2), a,
+                                   std::min(l2, a + kItemPlanes - 1)};
+                v.insert(v.end(), it, it + 6);
+            }
 }
 
 static FusedPlan& fused_plan(Solver& s) {
@@ -1442,41 +1439,44 @@ static FusedPlan& fused_plan(Solver& s) {
     FusedPlan* P = new FusedPlan();
     s.fplan = P;
     const Geom& g = s.g;
-    const int nj = g.i2node[0] - g.i1node[0] + 1, nk = g.i2node[1] - g.i1node[1] + 1;
-    P->nbx = (int)div_up(nj, FOJ);
-    P->nby = (int)div_up(nk, FOK);
-    auto colok = [&](int d, int b, int w) {  // tile b along axis d (w nodes) is interior
-        const int a0 = g.i1node[d] + b * w;
-        return a0 - 1 > g.i1pml[d] && a0 + w - 1 < g.i2pml[d] - 1 && a0 - 1 >= g.i1cell[d] &&
-               a0 + w - 1 <= g.i2cell[d] && a0 + w - 1 <= g.i2node[d];
+    // node c along axis d is interior when both adjacent cells are
+    auto cin = [&](int d, int c) { return c > g.i1pml[d] && c < g.i2pml[d] - 1 && c >= g.i1cell[d] && c <= g.i2cell[d]; };
+    auto range = [&](int d, int& a, int& b) {
+        a = 0;
+        b = -1;
+        for (int c = g.i1node[d]; c <= g.i2node[d]; c++)
+            if (cin(d, c - 1) && cin(d, c)) {
+                if (b < a) a = c;
+                if (b == c - 1 || b < a) b = c;
+            }
     };
-    for (int b = 0; b < P->nbx; b++)
-        if (colok(0, b, FOJ)) { if (P->fbx1 < P->fbx0) P->fbx0 = b; P->fbx1 = b; }
-    for (int b = 0; b < P->nby; b++)
-        if (colok(1, b, FOK)) { if (P->fby1 < P->fby0) P->fby0 = b; P->fby1 = b; }
-    auto cellok = [&](int c) {
-        return c < g.i1cell[2] || c > g.i2cell[2] || (c > g.i1pml[2] && c < g.i2pml[2] - 1);
-    };
+    range(0, P->jf, P->jend);
+    range(1, P->kf, P->kend);
+    // planes: cells l-1 and l interior, or outside the mesh's cells (free surface)
+    auto cellok = [&](int c) { return c < g.i1cell[2] || c > g.i2cell[2] || cin(2, c); };
     for (int l = g.i1node[2]; l <= g.i2node[2]; l++) {
         const bool f = l >= g.i1pml[2] + 1 && l <= g.i2pml[2] - 1 && cellok(l - 1) && cellok(l);
         if (f && P->lf1 < P->lf0) P->lf0 = P->lf1 = l;
         else if (f && P->lf1 == l - 1) P->lf1 = l;
     }
-    const bool anyfast = P->fbx1 >= P->fbx0 && P->fby1 >= P->fby0 && P->lf1 >= P->lf0;
-    for (int by = 0; by < P->nby; by++)
-        for (int bx = 0; bx < P->nbx; bx++) {
-            const bool fc = anyfast && bx >= P->fbx0 && bx <= P->fbx1 && by >= P->fby0 && by <= P->fby1;
-            if (!fc) {
-                push_items(P->base, bx, by, g.i1node[2], g.i2node[2]);
-            } else {
-                if (P->lf0 > g.i1node[2]) push_items(P->base, bx, by, g.i1node[2], P->lf0 - 1);
-                if (P->lf1 < g.i2node[2]) push_items(P->base, bx, by, P->lf1 + 1, g.i2node[2]);
-            }
-        }
-    if (!anyfast) P->fbx1 = P->fbx0 - 1;
-    P->cap = (int)P->base.size() + 4096;
-    SORD_CUDA(cudaMalloc((void**)&P->d_items, sizeof(int4) * P->cap));
-    SORD_CUDA(cudaMallocHost((void**)&P->h_items, sizeof(int4) * P->cap));
+    const bool inner = P->jend >= P->jf && P->kend >= P->kf && P->lf1 >= P->lf0;
+    const int L1 = g.i1node[2], L2 = g.i2node[2];
+    if (!inner) {
+        push_box(P->base, g.i1node[0], g.i2node[0], g.i1node[1], g.i2node[1], L1, L2);
+        P->jend = P->jf - 1;
+    } else {
+        P->nbx = (int)div_up(P->jend - P->jf + 1, FOJ);
+        P->nby = (int)div_up(P->kend - P->kf + 1, FOK);
+        push_box(P->base, g.i1node[0], P->jf - 1, g.i1node[1], g.i2node[1], L1, L2);
+        push_box(P->base, P->jend + 1, g.i2node[0], g.i1node[1], g.i2node[1], L1, L2);
+        push_box(P->base, P->jf, P->jend, g.i1node[1], P->kf - 1, L1, L2);
+        push_box(P->base, P->jf, P->jend, P->kend + 1, g.i2node[1], L1, L2);
+        push_box(P->base, P->jf, P->jend, P->kf, P->kend, L1, P->lf0 - 1);
+        push_box(P->base, P->jf, P->jend, P->kf, P->kend, P->lf1 + 1, L2);
+    }
+    P->cap = (int)P->base.size() / 6 + 4096;
+    SORD_CUDA(cudaMalloc((void**)&P->d_items, sizeof(int) * 6 * P->cap));
+    SORD_CUDA(cudaMallocHost((void**)&P->h_items, sizeof(int) * 6 * P->cap));
     SORD_CUDA(cudaEventCreateWithFlags(&P->done, cudaEventDisableTiming));
     SORD_CUDA(cudaEventCreateWithFlags(&P->fork, cudaEventDisableTiming));
     SORD_CUDA(cudaEventCreateWithFlags(&P->join, cudaEventDisableTiming));
@@ -1484,19 +1484,19 @@ static FusedPlan& fused_plan(Solver& s) {
     return *P;
 }
 
-// Interior columns whose (j, k) box holds a point source of this step; the
-// boxes are those the fast kernel tests (cells j0-1..j0+30 for potency /
-// moment entries, nodes j0..j0+30 for forces).
-static void source_columns(const Solver& s, const FusedPlan& P, const std::vector<Inject>& e, bool cell,
-                           std::vector<std::pair<int, int>>& out) {
+// Interior tiles whose (j, k) box holds a point source of this step; the
+// boxes are those the interior kernel tests (cells j0-1..j0+30 for potency /
+// moment entries, nodes j0..j0+30 for forces), so both sides agree.
+static void source_tiles(const Solver& s, const FusedPlan& P, const std::vector<Inject>& e, bool cell,
+                         std::vector<std::pair<int, int>>& out) {
     const Geom& g = s.g;
     for (const Inject& x : e) {
         const int j = (int)(x.idx % g.sy) + 1, k = (int)((x.idx / g.sy) % g.nm[1]) + 1;
-        for (int bx = P.fbx0; bx <= P.fbx1; bx++) {
-            const int j0 = g.i1node[0] + bx * FOJ;
+        for (int bx = 0; bx < P.nbx; bx++) {
+            const int j0 = P.jf + bx * FOJ;
             if (!(cell ? (j >= j0 - 1 && j <= j0 + FOJ - 1) : (j >= j0 && j <= j0 + FOJ - 1))) continue;
-            for (int by = P.fby0; by <= P.fby1; by++) {
-                const int k0 = g.i1node[1] + by * FOK;
+            for (int by = 0; by < P.nby; by++) {
+                const int k0 = P.kf + by * FOK;
                 if (cell ? (k >= k0 - 1 && k <= k0 + FOK - 1) : (k >= k0 && k <= k0 + FOK - 1)) out.push_back({bx, by});
             }
         }
@@ -1506,7 +1506,7 @@ static void source_columns(const Solver& s, const FusedPlan& P, const std::vecto
 template <int GEOM, bool FASTK>
 static void launch_mode(Solver& s, const StepArgs& A, dim3 grid, cudaStream_t st) {
     static bool set = false;
-    const size_t bytes = FASTK ? Lay<GEOM>::bytes : LayS<GEOM>::bytes;
+    const size_t bytes = FASTK ? Lay<GEOM>::bytes : LayS<GEOM, (SJ + 1) * (SK + 1), SJ * SK>::bytes;
     if (!set) {
         if (FASTK)
             SORD_CUDA(cudaFuncSetAttribute(k_interior<GEOM, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
@@ -1515,7 +1515,7 @@ static void launch_mode(Solver& s, const StepArgs& A, dim3 grid, cudaStream_t st
         set = true;
     }
     if (FASTK) k_interior<GEOM, true><<<grid, dim3(FJ, FK), bytes, st>>>(A);
-    else k_shell<GEOM><<<grid, dim3(FJ, FK), bytes, st>>>(A);
+    else k_shell<GEOM><<<grid, dim3(SJ, SK), bytes, st>>>(A);
     s.launches++;
     SORD_CUDA(cudaGetLastError());
 }
@@ -1557,56 +1557,56 @@ void launch_fused(Solver& s, const InjectList& pot, const InjectList& mom, const
     A.fold = fold ? 1 : 0;
     A.stats = stats ? 1 : 0;
     A.red = (unsigned*)d.red;
-    A.bx0 = P.fbx0;
-    A.by0 = P.fby0;
+    A.jf = P.jf;
+    A.kf = P.kf;
+    A.jend = P.jend;
+    A.kend = P.kend;
     A.lf0 = P.lf0;
     A.lf1 = P.lf1;
     A.segl = P.lf1 - P.lf0 + 1;
     A.items = P.d_items;
     A.negzero = -0.0f;
 
-    // general items of this step: the fixed list, plus whole columns for
-    // interior columns holding a point source
+    // shell items of this step: the fixed list, plus the interior planes of
+    // the interior tiles holding a point source
     std::vector<std::pair<int, int>> src;
-    if (P.fbx1 >= P.fbx0) {
-        source_columns(s, P, hpot, true, src);
-        source_columns(s, P, hmom, true, src);
-        source_columns(s, P, hforce, false, src);
+    if (P.nbx > 0) {
+        source_tiles(s, P, hpot, true, src);
+        source_tiles(s, P, hmom, true, src);
+        source_tiles(s, P, hforce, false, src);
         std::sort(src.begin(), src.end());
         src.erase(std::unique(src.begin(), src.end()), src.end());
     }
-    std::vector<int4> items;
-    items.reserve(P.base.size() + src.size() * 4);
-    for (const int4& it : P.base)
-        if (src.empty() || !std::binary_search(src.begin(), src.end(), std::make_pair(it.x, it.y))) items.push_back(it);
-    for (auto& c : src) push_items(items, c.first, c.second, s.g.i1node[2], s.g.i2node[2]);
-    const bool same = items.size() == P.cur.size() &&
-                      std::equal(items.begin(), items.end(), P.cur.begin(), [](const int4& a, const int4& b) {
-                          return a.x == b.x && a.y == b.y && a.z == b.z && a.w == b.w;
-                      });
-    if (!same) {
-        if ((int)items.size() > P.cap) throw SordError(SORD_E_PARAM, "too many point-source columns in one step");
+    std::vector<int> items(P.base);
+    for (auto& c : src) {
+        const int j0 = P.jf + c.first * FOJ, k0 = P.kf + c.second * FOK;
+        push_box(items, j0, std::min(P.jend, j0 + FOJ - 1), k0, std::min(P.kend, k0 + FOK - 1), P.lf0, P.lf1);
+    }
+    const int nitems = (int)items.size() / 6;
+    if (items != P.cur) {
+        if (nitems > P.cap) throw SordError(SORD_E_PARAM, "too many point-source tiles in one step");
         SORD_CUDA(cudaEventSynchronize(P.done));
-        std::memcpy(P.h_items, items.data(), sizeof(int4) * items.size());
-        SORD_CUDA(cudaMemcpyAsync(P.d_items, P.h_items, sizeof(int4) * items.size(), cudaMemcpyHostToDevice, s.stream));
+        std::memcpy(P.h_items, items.data(), sizeof(int) * items.size());
+        SORD_CUDA(cudaMemcpyAsync(P.d_items, P.h_items, sizeof(int) * items.size(), cudaMemcpyHostToDevice, s.stream));
         SORD_CUDA(cudaEventRecord(P.done, s.stream));
         P.cur = items;
     }
 
     cudaEvent_t e0 = nullptr;
     s.prof_begin(KC_FUSED, &e0);
-    const bool inner = P.fbx1 >= P.fbx0;
-    if (inner && !items.empty()) {
+    const bool inner = P.nbx > 0 && P.nby > 0;
+    const dim3 igrid(P.nbx, P.nby, 1);
+    if (inner && nitems > 0) {
         SORD_CUDA(cudaEventRecord(P.fork, s.stream));
         SORD_CUDA(cudaStreamWaitEvent(P.side, P.fork, 0));
-        launch_geom<false>(s, A, dim3((unsigned)items.size(), 1, 1), P.side);
-        launch_geom<true>(s, A, dim3(P.fbx1 - P.fbx0 + 1, P.fby1 - P.fby0 + 1, 1), s.stream);
+        launch_geom<false>(s, A, dim3((unsigned)nitems, 1, 1), P.side);
+        launch_geom<true>(s, A, igrid, s.stream);
         SORD_CUDA(cudaEventRecord(P.join, P.side));
         SORD_CUDA(cudaStreamWaitEvent(s.stream, P.join, 0));
     } else if (inner) {
-        launch_geom<true>(s, A, dim3(P.fbx1 - P.fbx0 + 1, P.fby1 - P.fby0 + 1, 1), s.stream);
-    } else if (!items.empty()) {
-        launch_geom<false>(s, A, dim3((unsigned)items.size(), 1, 1), s.stream);
+        launch_geom<true>(s, A, igrid, s.stream);
+    } else if (nitems > 0) {
+        launch_geom<false>(s, A, dim3((unsigned)nitems, 1, 1), s.stream);
     }
     s.prof_end(KC_FUSED, e0);
     if (fold) {

@@ -143,10 +143,11 @@ struct StepArgs {
     int hourglass, hgvisc, fold, stats;
     unsigned* red;
     int segl;
-    // fast kernel: first tile (bx0, by0) and node planes lf0..lf1;
-    // general kernel: work items (bx, by, first plane, last plane)
-    int bx0, by0, lf0, lf1;
-    const int4* items;
+    // interior kernel: tiles from node (jf, kf), output nodes up to
+    // (jend, kend), node planes lf0..lf1; shell kernel: work items of six
+    // ints (j0, k0, last j, last k, first plane, last plane)
+    int jf, kf, jend, kend, lf0, lf1;
+    const int* items;
     float negzero;  // -0.0, the addend of packed products (pair.cuh)
 };
 
