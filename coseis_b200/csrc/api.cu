@@ -514,7 +514,7 @@ void Solver::destroy() {
     prof_ev.clear();
     if (hinj) cudaFreeHost(hinj);
     if (d_stage) cudaFree(d_stage);
-    for (int i = 0; i < 2; i++) {
+    for (int i = 0; i < 4; i++) {
         if (pin_io[i]) cudaFreeHost(pin_io[i]);
         if (pin_ev[i]) cudaEventDestroy(pin_ev[i]);
     }

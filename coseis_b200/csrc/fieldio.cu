@@ -16,11 +16,16 @@
 //                 host path: the field is copied down, the op applied with
 //                 the reference's buffer / interpolation / half-dimension
 //                 fill rules, and copied back
+#include <fcntl.h>
+#include <unistd.h>
+
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <thread>
 
 #include "sord.cuh"
 
@@ -356,36 +361,52 @@ static void magnitude(Solver& s, const std::string& fl) {
 }
 
 // Read `count` floats of file `fn` from float offset `off` into device
-// memory `dst`: chunks of 16 M floats alternate between two pinned buffers,
-// so the file read of one chunk overlaps the copy of the previous one.
+// memory `dst`.  kReaders host threads each read every kReaders-th chunk of
+// 8 M floats with pread into their own pinned buffer and copy it to the
+// device on the solver's stream; a thread waits for its previous copy before
+// reusing its buffer.
+static constexpr int kReaders = 4;
+static constexpr size_t kChunk = (size_t)8 << 20;
 static void read_to_device(Solver& s, const std::string& fn, size_t off, size_t count, float* dst) {
-    constexpr size_t kChunk = (size_t)16 << 20;
-    for (int i = 0; i < 2; i++)
+    static_assert(kReaders <= (int)(sizeof(s.pin_io) / sizeof(s.pin_io[0])), "pinned buffers");
+    for (int i = 0; i < kReaders; i++)
         if (!s.pin_io[i]) {
             SORD_CUDA(cudaMallocHost((void**)&s.pin_io[i], sizeof(float) * kChunk));
             SORD_CUDA(cudaEventCreateWithFlags(&s.pin_ev[i], cudaEventDisableTiming));
         }
-    FILE* fp = fopen(s.path(fn).c_str(), "rb");
-    if (!fp) throw SordError(SORD_E_IO, "cannot open " + fn);
-    if (fseeko(fp, (off_t)(off * sizeof(float)), SEEK_SET) != 0) {
-        fclose(fp);
+    const int fd = open(s.path(fn).c_str(), O_RDONLY);
+    if (fd < 0) throw SordError(SORD_E_IO, "cannot open " + fn);
+    const size_t nchunk = (count + kChunk - 1) / kChunk;
+    std::atomic<int> err{0};  // 1 short read, 2 CUDA error
+    auto reader = [&](int t) {
+        for (size_t c = (size_t)t; c < nchunk && !err.load(); c += kReaders) {
+            const size_t want = std::min(kChunk, count - c * kChunk);
+            if (cudaEventSynchronize(s.pin_ev[t]) != cudaSuccess) { err = 2; return; }
+            char* p = reinterpret_cast<char*>(s.pin_io[t]);
+            size_t got = 0;
+            const size_t bytes = want * sizeof(float);
+            const off_t base = (off_t)((off + c * kChunk) * sizeof(float));
+            while (got < bytes) {
+                const ssize_t r = pread(fd, p + got, bytes - got, base + (off_t)got);
+                if (r <= 0) { err = 1; return; }
+                got += (size_t)r;
+            }
+            if (cudaMemcpyAsync(dst + c * kChunk, p, bytes, cudaMemcpyHostToDevice, s.stream) != cudaSuccess ||
+                cudaEventRecord(s.pin_ev[t], s.stream) != cudaSuccess) {
+                err = 2;
+                return;
+            }
+        }
+    };
+    std::thread th[kReaders];
+    for (int t = 0; t < kReaders; t++) th[t] = std::thread(reader, t);
+    for (int t = 0; t < kReaders; t++) th[t].join();
+    close(fd);
+    if (err == 1) {
+        SORD_CUDA(cudaStreamSynchronize(s.stream));
         throw SordError(SORD_E_IO, "short read " + fn);
     }
-    size_t done = 0;
-    for (int b = 0; done < count; b ^= 1) {
-        const size_t want = std::min(kChunk, count - done);
-        SORD_CUDA(cudaEventSynchronize(s.pin_ev[b]));  // the copy that last used this buffer
-        const size_t got = fread(s.pin_io[b], sizeof(float), want, fp);
-        if (got != want) {
-            fclose(fp);
-            SORD_CUDA(cudaStreamSynchronize(s.stream));
-            throw SordError(SORD_E_IO, "short read " + fn);
-        }
-        SORD_CUDA(cudaMemcpyAsync(dst + done, s.pin_io[b], sizeof(float) * want, cudaMemcpyHostToDevice, s.stream));
-        SORD_CUDA(cudaEventRecord(s.pin_ev[b], s.stream));
-        done += want;
-    }
-    fclose(fp);
+    if (err == 2) SORD_CUDA(cudaGetLastError());
 }
 
 // Device path of disk input for one whole-volume record with unit stride

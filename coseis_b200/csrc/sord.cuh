@@ -280,8 +280,8 @@ struct Solver {
     // pinned chunk buffers for the file reads
     float* d_stage = nullptr;
     size_t stage_cap = 0;
-    float* pin_io[2] = {nullptr, nullptr};
-    cudaEvent_t pin_ev[2] = {nullptr, nullptr};
+    float* pin_io[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t pin_ev[4] = {nullptr, nullptr, nullptr, nullptr};
     // work decomposition of the fused step kernels (fused.cu)
     FusedPlan* fplan = nullptr;
     cudaEvent_t inj_done[kInjectSlots] = {};
