@@ -1105,12 +1105,14 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
             return (1 - (o & 1)) + 2 * (1 - ((o >> 1) & 1)) + 4 * (1 - (o >> 2));
         };
         // stress (6) and divergence brackets by diff_cn term
-        float S[6][8], Bc[3][8];
+        float S[6][8], Bc[3][8], HA0[2][8];  // HA0: mode-0 (x, y) hourglass values by diff_cn term
 #pragma unroll
         for (int t = 0; t < 8; t++) {
             const float4* cp = cpos(pt(t));
             const float4 a = cp[0], b = cp[NCL];
             S[0][t] = a.x; S[1][t] = a.y; S[2][t] = a.z; S[3][t] = a.w; S[4][t] = b.x; S[5][t] = b.y;
+            HA0[0][t] = b.z;
+            HA0[1][t] = b.w;
             if (NDIR >= 2) {
                 const float2 bb = reinterpret_cast<const float2*>(cp + (5 + t / 2) * NCL)[t % 2];
                 Bc[0][t] = bb.x;
@@ -1216,7 +1218,29 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
             hB[t] = cp_[4 * NCL].y;                                            \
         }                                                                      \
     }
-            if (ne && (!F || !kPaired)) {
+            if (ne && F && !kPaired) {
+                // each cell's hourglass groups once, as 128 / 64-bit loads:
+                // g1.zw = mode 0 (x, y), g2 = modes 1, 2 (x, y), g3 = mode 3
+                // (x, y), z of modes 0, 1, g4 = z of modes 2, 3
+                float H[4][3][8];
+#pragma unroll
+                for (int t = 0; t < 8; t++) {
+                    const int p = ph(t);
+                    // diff_cn term at the same cell position
+                    const int tp = (p & 1) + 4 * ((p >> 1) & 1) + 2 * (p >> 2);
+                    const float4* cp_ = cpos(p);
+                    const float4 g2 = cp_[2 * NCL], g3 = cp_[3 * NCL];
+                    const float2 g4 = reinterpret_cast<const float2*>(cp_ + 4 * NCL)[0];
+                    H[0][0][t] = HA0[0][tp]; H[0][1][t] = HA0[1][tp]; H[0][2][t] = g3.z;
+                    H[1][0][t] = g2.x; H[1][1][t] = g2.y; H[1][2][t] = g3.w;
+                    H[2][0][t] = g2.z; H[2][1][t] = g2.w; H[2][2][t] = g4.x;
+                    H[3][0][t] = g3.x; H[3][1][t] = g3.y; H[3][2][t] = g4.y;
+                }
+#pragma unroll
+                for (int iq = 0; iq < 4; iq++)
+#pragma unroll
+                    for (int ic = 0; ic < 3; ic++) f[ic] = f[ic] - hg_sum(H[iq][ic], iq);
+            } else if (ne && (!F || !kPaired)) {
 #pragma unroll
                 for (int iq = 0; iq < 4; iq++) {
                     F2 hA[8];
