@@ -161,6 +161,90 @@ def stage_in(prm, workdir, inputs):
     return open(os.path.join(workdir, 'sord.in')).read()
 
 
+# ------------------------------------------------------- rupture ensemble
+ENS_DX, ENS_DT, ENS_NT, ENS_NPML = 100.0, 0.008, 600, 10
+
+
+def gaussian_field_2d(shape, dx, corr, std, rng):
+    """Seeded Gaussian random field on a (nx, ny) plane with a Gaussian
+    correlation of length `corr`, zero mean and standard deviation `std`."""
+    w = rng.standard_normal(shape)
+    k0 = np.fft.fftfreq(shape[0], d=dx) * 2 * np.pi
+    k1 = np.fft.rfftfreq(shape[1], d=dx) * 2 * np.pi
+    F = np.fft.rfft2(w) * np.exp(-(k0[:, None] ** 2 + k1[None, :] ** 2) * corr * corr / 8.0)
+    f = np.fft.irfft2(F, s=shape)
+    f -= f.mean()
+    f *= std / f.std()
+    return f
+
+
+def rupture_scenario(i, seed=SEED, nt=ENS_NT, shape=None):
+    """Scenario `i` of the batched rupture ensemble: a spontaneous
+    slip-weakening rupture on the k-midplane ('+z' double-node fault) of a
+    seeded grid between 64x64x64 and 192x96x96 nodes (dx 100 m, dt 0.008 s,
+    homogeneous rho 2670, vp 6000, vs 3464, 10-node PML on all faces).
+    Seeded per scenario: mu_s in [0.6, 0.7], mu_d in [0.45, 0.55], Dc in
+    [0.2, 0.5] m, normal stress in [-120, -60] MPa; initial shear stress
+    0.58 |tn| (58 MPa at -100 MPa) plus a Gaussian random field of std
+    0.03 |tn| (3 MPa at -100 MPa) and correlation length 1 km; frictional
+    region the central 2/3 x 2/3 of the fault (mu_s = 1e4 outside), and a
+    square nucleation patch (3 km, at most a third of the region) at
+    1.02 mu_s |tn|.  Outputs: final slip, slip rate and shear traction
+    magnitude and the rupture time on the fault.
+
+    Returns (cst.sord parameter dict, {file name: float32 array}) where the
+    arrays are the '=<' input files (Fortran order, j fastest)."""
+    rng = np.random.default_rng([seed, 5, i])
+    if shape is None:
+        shape = (16 * int(rng.integers(4, 13)), 16 * int(rng.integers(4, 7)), 16 * int(rng.integers(4, 7)))
+    nx, ny, nz = shape
+    mus = float(rng.uniform(0.6, 0.7))
+    mud = float(rng.uniform(0.45, 0.55))
+    dc = float(rng.uniform(0.2, 0.5))
+    tn = -float(rng.uniform(60e6, 120e6))
+    ts = 0.58 * abs(tn) + gaussian_field_2d((nx, ny), ENS_DX, 1000.0, 0.03 * abs(tn), rng)
+    # frictional region and nucleation patch, in fault-plane node indices
+    rj, rk = max(1, nx // 6), max(1, ny // 6)
+    reg = [[rj, nx - rj], [rk, ny - rk]]
+    half = max(1, min(int(1500.0 / ENS_DX), (nx - 2 * rj) // 6, (ny - 2 * rk) // 6))
+    jc, kc = nx // 2, ny // 2
+    ts[jc - half:jc + half, kc - half:kc + half] = 1.02 * mus * abs(tn)
+    prm = {
+        'shape': [nx, ny, nz, nt], 'delta': [ENS_DX, ENS_DX, ENS_DX, ENS_DT],
+        'rho': [2670.0], 'vp': [6000.0], 'vs': [3464.0], 'gam': [0.1], 'hourglass': [1.0, 2.0],
+        'bc1': ['pml'] * 3, 'bc2': ['pml'] * 3, 'npml': ENS_NPML,
+        'faultnormal': '+z', 'hypocenter': [float(jc), float(kc), nz * 0.5 - 0.5], 'vrup': -1.0,
+        'mus': [1e4, (reg, '=', mus)], 'mud': [mud], 'dc': [dc], 'tn': [tn],
+        'ts': [([], '=<', 'ts.bin')],
+        'itstats': 10, 'itio': 100,
+    }
+    for f in ('sum', 'svm', 'tsm', 'trup'):
+        prm[f] = [([[], [], -1], '=>', f + '.bin')]
+    # the file holds the plane in Fortran order: j fastest
+    return prm, {'ts.bin': np.ascontiguousarray(ts.T, dtype='<f4')}
+
+
+def stage_scenarios(indices, root, seed=SEED, nt=ENS_NT, shape=None):
+    """Stage ensemble scenarios into root/s<i>; returns the directories."""
+    from coseis_b200 import sord
+    dirs = []
+    cwd = os.getcwd()
+    try:
+        for i in indices:
+            d = os.path.join(root, 's%03d' % i)
+            os.makedirs(d, exist_ok=True)
+            prm, files = rupture_scenario(i, seed, nt, shape)
+            for f, a in files.items():
+                a.tofile(os.path.join(d, f))
+            os.chdir(d)
+            sord.stage(prm)
+            os.chdir(cwd)
+            dirs.append(d)
+    finally:
+        os.chdir(cwd)
+    return dirs
+
+
 def pml_memberships(shape):
     """Node and cell PML slab memberships (one per node/cell per PML face)."""
     nn = np.array(shape)
@@ -361,6 +445,9 @@ def run_ours(args):
         if not args.no_e2e:
             e2e = run_e2e(args, shape, inputs, local)
             barrier(pg)
+        ens = None
+        if ws == 1 and args.ensemble > 0:
+            ens = run_ensemble_bench(args.ensemble, args.ensemble_threads, local)
     finally:
         shutil.rmtree(work, ignore_errors=True)
     if rank != 0:
@@ -396,6 +483,7 @@ def run_ours(args):
         'gpu_launches': int(launches),
         'clocks': clocks,
         'e2e': e2e,
+        'ensemble': ens,
     }
     if ws == 1 and not args.no_cpu:
         try:
@@ -427,6 +515,37 @@ def run_e2e(args, shape, inputs, device):
                 'h2d_bytes_per_step': h2d / args.steps, 'd2h_bytes_per_step': d2h / args.steps,
                 'wall_s': round(wall, 3), 'includes': 'setup from staged host files, %d steps, output files'
                                                       % args.steps}
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
+def run_ensemble_bench(n, nthreads, device, nt=ENS_NT, seed=SEED):
+    """Batched rupture ensemble: scenarios 0..n-1 run one at a time, then
+    the same scenarios through one sord_run_ensemble call with `nthreads`
+    concurrent scenarios.  Each arm is timed by the host clock around the
+    whole call (setup from staged files, nt steps, outputs written): the
+    metric is scenarios/s of finished runs."""
+    from coseis_b200 import _lib
+    work = tempfile.mkdtemp(prefix='sord_ens_')
+    try:
+        ser = stage_scenarios(range(n), os.path.join(work, 'serial'), seed, nt)
+        ens = stage_scenarios(range(n), os.path.join(work, 'batched'), seed, nt)
+        _lib.run_ensemble(stage_scenarios([n], os.path.join(work, 'warm'), seed, 20), device, 1)
+        t0 = time.time()
+        _lib.run_ensemble(ser, device, 1)
+        t_ser = time.time() - t0
+        t0 = time.time()
+        _lib.run_ensemble(ens, device, nthreads)
+        t_ens = time.time() - t0
+        same = all(open(os.path.join(a, f), 'rb').read() == open(os.path.join(b, f), 'rb').read()
+                   for a, b in zip(ser, ens) for f in ('sum.bin', 'trup.bin'))
+        nodes = [int(np.prod(rupture_scenario(i, seed, nt)[0]['shape'][:3])) for i in range(n)]
+        return {'metric': 'scenarios/s', 'value': n / t_ens, 'unit': 'scenarios/s',
+                'one_at_a_time': n / t_ser, 'speedup': t_ser / t_ens, 'scenarios': n,
+                'concurrent': nthreads, 'steps': nt, 'wall_s': round(t_ens, 3), 'serial_wall_s': round(t_ser, 3),
+                'node_updates_per_s': float(sum(nodes)) * nt / t_ens, 'outputs_identical': bool(same),
+                'workload': 'rupture ensemble: seeded grids 64x64x64..192x96x96, dx 100 m, dt 0.008 s, '
+                            'slip-weakening +z fault, seeded friction / stresses (scenarios 0..%d)' % (n - 1)}
     finally:
         shutil.rmtree(work, ignore_errors=True)
 
@@ -465,6 +584,8 @@ def main():
     ap.add_argument('--cache', default=os.environ.get('SORD_BENCH_CACHE', os.path.join(tempfile.gettempdir(), 'sord_bench')))
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu', action='store_true')
+    ap.add_argument('--ensemble', type=int, default=32, help='rupture-ensemble scenarios (0: skip)')
+    ap.add_argument('--ensemble-threads', type=int, default=8)
     ap.add_argument('--hill', type=float, default=500.0, help='topography peak (m); 0 gives a rectilinear mesh')
     args = ap.parse_args()
     if args.impl == 'reference':

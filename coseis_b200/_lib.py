@@ -15,8 +15,12 @@ SYMBOLS = [
     'sord_get_field', 'sord_info', 'sord_stats', 'sord_last_step_ms',
     'sord_kernel_launches', 'sord_set_profiling', 'sord_kernel_times',
     'sord_last_error', 'sord_error_string', 'sord_destroy',
-    'sord_vector_max_noalloc',
+    'sord_vector_max_noalloc', 'sord_run_ensemble',
 ]
+
+# return codes (enum in include/sordgpu.h)
+SORD_OK, SORD_E_PARAM, SORD_E_CFL, SORD_E_NEGVOL, SORD_E_NANINF = 0, -1, -2, -3, -4
+SORD_E_IO, SORD_E_CUDA, SORD_E_STATE, SORD_E_NOMEM = -5, -6, -7, -8
 
 _lib = None
 
@@ -66,6 +70,8 @@ def load():
     lib.sord_destroy.argtypes = [P]
     lib.sord_destroy.restype = None
     IP = ctypes.POINTER(ctypes.c_int)
+    lib.sord_run_ensemble.argtypes = [ctypes.POINTER(ctypes.c_char_p), ctypes.c_int, ctypes.c_int, ctypes.c_int, IP]
+    lib.sord_run_ensemble.restype = ctypes.c_int
     lib.sord_vector_max_noalloc.argtypes = [P, P, P, IP, IP, IP, P, P]
     lib.sord_vector_max_noalloc.restype = ctypes.c_int
     _lib = lib
@@ -89,6 +95,17 @@ def _check(rc, handle=None):
         msg = lib.sord_last_error(handle).decode(errors='replace')
         name = lib.sord_error_string(rc).decode()
         raise SordError(rc, '%s: %s' % (name, msg))
+
+
+def run_ensemble(paths, device=0, nthreads=8):
+    """Run many staged directories, `nthreads` concurrently (include/sordgpu.h);
+    returns the list of per-scenario return codes, raises on the first failure."""
+    lib = load()
+    n = len(paths)
+    arr = (ctypes.c_char_p * max(n, 1))(*[os.fsencode(p) for p in paths])
+    st = (ctypes.c_int * max(n, 1))()
+    _check(lib.sord_run_ensemble(arr, n, device, nthreads, st))
+    return list(st)[:n]
 
 
 def run_directory(path, device=0):

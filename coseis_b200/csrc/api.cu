@@ -6,6 +6,11 @@
 #include <cstring>
 #include <limits>
 #include <sstream>
+#include <thread>
+#include <vector>
+#include <atomic>
+#include <mutex>
+#include <algorithm>
 
 #include "sord.cuh"
 
@@ -534,7 +539,8 @@ struct sord_handle {
     Solver s;
 };
 
-static std::string g_create_error;
+// last error of a call without a handle, per host thread
+static thread_local std::string g_create_error;
 
 namespace sordgpu {
 void set_global_error(const char* msg) { g_create_error = msg; }
@@ -621,6 +627,41 @@ int sord_run_directory(const char* workdir, int device) {
     if (rc) g_create_error = h->s.err;
     sord_destroy(h);
     return rc;
+}
+
+int sord_run_ensemble(const char* const* workdirs, int n, int device, int nthreads, int* status) {
+    if (!workdirs || n < 0 || nthreads < 1) {
+        g_create_error = "bad ensemble arguments";
+        return SORD_E_PARAM;
+    }
+    std::atomic<int> next{0};
+    std::mutex m;
+    int first = SORD_OK;
+    std::string msg;
+    // each worker runs whole scenarios; every scenario has its own handle and
+    // stream, so the device overlaps the kernels of different scenarios
+    auto worker = [&]() {
+        for (;;) {
+            const int i = next++;
+            if (i >= n) return;
+            const int rc = workdirs[i] ? sord_run_directory(workdirs[i], device) : SORD_E_PARAM;
+            if (status) status[i] = rc;
+            if (rc != SORD_OK) {
+                std::lock_guard<std::mutex> lock(m);
+                if (first == SORD_OK) {
+                    first = rc;
+                    msg = std::string(workdirs[i] ? workdirs[i] : "(null)") + ": " + g_create_error;
+                }
+            }
+        }
+    };
+    const int nt = std::min(nthreads, std::max(n, 1));
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; t++) pool.emplace_back(worker);
+    worker();
+    for (auto& t : pool) t.join();
+    if (first != SORD_OK) g_create_error = msg;
+    return first;
 }
 
 int sord_get_field(sord_handle* h, const char* name, float* host, size_t n) {

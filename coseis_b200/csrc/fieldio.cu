@@ -25,6 +25,8 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <map>
+#include <mutex>
 #include <thread>
 
 #include "sord.cuh"
@@ -294,10 +296,16 @@ struct ProbeTable {
     Probe* dev = nullptr;
     std::vector<int> id_of_op;  // op index -> probe id (-1 none)
 };
-static std::map<const Solver*, ProbeTable> g_probes;
+static std::map<const Solver*, ProbeTable> g_probes;  // guarded by g_probes_m
+static std::mutex g_probes_m;
+
+static ProbeTable& probe_table(const Solver& s) {
+    std::lock_guard<std::mutex> lock(g_probes_m);
+    return g_probes[&s];  // element references stay valid while the map changes
+}
 
 static int probe_id(Solver& s, size_t opi, const IoOp& io, const FieldView& f) {
-    ProbeTable& T = g_probes[&s];
+    ProbeTable& T = probe_table(s);
     if (T.id_of_op.size() != s.ops.size()) T.id_of_op.assign(s.ops.size(), -1);
     if (T.id_of_op[opi] >= 0) return T.id_of_op[opi];
     PointGeom P;
@@ -324,6 +332,7 @@ static int probe_id(Solver& s, size_t opi, const IoOp& io, const FieldView& f) {
 }
 
 void probes_free(const Solver* s) {
+    std::lock_guard<std::mutex> lock(g_probes_m);
     auto it = g_probes.find(s);
     if (it != g_probes.end()) {
         if (it->second.dev) cudaFree(it->second.dev);
@@ -683,7 +692,7 @@ static void field_io_op(Solver& s, size_t opi, FieldView f, ProbeBatch& batch) {
                 FCHK(s);
                 batch.count = 0;
             }
-            batch.probes = g_probes[&s].dev;
+            batch.probes = probe_table(s).dev;
             batch.id[batch.count] = id;
             batch.dst[batch.count] = dst;
             batch.count++;

@@ -1529,15 +1529,9 @@ static void source_tiles(const Solver& s, const FusedPlan& P, const std::vector<
 
 template <int GEOM, bool FASTK>
 static void launch_mode(Solver& s, const StepArgs& A, dim3 grid, cudaStream_t st) {
-    static bool set = false;
     const size_t bytes = FASTK ? Lay<GEOM>::bytes : LayS<GEOM, (SJ + 1) * (SK + 1), SJ * SK>::bytes;
-    if (!set) {
-        if (FASTK)
-            SORD_CUDA(cudaFuncSetAttribute(k_interior<GEOM, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-        else
-            SORD_CUDA(cudaFuncSetAttribute(k_shell<GEOM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-        set = true;
-    }
+    if (FASTK) smem_limit((const void*)k_interior<GEOM, true>, (int)bytes);
+    else smem_limit((const void*)k_shell<GEOM>, (int)bytes);
     if (FASTK) k_interior<GEOM, true><<<grid, dim3(FJ, FK), bytes, st>>>(A);
     else k_shell<GEOM><<<grid, dim3(SJ, SK), bytes, st>>>(A);
     s.launches++;

@@ -592,12 +592,10 @@ void launch_accel(Solver& s, bool mass, bool stats, const InjectList& force) {
     cudaEvent_t e0 = nullptr;
     s.prof_begin(KC_ACCEL, &e0);
     if (s.rect) {
-        static bool set = false;
-        if (!set) { SORD_CUDA(cudaFuncSetAttribute(k_accel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)accel_smem(true))); set = true; }
+        smem_limit((const void*)k_accel<true>, (int)accel_smem(true));
         k_accel<true><<<gr, b, sm, s.stream>>>(A);
     } else {
-        static bool set = false;
-        if (!set) { SORD_CUDA(cudaFuncSetAttribute(k_accel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)accel_smem(false))); set = true; }
+        smem_limit((const void*)k_accel<false>, (int)accel_smem(false));
         k_accel<false><<<gr, b, sm, s.stream>>>(A);
     }
     s.launches++;

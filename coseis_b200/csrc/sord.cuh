@@ -302,6 +302,8 @@ struct Solver {
     void destroy();
 };
 
+void smem_limit(const void* func, int bytes);
+
 // cell / node counts for launches
 inline unsigned div_up(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
 

@@ -1,6 +1,10 @@
 // Device helpers used by setup, field I/O and statistics: fills, set_halo
 // (utilities.f90:103-117), region reductions, vector/tensor norms
 // (utilities.f90:120-165) and rinvert (utilities.f90:40-49).
+#include <mutex>
+#include <set>
+#include <utility>
+
 #include "sord.cuh"
 
 namespace sordgpu {
@@ -182,6 +186,19 @@ void dev_tensor_norm(Solver& s, float* dst, float* const a[3], float* const bb[3
     k_tnorm<<<grid_for(n), 256, 0, s.stream>>>(dst, a[0], a[1], a[2], bb[0], bb[1], bb[2], b, di[0], di[1], di[2], s.g.sy, s.g.sz);
     s.launches++;
     SORD_CUDA(cudaGetLastError());
+}
+
+// Raise a kernel's dynamic shared-memory limit once per device; safe when
+// several host threads launch on one or more devices.
+void smem_limit(const void* func, int bytes) {
+    static std::mutex m;
+    static std::set<std::pair<int, const void*>> done;
+    int dev = 0;
+    SORD_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(m);
+    if (done.count({dev, func})) return;
+    SORD_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    done.insert({dev, func});
 }
 
 }  // namespace sordgpu

@@ -522,3 +522,34 @@ def run(args=None, **kwargs):
     from . import _lib
     _lib.run_directory(os.getcwd())
     return meta
+
+
+def run_ensemble(cases, rundirs, nthreads=8, device=0):
+    """Stage each parameter dict of ``cases`` in its directory of ``rundirs``
+    and run all of them on one GPU, ``nthreads`` scenarios at a time.
+
+    Where the reference submits one ``sord.x`` job per scenario
+    (cst/sord.py:558-561 -> cst/job.py:176-195), this stages every scenario
+    with ``stage()`` and hands the directories to one ``sord_run_ensemble``
+    call (include/sordgpu.h): each scenario runs on its own handle and CUDA
+    stream, so the kernels of different scenarios overlap on the device.
+    Input files named by '=<' ops must already be in each directory.  Each
+    scenario writes exactly the outputs ``run()`` writes.  Returns the list
+    of ``meta`` dicts.
+    """
+    if len(cases) != len(rundirs):
+        raise ValueError('one run directory per case')
+    metas = []
+    cwd = os.getcwd()
+    try:
+        for args, d in zip(cases, rundirs):
+            os.makedirs(d, exist_ok=True)
+            os.chdir(d)
+            job, meta = stage(args)
+            metas.append(meta)
+            os.chdir(cwd)
+    finally:
+        os.chdir(cwd)
+    from . import _lib
+    _lib.run_ensemble([os.path.abspath(d) for d in rundirs], device=device, nthreads=nthreads)
+    return metas

@@ -57,6 +57,17 @@ int sord_run(sord_handle* h);
  * This is the whole of `sord.x` (cst/job.py:193-194 `subprocess.check_call`). */
 int sord_run_directory(const char* workdir, int device);
 
+/* Run `n` staged directories (each with its sord.in) to completion on CUDA
+ * device `device`, up to `nthreads` at a time: host threads take scenarios in
+ * turn, each scenario with its own handle and stream, so the device overlaps
+ * the kernels of different scenarios (ensembles of small runs are bound by
+ * launch latency when run one at a time).  Each scenario's outputs are those
+ * of sord_run_directory on its own.  status[i] (if not NULL) receives each
+ * scenario's return code; the call returns the first failure, whose message
+ * sord_last_error(NULL) gives.  Replaces: one `sord.x` process per scenario
+ * (cst/job.py:176-195), which the reference runs one job at a time. */
+int sord_run_ensemble(const char* const* workdirs, int n, int device, int nthreads, int* status);
+
 /* Copy a node or cell volume field to host memory (core region only, j
  * fastest; nn or nn-1 values per axis).  Names: vx vy vz ux uy uz ax ay az
  * (nodes; `a` holds the last acceleration) and lam mu yy vc (cells).
