@@ -520,11 +520,12 @@ def run_e2e(args, shape, inputs, device):
 
 
 def run_ensemble_bench(n, nthreads, device, nt=ENS_NT, seed=SEED):
-    """Batched rupture ensemble: scenarios 0..n-1 run one at a time, then
-    the same scenarios through one sord_run_ensemble call with `nthreads`
-    concurrent scenarios.  Each arm is timed by the host clock around the
-    whole call (setup from staged files, nt steps, outputs written): the
-    metric is scenarios/s of finished runs."""
+    """Batched rupture ensemble: scenarios 0..n-1 run one at a time by the
+    plain solver (one sord_run_directory call each), then the same scenarios
+    through one sord_run_ensemble call with `nthreads` concurrent scenarios.
+    Each arm is timed by the host clock around all its calls (setup from
+    staged files, nt steps, outputs written): the metric is scenarios/s of
+    finished runs."""
     from coseis_b200 import _lib
     work = tempfile.mkdtemp(prefix='sord_ens_')
     try:
@@ -532,7 +533,8 @@ def run_ensemble_bench(n, nthreads, device, nt=ENS_NT, seed=SEED):
         ens = stage_scenarios(range(n), os.path.join(work, 'batched'), seed, nt)
         _lib.run_ensemble(stage_scenarios([n], os.path.join(work, 'warm'), seed, 20), device, 1)
         t0 = time.time()
-        _lib.run_ensemble(ser, device, 1)
+        for d in ser:
+            _lib.run_directory(d, device)
         t_ser = time.time() - t0
         t0 = time.time()
         _lib.run_ensemble(ens, device, nthreads)

@@ -18,7 +18,7 @@ namespace sordgpu {
 
 float host_time_function(const std::string& pulse, float t, float dt, float tau);
 bool point_injection(Solver& s, IoOp& io, const FieldView& f, int comp, std::vector<Inject>& out);
-void probes_free(const Solver* s);
+void probes_free(Solver& s);
 
 // sord.in: the first line holds the values of the sorted parameter keys, one
 // field-I/O op per following line (cst/sord.py:538-544,
@@ -217,12 +217,25 @@ static float norm_max(Solver& s, float* const w[3]) {
     return dev_reduce_max(s, vol(s, s.d.s1), s.g.i1core, s.g.i2core);
 }
 
+// Fault-plane fields (the 'f' class of cst/sord.py:59-163): their outputs
+// are read between the fault kernels, which run beside the fused kernel.
+static bool fault_field(const std::string& f) {
+    static const char* const names[] = {"mus", "mud", "dc", "co", "tn", "ts", "td", "sxx", "syy", "szz", "syz",
+                                        "szx", "sxy", "nsx", "nsy", "nsz", "tx", "ty", "tz", "tsx", "tsy", "tsz",
+                                        "tnm", "tsm", "fr", "sax", "say", "saz", "sam", "svx", "svy", "svz", "svm",
+                                        "psv", "sux", "suy", "suz", "sum", "sl", "trup", "tarr"};
+    for (const char* n : names)
+        if (f == n) return true;
+    return false;
+}
+
 // Can step `n` run as one fused kernel?  Every field-I/O op firing at that
-// step must be an output of v, u, a or their magnitudes (read between
-// kernels) or a '.' point op on the potency / moment tensor (applied inside
-// the kernel); no fault, and no boundary condition that copies planes.
+// step must be an output of v, u, a or their magnitudes or of a fault-plane
+// field (read between kernels) or a '.' point op on the potency / moment
+// tensor (applied inside the kernel), and no boundary condition may copy
+// planes.  A fault is finished by its own kernels around the fused one.
 bool Solver::fusable(int n) const {
-    if (!use_fused || g.ifn != 0 || !bc_noop(prm)) return false;
+    if (!use_fused || !bc_noop(prm)) return false;
     for (auto& io : ops) {
         int it1 = io.ii[3][0], it2 = io.ii[3][1], dit = io.ii[3][2];
         if (n > it2 || io.op[0] == '#' || n < it1 || ((n - it1) % dit) != 0) continue;
@@ -231,7 +244,7 @@ bool Solver::fusable(int n) const {
         bool out = op2 == '>';
         if (out) {
             bool ok = f == "vx" || f == "vy" || f == "vz" || f == "ux" || f == "uy" || f == "uz" || f == "ax" ||
-                      f == "ay" || f == "az" || f == "vm2" || f == "um2" || f == "am2";
+                      f == "ay" || f == "az" || f == "vm2" || f == "um2" || f == "am2" || (g.ifn && fault_field(f));
             if (!ok) return false;
         } else {
             bool tensor = f[0] == 'p' || f[0] == 'm';
@@ -261,12 +274,19 @@ void Solver::step(bool last_in_call) {
         tio += clock_us() - t0;
     };
     // leapfrog update of this step, unless the previous fused step did it
+    // (for all nodes but the fault's, which fault_fold advances)
     tm = prm.tm0 + g.dt * (float)(it - 1);
-    if (!folded) launch_time_update(*this, false);
+    if (!folded) {
+        if (g.ifn) fault_time_pre(*this);
+        launch_time_update(*this, false);
+    } else if (g.ifn) {
+        fault_fold(*this);
+    }
     for (int i = 0; i < 3; i++) io("<>", kVel[i], vol(*this, d.v[i]));
     io(">", "vm2", vol(*this, d.s1));
     for (int i = 0; i < 3; i++) io("<>", kDis[i], vol(*this, d.u[i]));
     io(">", "um2", vol(*this, d.s1));
+    if (g.ifn && !folded) fault_time_post(*this);
     std::vector<Inject> pot, mom, frc;
     if (prm.source == "potency") finite_source_entries(*this, pot);
     if (prm.source == "moment") finite_source_entries(*this, mom);
@@ -279,6 +299,7 @@ void Solver::step(bool last_in_call) {
     const bool write_a = any_pass(*this, kAcc, 3, '>') || field_active(*this, "am2", '>') || it == nt;
     InjectList lp = upload(*this, 0, pot), lm = upload(*this, 1, mom), lf = upload(*this, 2, frc);
     launch_fused(*this, lp, lm, lf, pot, mom, frc, fold, write_a, st);
+    if (g.ifn) fault_rupture_fused(*this);
     folded = fold;
     for (int i = 0; i < 3; i++) io("<>", kAcc[i], vol(*this, d.w1n[i]));
     io(">", "am2", vol(*this, d.s1));
@@ -506,27 +527,35 @@ void Solver::prof_collect() {
 void Solver::destroy() {
     if (device >= 0) cudaSetDevice(device);
     if (stream) cudaStreamSynchronize(stream);
-    auto fr = [](void* p) { if (p) cudaFree(p); };
+    auto fr = [this](void* p) { dev_free(*this, p); };
     for (int i = 0; i < 3; i++) { fr(d.x[i]); fr(d.v[i]); fr(d.u[i]); fr(d.w1n[i]); fr(d.sd[i]); fr(d.so[i]); }
     fr(d.vc); fr(d.mr); fr(d.lam); fr(d.mu); fr(d.gam); fr(d.yy); fr(d.s1); fr(d.s2); fr(d.pmlc); fr(d.red); fr(d.inj); fr(d.fp);
     for (int i = 0; i < 6; i++) { fr(d.slabs.p[i]); fr(d.slabs.g[i]); fr(d.gb[i]); }
     for (int i = 0; i < 3; i++) { fr(d.vb[i]); fr(d.ub[i]); }
     fr(d.x1d); fr(d.y1d);
     for (auto& io : ops) fr(io.dbuf);
-    probes_free(this);
+    probes_free(*this);
     fused_free(*this);
     for (auto& p : prof_ev) { cudaEventDestroy(p.second.first); cudaEventDestroy(p.second.second); }
     prof_ev.clear();
-    if (hinj) cudaFreeHost(hinj);
-    if (d_stage) cudaFree(d_stage);
+    pinned_put(hinj);
+    fr(d_stage);
     for (int i = 0; i < 4; i++) {
-        if (pin_io[i]) cudaFreeHost(pin_io[i]);
+        pinned_put(pin_io[i]);
         if (pin_ev[i]) cudaEventDestroy(pin_ev[i]);
     }
     for (auto& e : inj_done) if (e) cudaEventDestroy(e);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
-    if (stream) cudaStreamDestroy(stream);
+    if (stream) {
+        cudaStreamSynchronize(stream);
+        cudaStreamDestroy(stream);
+    }
+    if (mem_attached) mem_detach(device);
+    mem_attached = false;
+    hinj = nullptr;
+    d_stage = nullptr;
+    for (auto& p : pin_io) p = nullptr;
     d = Device{};
     stream = nullptr;
 }
@@ -571,6 +600,8 @@ int sord_create(const char* workdir, const char* sord_in_text, int device, sord_
         s.clock0_us = 0;
         s.clock0_us = s.clock_us();
         SORD_CUDA(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+        mem_attach(device);
+        s.mem_attached = true;
         SORD_CUDA(cudaEventCreate(&s.ev0));
         SORD_CUDA(cudaEventCreate(&s.ev1));
         for (auto& e : s.inj_done) SORD_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));

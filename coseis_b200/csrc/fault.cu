@@ -214,21 +214,19 @@ struct RuptArgs {
 };
 
 // trial traction, slip-weakening friction, nucleation, force update
-// (dynamic_rupture.f90:268-334)
-__global__ void k_rupture(RuptArgs A) {
+// (dynamic_rupture.f90:268-334) at fault node q (volume nodes c1, c2);
+// returns the new traction t1
+__device__ __forceinline__ void rupture_node(const RuptArgs& A, long long q, long long c1, long long c2, float (&t1)[3]) {
     const Plane& P = A.P;
     float* F = A.F;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < P.np; q += (long long)gridDim.x * blockDim.x) {
-        int p[3];
-        plane_pos(P, q, p);
-        long long c1 = vol_minus(A.g, P, p), c2 = c1 + P.off;
+    {
         const float dt = A.dt;
         float m1 = A.mr[c1], m2 = A.mr[c2];
         float area = FA(F_AREA)[q];
         float f1 = dt * dt * area * (m1 + m2);
         if (f1 != 0.f) f1 = 1.0f / f1;
         float n[3] = {FA(F_NHAT)[q], FA(F_NHAT + 1)[q], FA(F_NHAT + 2)[q]};
-        float t0[3], t1[3], t2[3], t3[3];
+        float t0[3], t2[3], t3[3];
         for (int i = 0; i < 3; i++) {
             t0[i] = FA(F_T0 + i)[q];
             t1[i] = t0[i] + f1 * dt * (A.v[i][c2] - A.v[i][c1] + A.w[i][c2] * m2 * dt - A.w[i][c1] * m1 * dt);
@@ -272,6 +270,16 @@ __global__ void k_rupture(RuptArgs A) {
         FA(F_TS)[q] = ts;
         FA(F_F1)[q] = f1;
         FA(F_F2)[q] = f2;
+    }
+}
+__global__ void k_rupture(RuptArgs A) {
+    const Plane& P = A.P;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < P.np; q += (long long)gridDim.x * blockDim.x) {
+        int p[3];
+        plane_pos(P, q, p);
+        const long long c1 = vol_minus(A.g, P, p), c2 = c1 + P.off;
+        float t1[3];
+        rupture_node(A, q, c1, c2, t1);
     }
 }
 
@@ -327,6 +335,132 @@ __global__ void k_slip_accel(Geom g, Plane P, const float* w0, const float* w1, 
     }
 }
 
+// ------------------------------------------------------------ fused step
+// With the fused volume kernel, the two fault planes are finished here: the
+// volume kernel leaves their force in w and their v, u unchanged.
+
+__device__ __forceinline__ bool node_box(const Geom& g, long long c) {
+    const int j = (int)(c % g.sy) + 1, k = (int)((c / g.sy) % g.nm[1]) + 1, l = (int)(c / g.sz) + 1;
+    return j >= g.i1node[0] && j <= g.i2node[0] && k >= g.i1node[1] && k <= g.i2node[1] && l >= g.i1node[2] &&
+           l <= g.i2node[2];
+}
+__device__ __forceinline__ bool node_core(const Geom& g, long long c) {
+    const int j = (int)(c % g.sy) + 1, k = (int)((c / g.sy) % g.nm[1]) + 1, l = (int)(c / g.sz) + 1;
+    return j >= g.i1core[0] && j <= g.i2core[0] && k >= g.i1core[1] && k <= g.i2core[1] && l >= g.i1core[2] &&
+           l <= g.i2core[2];
+}
+__device__ __forceinline__ void block_max3(unsigned* dst, float v) {
+    unsigned b = __float_as_uint(v);
+    if (v != v) b = 0x7fc00000u;
+    for (int o = 16; o > 0; o >>= 1) b = max(b, __shfl_xor_sync(0xffffffffu, b, o));
+    __shared__ unsigned s[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    if (lane == 0) s[warp] = b;
+    __syncthreads();
+    if (warp == 0) {
+        b = lane < nw ? s[lane] : 0u;
+        for (int o = 16; o > 0; o >>= 1) b = max(b, __shfl_xor_sync(0xffffffffu, b, o));
+        if (lane == 0 && b) atomicMax(dst, b);
+    }
+}
+
+// Rupture of step n after the fused volume kernel: trial traction and
+// friction (rupture_node), the energy and moment partials of k_fault_energy,
+// the slip acceleration of k_slip_accel and the mass division of both fault
+// nodes (acceleration.f90:235-238) with their share of max |a|.
+__global__ void k_rupture_fused(RuptArgs A, double* part, int stats, unsigned* red) {
+    const Plane& P = A.P;
+    const Geom& g = A.g;
+    float* F = A.F;
+    double e0 = 0, e1 = 0, e2 = 0;
+    float am = 0.f;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < P.np; q += (long long)gridDim.x * blockDim.x) {
+        int p[3];
+        plane_pos(P, q, p);
+        const long long c1 = vol_minus(g, P, p), c2 = c1 + P.off;
+        float t1[3];
+        rupture_node(A, q, c1, c2, t1);
+        if (plane_core(g, P, p)) {
+            const float area = FA(F_AREA)[q];
+            const float t0[3] = {FA(F_T0)[q], FA(F_T0 + 1)[q], FA(F_T0 + 2)[q]};
+            const float dv[3] = {A.v[0][c2] - A.v[0][c1], A.v[1][c2] - A.v[1][c1], A.v[2][c2] - A.v[2][c1]};
+            const float du[3] = {A.u[0][c2] - A.u[0][c1], A.u[1][c2] - A.u[1][c1], A.u[2][c2] - A.u[2][c1]};
+            e0 += (double)((t1[0] * dv[0] + t1[1] * dv[1] + t1[2] * dv[2]) * area);
+            e1 += (double)(((t0[0] + t1[0]) * du[0] + (t0[1] + t1[1]) * du[1] + (t0[2] + t1[2]) * du[2]) * area);
+            e2 += (double)(FA(F_MUF)[q] * area * sqrtf(du[0] * du[0] + du[1] * du[1] + du[2] * du[2]));
+        }
+        const float m1 = A.mr[c1], m2 = A.mr[c2];
+        float a1[3], a2[3];
+        for (int i = 0; i < 3; i++) { a1[i] = A.w[i][c1] * m1; a2[i] = A.w[i][c2] * m2; }
+        const float sa = a2[0] - a1[0], sb = a2[1] - a1[1], sd = a2[2] - a1[2];
+        FA(F_T2)[q] = sa; FA(F_T2 + 1)[q] = sb; FA(F_T2 + 2)[q] = sd;
+        FA(F_F2)[q] = sqrtf(sa * sa + sb * sb + sd * sd);
+        if (node_box(g, c1)) {
+            for (int i = 0; i < 3; i++) A.w[i][c1] = a1[i];
+            if (stats && node_core(g, c1)) {
+                const float n = a1[0] * a1[0] + a1[1] * a1[1] + a1[2] * a1[2];
+                am = (n != n || n > am) ? n : am;
+            }
+        }
+        if (node_box(g, c2)) {
+            for (int i = 0; i < 3; i++) A.w[i][c2] = a2[i];
+            if (stats && node_core(g, c2)) {
+                const float n = a2[0] * a2[0] + a2[1] * a2[1] + a2[2] * a2[2];
+                am = (n != n || n > am) ? n : am;
+            }
+        }
+    }
+    __shared__ double s[3][256];
+    s[0][threadIdx.x] = e0; s[1][threadIdx.x] = e1; s[2][threadIdx.x] = e2;
+    __syncthreads();
+    for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+        if (threadIdx.x < k)
+            for (int i = 0; i < 3; i++) s[i][threadIdx.x] += s[i][threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int i = 0; i < 3; i++) part[3 * blockIdx.x + i] = s[i][0];
+    if (stats) block_max3(red + 0, am);
+}
+
+// Start of step n+1 for the two fault planes when the fused kernel of step
+// n folded the leapfrog update: the previous slip rate of k_fault_pre, the
+// update of both fault nodes (time_integration.f90:32-35) and the slip
+// bookkeeping of k_fault_post.
+__global__ void k_fault_fold(Geom g, Plane P, float* v0, float* v1, float* v2, float* u0, float* u1, float* u2,
+                             const float* w0, const float* w1, const float* w2, float* F, float tm, float dt, float svtol) {
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < P.np; q += (long long)gridDim.x * blockDim.x) {
+        int p[3];
+        plane_pos(P, q, p);
+        const long long c = vol_minus(g, P, p), c2 = c + P.off;
+        float a = v0[c2] - v0[c], b = v1[c2] - v1[c], d = v2[c2] - v2[c];
+        FA(F_T2)[q] = a; FA(F_T2 + 1)[q] = b; FA(F_T2 + 2)[q] = d;
+        FA(F_F2)[q] = sqrtf(a * a + b * b + d * d);
+        for (long long cc : {c, c2}) {
+            if (!node_box(g, cc)) continue;
+            float x;
+            x = v0[cc] + dt * w0[cc]; v0[cc] = x; u0[cc] = u0[cc] + dt * x;
+            x = v1[cc] + dt * w1[cc]; v1[cc] = x; u1[cc] = u1[cc] + dt * x;
+            x = v2[cc] + dt * w2[cc]; v2[cc] = x; u2[cc] = u2[cc] + dt * x;
+        }
+        a = v0[c2] - v0[c]; b = v1[c2] - v1[c]; d = v2[c2] - v2[c];
+        FA(F_T1)[q] = a; FA(F_T1 + 1)[q] = b; FA(F_T1 + 2)[q] = d;
+        float f1 = sqrtf(a * a + b * b + d * d);
+        FA(F_F1)[q] = f1;
+        FA(F_SL)[q] = FA(F_SL)[q] + dt * f1;
+        FA(F_PSV)[q] = fmax_(FA(F_PSV)[q], f1);
+        if (svtol > 0.f) {
+            float f2 = FA(F_F2)[q];
+            if (f1 >= svtol && FA(F_TRUP)[q] > 1e8f) FA(F_TRUP)[q] = tm - dt * (0.5f + (svtol - f1) / (f2 - f1));
+            if (f1 >= svtol) FA(F_TARR)[q] = 1e9f;
+            if (f1 < svtol && f2 >= svtol) FA(F_TARR)[q] = tm - dt * (0.5f + (svtol - f1) / (f2 - f1));
+        }
+        a = u0[c2] - u0[c]; b = u1[c2] - u1[c]; d = u2[c2] - u2[c];
+        FA(F_T2)[q] = a; FA(F_T2 + 1)[q] = b; FA(F_T2 + 2)[q] = d;
+        FA(F_F2)[q] = sqrtf(a * a + b * b + d * d);
+    }
+}
+
 // ------------------------------------------------------------ host
 static unsigned gp(long long n) {
     long long b = (n + 255) / 256;
@@ -363,7 +497,7 @@ void fault_init(Solver& s) {
     for (int i = 0; i < 3; i++) s.fn3[i] = g.nm[i];
     s.fn3[g.ifn - 1] = 1;
     s.d.np = (long long)s.fn3[0] * s.fn3[1] * s.fn3[2];
-    SORD_CUDA(cudaMalloc((void**)&s.d.fp, sizeof(float) * (size_t)(F_COUNT * s.d.np)));
+    SORD_CUDA(dev_malloc(s, (void**)&s.d.fp, sizeof(float) * (size_t)(F_COUNT * s.d.np)));
     SORD_CUDA(cudaMemsetAsync(s.d.fp, 0, sizeof(float) * (size_t)(F_COUNT * s.d.np), s.stream));
     SORD_CUDA(cudaMemsetAsync(energy_acc(s), 0, sizeof(double) * 3, s.stream));
     Plane P = plane_of(s);
@@ -436,11 +570,18 @@ void fault_time_pre(Solver& s) {
     k_fault_pre<<<gp(P.np), 256, 0, s.stream>>>(s.g, P, s.d.v[0], s.d.v[1], s.d.v[2], s.d.fp); LCHK(s);
 }
 
+static void fault_post_outputs(Solver& s);
+
 void fault_time_post(Solver& s) {
     Plane P = plane_of(s);
     k_fault_post<<<gp(P.np), 256, 0, s.stream>>>(s.g, P, s.d.v[0], s.d.v[1], s.d.v[2], s.d.u[0], s.d.u[1], s.d.u[2], s.d.fp,
                                                  s.tm, s.g.dt, s.prm.svtol);
     LCHK(s);
+    fault_post_outputs(s);
+}
+
+// outputs and statistics of the slip bookkeeping (time_integration.f90:94-113)
+static void fault_post_outputs(Solver& s) {
     field_io(s, ">", "svx", pv(s, F_T1));
     field_io(s, ">", "svy", pv(s, F_T1 + 1));
     field_io(s, ">", "svz", pv(s, F_T1 + 2));
@@ -463,12 +604,11 @@ void fault_time_post(Solver& s) {
     }
 }
 
-void fault_rupture(Solver& s) {
-    Plane P = plane_of(s);
+static RuptArgs rupt_args(Solver& s) {
     Params& Pm = s.prm;
     RuptArgs A;
     A.g = s.g;
-    A.P = P;
+    A.P = plane_of(s);
     for (int i = 0; i < 3; i++) { A.v[i] = s.d.v[i]; A.u[i] = s.d.u[i]; A.w[i] = s.d.w1n[i]; }
     A.mr = s.d.mr;
     A.F = s.d.fp;
@@ -479,8 +619,11 @@ void fault_rupture(Solver& s) {
     A.trelax = Pm.trelax;
     A.it = s.it;
     A.faultopening = Pm.faultopening;
-    k_rupture<<<gp(P.np), 256, 0, s.stream>>>(A); LCHK(s);
-    launch_vector_bc(s, s.d.w1n, Pm.bc1, Pm.bc2, s.g.i1bc, s.g.i2bc);
+    return A;
+}
+
+// outputs and statistics of the traction and friction (dynamic_rupture.f90:336-352)
+static void rupture_outputs(Solver& s, bool st, const int* a1, const int* a2) {
     field_io(s, ">", "tx", pv(s, F_T1));
     field_io(s, ">", "ty", pv(s, F_T1 + 1));
     field_io(s, ">", "tz", pv(s, F_T1 + 2));
@@ -490,19 +633,15 @@ void fault_rupture(Solver& s) {
     field_io(s, ">", "tsm", pv(s, F_TS));
     field_io(s, ">", "tnm", pv(s, F_TN));
     field_io(s, ">", "fr", pv(s, F_F1));
-    bool st = s.it % s.prm.itstats == 0;
-    int a1[3], a2[3];
-    core_box(s, a1, a2);
     if (st) {
         s.tsmax = std::max(-1.0f, dev_reduce_max(s, pv(s, F_TS), a1, a2));
         s.tnmin = dev_reduce_min(s, pv(s, F_TN), a1, a2);
         s.tnmax = dev_reduce_max(s, pv(s, F_TN), a1, a2);
     }
-    double* part = (double*)s.d.red + kRedPart;
-    unsigned nb = gp(P.np);
-    k_fault_energy<<<nb, 256, 0, s.stream>>>(s.g, P, s.d.v[0], s.d.v[1], s.d.v[2], s.d.u[0], s.d.u[1], s.d.u[2], s.d.fp, part); LCHK(s);
-    k_fault_energy_fin<<<1, 32, 0, s.stream>>>(part, (int)nb, energy_acc(s), (double)s.g.dt); LCHK(s);
-    k_slip_accel<<<gp(P.np), 256, 0, s.stream>>>(s.g, P, s.d.w1n[0], s.d.w1n[1], s.d.w1n[2], s.d.mr, s.d.fp); LCHK(s);
+}
+
+// outputs of the slip acceleration and the energy statistics (dynamic_rupture.f90:371-384)
+static void slip_accel_outputs(Solver& s, bool st, const int* a1, const int* a2) {
     field_io(s, ">", "sax", pv(s, F_T2));
     field_io(s, ">", "say", pv(s, F_T2 + 1));
     field_io(s, ">", "saz", pv(s, F_T2 + 2));
@@ -514,6 +653,53 @@ void fault_rupture(Solver& s) {
         SORD_CUDA(cudaStreamSynchronize(s.stream));
         s.efric = e[0]; s.estrain = e[1]; s.moment = e[2];
     }
+}
+
+void fault_rupture(Solver& s) {
+    RuptArgs A = rupt_args(s);
+    const Plane& P = A.P;
+    Params& Pm = s.prm;
+    k_rupture<<<gp(P.np), 256, 0, s.stream>>>(A); LCHK(s);
+    launch_vector_bc(s, s.d.w1n, Pm.bc1, Pm.bc2, s.g.i1bc, s.g.i2bc);
+    const bool st = s.it % s.prm.itstats == 0;
+    int a1[3], a2[3];
+    core_box(s, a1, a2);
+    rupture_outputs(s, st, a1, a2);
+    double* part = (double*)s.d.red + kRedPart;
+    unsigned nb = gp(P.np);
+    k_fault_energy<<<nb, 256, 0, s.stream>>>(s.g, P, s.d.v[0], s.d.v[1], s.d.v[2], s.d.u[0], s.d.u[1], s.d.u[2], s.d.fp, part); LCHK(s);
+    k_fault_energy_fin<<<1, 32, 0, s.stream>>>(part, (int)nb, energy_acc(s), (double)s.g.dt); LCHK(s);
+    k_slip_accel<<<gp(P.np), 256, 0, s.stream>>>(s.g, P, s.d.w1n[0], s.d.w1n[1], s.d.w1n[2], s.d.mr, s.d.fp); LCHK(s);
+    slip_accel_outputs(s, st, a1, a2);
+}
+
+// The fault half of a fused step, after the fused volume kernel (whose
+// boundary conditions are no-ops, so vector_bc is skipped): rupture, energy
+// sums, slip acceleration and the mass division of the fault nodes in one
+// kernel, then the same outputs and statistics as fault_rupture.
+void fault_rupture_fused(Solver& s) {
+    RuptArgs A = rupt_args(s);
+    const Plane& P = A.P;
+    const bool st = s.it % s.prm.itstats == 0;
+    double* part = (double*)s.d.red + kRedPart;
+    unsigned nb = gp(P.np);
+    k_rupture_fused<<<nb, 256, 0, s.stream>>>(A, part, st ? 1 : 0, (unsigned*)s.d.red); LCHK(s);
+    k_fault_energy_fin<<<1, 32, 0, s.stream>>>(part, (int)nb, energy_acc(s), (double)s.g.dt); LCHK(s);
+    int a1[3], a2[3];
+    core_box(s, a1, a2);
+    rupture_outputs(s, st, a1, a2);
+    slip_accel_outputs(s, st, a1, a2);
+}
+
+// Start of a step after a folded fused step: previous slip rate, leapfrog
+// update of the fault nodes and slip bookkeeping in one kernel, then the
+// outputs of fault_time_post.
+void fault_fold(Solver& s) {
+    Plane P = plane_of(s);
+    k_fault_fold<<<gp(P.np), 256, 0, s.stream>>>(s.g, P, s.d.v[0], s.d.v[1], s.d.v[2], s.d.u[0], s.d.u[1], s.d.u[2],
+                                                 s.d.w1n[0], s.d.w1n[1], s.d.w1n[2], s.d.fp, s.tm, s.g.dt, s.prm.svtol);
+    LCHK(s);
+    fault_post_outputs(s);
 }
 
 }  // namespace sordgpu

@@ -323,19 +323,19 @@ static int probe_id(Solver& s, size_t opi, const IoOp& io, const FieldView& f) {
                 pr.n++;
             }
     T.host.push_back(pr);
-    if (T.dev) cudaFree(T.dev);
-    SORD_CUDA(cudaMalloc((void**)&T.dev, sizeof(Probe) * T.host.size()));
+    dev_free(s, T.dev);
+    SORD_CUDA(dev_malloc(s, (void**)&T.dev, sizeof(Probe) * T.host.size()));
     SORD_CUDA(cudaMemcpyAsync(T.dev, T.host.data(), sizeof(Probe) * T.host.size(), cudaMemcpyHostToDevice, s.stream));
     SORD_CUDA(cudaStreamSynchronize(s.stream));
     T.id_of_op[opi] = (int)T.host.size() - 1;
     return T.id_of_op[opi];
 }
 
-void probes_free(const Solver* s) {
+void probes_free(Solver& s) {
     std::lock_guard<std::mutex> lock(g_probes_m);
-    auto it = g_probes.find(s);
+    auto it = g_probes.find(&s);
     if (it != g_probes.end()) {
-        if (it->second.dev) cudaFree(it->second.dev);
+        dev_free(s, it->second.dev);
         g_probes.erase(it);
     }
 }
@@ -355,7 +355,8 @@ static void flush_output(Solver& s, IoOp& io, int n3[3], int m3[3]) {
     }
     io.ib = 0;
     if (s.it == it2 || n3[0] < 1 || n3[1] < 1 || n3[2] < 1 || n4 < 1) {
-        if (io.dbuf) { cudaFree(io.dbuf); io.dbuf = nullptr; }
+        dev_free(s, io.dbuf);
+        io.dbuf = nullptr;
         io.op = "#";
     }
 }
@@ -380,7 +381,7 @@ static void read_to_device(Solver& s, const std::string& fn, size_t off, size_t 
     static_assert(kReaders <= (int)(sizeof(s.pin_io) / sizeof(s.pin_io[0])), "pinned buffers");
     for (int i = 0; i < kReaders; i++)
         if (!s.pin_io[i]) {
-            SORD_CUDA(cudaMallocHost((void**)&s.pin_io[i], sizeof(float) * kChunk));
+            s.pin_io[i] = (float*)pinned_get(sizeof(float) * kChunk);
             SORD_CUDA(cudaEventCreateWithFlags(&s.pin_ev[i], cudaEventDisableTiming));
         }
     const int fd = open(s.path(fn).c_str(), O_RDONLY);
@@ -433,10 +434,10 @@ static bool device_volume_input(Solver& s, IoOp& io, FieldView f, const int* i1,
     const size_t nsp = (size_t)n[0] * n[1] * n[2];
     if (nsp == 0) return false;
     if (s.stage_cap < nsp) {
-        if (s.d_stage) SORD_CUDA(cudaFree(s.d_stage));
+        dev_free(s, s.d_stage);
         s.d_stage = nullptr;
         s.stage_cap = 0;
-        if (cudaMalloc((void**)&s.d_stage, sizeof(float) * (nsp + 1)) != cudaSuccess) {
+        if (dev_malloc(s, (void**)&s.d_stage, sizeof(float) * (nsp + 1)) != cudaSuccess) {
             cudaGetLastError();
             throw SordError(SORD_E_NOMEM, "cannot allocate the input staging record");
         }
@@ -675,7 +676,7 @@ static void field_io_op(Solver& s, size_t opi, FieldView f, ProbeBatch& batch) {
         if (io.ib < 0) {
             io.bufn = std::max(nsp, 0);
             size_t bytes = sizeof(float) * (size_t)std::max(io.bufn * io.nb, 1);
-            cudaError_t e = cudaMalloc((void**)&io.dbuf, bytes);
+            cudaError_t e = dev_malloc(s, (void**)&io.dbuf, bytes);
             if (e != cudaSuccess) throw SordError(SORD_E_NOMEM, "output buffer: " + std::string(cudaGetErrorString(e)));
             io.ib = 0;
             io.open = false;

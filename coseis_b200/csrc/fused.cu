@@ -105,6 +105,50 @@ __device__ __forceinline__ void bmax(unsigned* dst, float v) {
 }
 __device__ __forceinline__ float fmaxn(float m, float c) { return (c != c || c > m) ? c : m; }
 
+// Mass, statistics, acceleration output and the folded leapfrog update of
+// node q = (jn, kn, l) with force f (acceleration.f90:235-238,
+// time_integration.f90:32-35).  A node on either plane of a double-node
+// fault keeps its force: the rupture step adds the fault traction to it,
+// divides by the mass and, when the step is folded, advances its v and u;
+// the fold copies its v and u into the new buffers.
+__device__ __forceinline__ void finish_node(const StepArgs& A, long long q, int jn, int kn, int l, float (&f)[3],
+                                            float m, const float (&uv)[6], float dt, float& st_a, float& st_v,
+                                            float& st_u) {
+    const int fc = A.fax == 0 ? jn : A.fax == 1 ? kn : l;
+    const bool fnode = A.fax >= 0 && (unsigned)(fc - A.firup) <= 1u;
+    const float u0 = uv[0], u1 = uv[1], u2 = uv[2], v0 = uv[3], v1 = uv[4], v2 = uv[5];
+    if (fnode) {
+#pragma unroll
+        for (int i = 0; i < 3; i++) A.fout[i][q] = f[i];
+        if (A.stats) {
+            st_v = fmaxn(st_v, v0 * v0 + v1 * v1 + v2 * v2);
+            st_u = fmaxn(st_u, u0 * u0 + u1 * u1 + u2 * u2);
+        }
+        if (A.fold) {
+            A.vout[0][q] = v0; A.uout[0][q] = u0;
+            A.vout[1][q] = v1; A.uout[1][q] = u1;
+            A.vout[2][q] = v2; A.uout[2][q] = u2;
+        }
+        return;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; i++) f[i] = f[i] * m;
+    if (A.stats) {
+        st_a = fmaxn(st_a, f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
+        st_v = fmaxn(st_v, v0 * v0 + v1 * v1 + v2 * v2);
+        st_u = fmaxn(st_u, u0 * u0 + u1 * u1 + u2 * u2);
+    }
+    if (A.aout[0])
+#pragma unroll
+        for (int i = 0; i < 3; i++) A.aout[i][q] = f[i];
+    if (A.fold) {
+        float a, b;
+        a = v0 + dt * f[0]; b = u0 + dt * a; A.vout[0][q] = a; A.uout[0][q] = b;
+        a = v1 + dt * f[1]; b = u1 + dt * a; A.vout[1][q] = a; A.uout[1][q] = b;
+        a = v2 + dt * f[2]; b = u2 + dt * a; A.vout[2][q] = a; A.uout[2][q] = b;
+    }
+}
+
 __device__ __forceinline__ long long slab_idx(const Geom& g, int axis, int t, int ii, int j, int k, int l, int ic) {
     long long e0 = axis == 0 ? t : g.nm[0], e1 = axis == 1 ? t : g.nm[1], e2 = axis == 2 ? t : g.nm[2];
     long long a0 = axis == 0 ? ii : j - 1, a1 = axis == 1 ? ii : k - 1, a2 = axis == 2 ? ii : l - 1;
@@ -607,25 +651,7 @@ __global__ void __launch_bounds__(SJ * SK, GEOM == GEOM_GENERAL ? 1 : 2) k_shell
                     else f[2] = f[2] + inc;
                 }
         }
-        const float m = cur[4];
-#pragma unroll
-        for (int i = 0; i < 3; i++) f[i] = f[i] * m;
-        const float u0 = uv[0], u1 = uv[1], u2 = uv[2], v0 = uv[3], v1 = uv[4], v2 = uv[5];
-        if (A.stats) {
-            st_a = fmaxn(st_a, f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
-            st_v = fmaxn(st_v, v0 * v0 + v1 * v1 + v2 * v2);
-            st_u = fmaxn(st_u, u0 * u0 + u1 * u1 + u2 * u2);
-        }
-        if (A.aout[0])
-#pragma unroll
-            for (int i = 0; i < 3; i++) A.aout[i][q] = f[i];
-        if (A.fold) {
-            // leapfrog update of the next step (time_integration.f90:32-35)
-            float a, b;
-            a = v0 + dt * f[0]; b = u0 + dt * a; A.vout[0][q] = a; A.uout[0][q] = b;
-            a = v1 + dt * f[1]; b = u1 + dt * a; A.vout[1][q] = a; A.uout[1][q] = b;
-            a = v2 + dt * f[2]; b = u2 + dt * a; A.vout[2][q] = a; A.uout[2][q] = b;
-        }
+        finish_node(A, q, jn, kn, l, f, cur[4], uv, dt, st_a, st_v, st_u);
     };
 
     // ---------------------------------------------------------------- stream
@@ -1339,25 +1365,7 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
                     else f[2] = f[2] + inc;
                 }
         }
-        const float m = cur[4];
-#pragma unroll
-        for (int i = 0; i < 3; i++) f[i] = f[i] * m;
-        const float u0 = uv[0], u1 = uv[1], u2 = uv[2], v0 = uv[3], v1 = uv[4], v2 = uv[5];
-        if (A.stats) {
-            st_a = fmaxn(st_a, f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
-            st_v = fmaxn(st_v, v0 * v0 + v1 * v1 + v2 * v2);
-            st_u = fmaxn(st_u, u0 * u0 + u1 * u1 + u2 * u2);
-        }
-        if (A.aout[0])
-#pragma unroll
-            for (int i = 0; i < 3; i++) A.aout[i][q] = f[i];
-        if (A.fold) {
-            // leapfrog update of the next step (time_integration.f90:32-35)
-            float a, b;
-            a = v0 + dt * f[0]; b = u0 + dt * a; A.vout[0][q] = a; A.uout[0][q] = b;
-            a = v1 + dt * f[1]; b = u1 + dt * a; A.vout[1][q] = a; A.uout[1][q] = b;
-            a = v2 + dt * f[2]; b = u2 + dt * a; A.vout[2][q] = a; A.uout[2][q] = b;
-        }
+        finish_node(A, q, jn, kn, l, f, cur[4], uv, dt, st_a, st_v, st_u);
     };
 
     // ---------------------------------------------------------------- stream
@@ -1419,6 +1427,8 @@ struct FusedPlan {
     int jf = 0, jend = -1, kf = 0, kend = -1;   // interior rectangle (inclusive)
     int nbx = 0, nby = 0;                       // interior tiles
     int lf0 = 0, lf1 = -1;                      // interior node planes (inclusive)
+    int segl = 0, nseg = 1;                     // interior planes per block, blocks per column
+    int ipl = 96;                               // deepest shell item
     std::vector<int> base;                      // shell items without point sources (6 ints each)
     std::vector<int> cur;                       // items of the last upload
     int* d_items = nullptr;
@@ -1438,22 +1448,28 @@ void fused_free(Solver& s) {
     if (P->fork) cudaEventDestroy(P->fork);
     if (P->join) cudaEventDestroy(P->join);
     if (P->side) cudaStreamDestroy(P->side);
-    if (P->d_items) cudaFree(P->d_items);
-    if (P->h_items) cudaFreeHost(P->h_items);
+    dev_free(s, P->d_items);
+    pinned_put(P->h_items);
     delete P;
     s.fplan = nullptr;
 }
 
-static constexpr int kItemPlanes = 96;  // deepest shell item, for load balance
+// Planes per block.  Each block streams its column through the planes, so
+// a small mesh is cut into shorter plane ranges until both kernels have
+// about kWaveBlocks blocks per SM; a range starts with a prologue of about
+// two planes, so it is kept at kMinPlanes planes or more.
+static constexpr int kItemPlanes = 96;
+static constexpr int kMinPlanes = 8;
+static constexpr int kWaveBlocks = 4;
 
 // shell items covering node box [j1, j2] x [k1, k2] x [l1, l2]
-static void push_box(std::vector<int>& v, int j1, int j2, int k1, int k2, int l1, int l2) {
+static void push_box(std::vector<int>& v, int ipl, int j1, int j2, int k1, int k2, int l1, int l2) {
     if (j1 > j2 || k1 > k2 || l1 > l2) return;
-    for (int a = l1; a <= l2; a += kItemPlanes)
+    for (int a = l1; a <= l2; a += ipl)
         for (int k = k1; k <= k2; k += SK - 1)
             for (int j = j1; j <= j2; j += SJ - 1) {
                 const int it[6] = {j, k, std::min(j2, j + SJ - 2), std::min(k2, k + SK - 2), a,
-                                   std::min(l2, a + kItemPlanes - 1)};
+                                   std::min(l2, a + ipl - 1)};
                 v.insert(v.end(), it, it + 6);
             }
 }
@@ -1485,22 +1501,42 @@ static FusedPlan& fused_plan(Solver& s) {
     }
     const bool inner = P->jend >= P->jf && P->kend >= P->kf && P->lf1 >= P->lf0;
     const int L1 = g.i1node[2], L2 = g.i2node[2];
+    int sms = 148;
+    SORD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s.device));
+    const int want = kWaveBlocks * sms;
+    auto shell = [&](int ipl) {
+        std::vector<int> v;
+        if (!inner) {
+            push_box(v, ipl, g.i1node[0], g.i2node[0], g.i1node[1], g.i2node[1], L1, L2);
+        } else {
+            push_box(v, ipl, g.i1node[0], P->jf - 1, g.i1node[1], g.i2node[1], L1, L2);
+            push_box(v, ipl, P->jend + 1, g.i2node[0], g.i1node[1], g.i2node[1], L1, L2);
+            push_box(v, ipl, P->jf, P->jend, g.i1node[1], P->kf - 1, L1, L2);
+            push_box(v, ipl, P->jf, P->jend, P->kend + 1, g.i2node[1], L1, L2);
+            push_box(v, ipl, P->jf, P->jend, P->kf, P->kend, L1, P->lf0 - 1);
+            push_box(v, ipl, P->jf, P->jend, P->kf, P->kend, P->lf1 + 1, L2);
+        }
+        return v;
+    };
+    P->ipl = kItemPlanes;
+    P->base = shell(P->ipl);
+    while (P->ipl > kMinPlanes && (int)P->base.size() / 6 < want) {
+        P->ipl = std::max(kMinPlanes, P->ipl * 2 / 3);
+        P->base = shell(P->ipl);
+    }
     if (!inner) {
-        push_box(P->base, g.i1node[0], g.i2node[0], g.i1node[1], g.i2node[1], L1, L2);
         P->jend = P->jf - 1;
     } else {
         P->nbx = (int)div_up(P->jend - P->jf + 1, FOJ);
         P->nby = (int)div_up(P->kend - P->kf + 1, FOK);
-        push_box(P->base, g.i1node[0], P->jf - 1, g.i1node[1], g.i2node[1], L1, L2);
-        push_box(P->base, P->jend + 1, g.i2node[0], g.i1node[1], g.i2node[1], L1, L2);
-        push_box(P->base, P->jf, P->jend, g.i1node[1], P->kf - 1, L1, L2);
-        push_box(P->base, P->jf, P->jend, P->kend + 1, g.i2node[1], L1, L2);
-        push_box(P->base, P->jf, P->jend, P->kf, P->kend, L1, P->lf0 - 1);
-        push_box(P->base, P->jf, P->jend, P->kf, P->kend, P->lf1 + 1, L2);
+        const int planes = P->lf1 - P->lf0 + 1, cols = P->nbx * P->nby;
+        const int nseg = std::max(1, std::min((want + cols - 1) / cols, planes / kMinPlanes));
+        P->segl = (planes + nseg - 1) / nseg;
+        P->nseg = (planes + P->segl - 1) / P->segl;
     }
     P->cap = (int)P->base.size() / 6 + 4096;
-    SORD_CUDA(cudaMalloc((void**)&P->d_items, sizeof(int) * 6 * P->cap));
-    SORD_CUDA(cudaMallocHost((void**)&P->h_items, sizeof(int) * 6 * P->cap));
+    SORD_CUDA(dev_malloc(s, (void**)&P->d_items, sizeof(int) * 6 * P->cap));
+    P->h_items = (int*)pinned_get(sizeof(int) * 6 * P->cap);
     SORD_CUDA(cudaEventCreateWithFlags(&P->done, cudaEventDisableTiming));
     SORD_CUDA(cudaEventCreateWithFlags(&P->fork, cudaEventDisableTiming));
     SORD_CUDA(cudaEventCreateWithFlags(&P->join, cudaEventDisableTiming));
@@ -1581,9 +1617,12 @@ void launch_fused(Solver& s, const InjectList& pot, const InjectList& mom, const
     A.kend = P.kend;
     A.lf0 = P.lf0;
     A.lf1 = P.lf1;
-    A.segl = P.lf1 - P.lf0 + 1;
+    A.segl = P.segl;
     A.items = P.d_items;
     A.negzero = -0.0f;
+    A.fax = s.g.ifn - 1;
+    A.firup = s.g.irup;
+    for (int i = 0; i < 3; i++) A.fout[i] = d.w1n[i];
 
     // shell items of this step: the fixed list, plus the interior planes of
     // the interior tiles holding a point source
@@ -1598,7 +1637,7 @@ void launch_fused(Solver& s, const InjectList& pot, const InjectList& mom, const
     std::vector<int> items(P.base);
     for (auto& c : src) {
         const int j0 = P.jf + c.first * FOJ, k0 = P.kf + c.second * FOK;
-        push_box(items, j0, std::min(P.jend, j0 + FOJ - 1), k0, std::min(P.kend, k0 + FOK - 1), P.lf0, P.lf1);
+        push_box(items, P.ipl, j0, std::min(P.jend, j0 + FOJ - 1), k0, std::min(P.kend, k0 + FOK - 1), P.lf0, P.lf1);
     }
     const int nitems = (int)items.size() / 6;
     if (items != P.cur) {
@@ -1613,7 +1652,7 @@ void launch_fused(Solver& s, const InjectList& pot, const InjectList& mom, const
     cudaEvent_t e0 = nullptr;
     s.prof_begin(KC_FUSED, &e0);
     const bool inner = P.nbx > 0 && P.nby > 0;
-    const dim3 igrid(P.nbx, P.nby, 1);
+    const dim3 igrid(P.nbx, P.nby, P.nseg);
     if (inner && nitems > 0) {
         SORD_CUDA(cudaEventRecord(P.fork, s.stream));
         SORD_CUDA(cudaStreamWaitEvent(P.side, P.fork, 0));

@@ -277,8 +277,8 @@ static FieldView vol(Solver& s, float* p) {
 }
 
 static void alloc(Solver& s, float** p, long long n) {
-    cudaError_t e = cudaMalloc((void**)p, sizeof(float) * (size_t)(n > 0 ? n : 1));
-    if (e != cudaSuccess) throw SordError(SORD_E_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    cudaError_t e = dev_malloc(s, (void**)p, sizeof(float) * (size_t)(n > 0 ? n : 1));
+    if (e != cudaSuccess) throw SordError(SORD_E_NOMEM, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
     SORD_CUDA(cudaMemsetAsync(*p, 0, sizeof(float) * (size_t)(n > 0 ? n : 1), s.stream));
 }
 
@@ -347,8 +347,8 @@ static void allocate_arrays(Solver& s) {
     for (int i = 0; i < 3; i++) { alloc(s, &d.vb[i], nv); alloc(s, &d.ub[i], nv); }
     const char* fz = getenv("SORD_FUSED");
     s.use_fused = !(fz && fz[0] == '0');
-    SORD_CUDA(cudaMalloc((void**)&d.inj, sizeof(Inject) * kInjectSlots * kMaxInject));
-    SORD_CUDA(cudaMallocHost((void**)&s.hinj, sizeof(Inject) * kInjectSlots * kMaxInject));
+    SORD_CUDA(dev_malloc(s, (void**)&d.inj, sizeof(Inject) * kInjectSlots * kMaxInject));
+    s.hinj = (Inject*)pinned_get(sizeof(Inject) * kInjectSlots * kMaxInject);
 }
 
 static void init_grid(Solver& s) {

@@ -149,6 +149,11 @@ struct StepArgs {
     int jf, kf, jend, kend, lf0, lf1;
     const int* items;
     float negzero;  // -0.0, the addend of packed products (pair.cuh)
+    // double-node fault: normal axis (0..2, -1 without a fault) and the
+    // minus-side node index; nodes of planes firup and firup + 1 keep their
+    // force in fout, unscaled, and their v, u are copied by the fold
+    int fax, firup;
+    float* fout[3];
 };
 
 // Device state of one handle.
@@ -209,6 +214,8 @@ void setup_all(Solver& s);
 void fault_time_pre(Solver& s);
 void fault_time_post(Solver& s);
 void fault_rupture(Solver& s);
+void fault_rupture_fused(Solver& s);
+void fault_fold(Solver& s);
 // fieldio.cu
 struct FieldView {
     float* p;
@@ -284,6 +291,7 @@ struct Solver {
     cudaEvent_t pin_ev[4] = {nullptr, nullptr, nullptr, nullptr};
     // work decomposition of the fused step kernels (fused.cu)
     FusedPlan* fplan = nullptr;
+    bool mem_attached = false;  // holds a reference on the device's memory pool
     cudaEvent_t inj_done[kInjectSlots] = {};
     // fault bookkeeping
     int fn3[3] = {0, 0, 0};
@@ -303,6 +311,12 @@ struct Solver {
 };
 
 void smem_limit(const void* func, int bytes);
+void mem_attach(int device);
+void mem_detach(int device);
+cudaError_t dev_malloc(Solver& s, void** p, size_t bytes);
+void dev_free(Solver& s, void* p);
+void* pinned_get(size_t bytes);
+void pinned_put(void* p);
 
 // cell / node counts for launches
 inline unsigned div_up(long long a, long long b) { return (unsigned)((a + b - 1) / b); }

@@ -1,6 +1,8 @@
 // Device helpers used by setup, field I/O and statistics: fills, set_halo
 // (utilities.f90:103-117), region reductions, vector/tensor norms
 // (utilities.f90:120-165) and rinvert (utilities.f90:40-49).
+#include <cstdint>
+#include <map>
 #include <mutex>
 #include <set>
 #include <utility>
@@ -189,16 +191,89 @@ void dev_tensor_norm(Solver& s, float* dst, float* const a[3], float* const bb[3
 }
 
 // Raise a kernel's dynamic shared-memory limit once per device; safe when
-// several host threads launch on one or more devices.
+// several host threads launch on one or more devices (each thread remembers
+// what it has seen, so the shared set is consulted once per thread).
 void smem_limit(const void* func, int bytes) {
     static std::mutex m;
     static std::set<std::pair<int, const void*>> done;
+    thread_local std::set<std::pair<int, const void*>> seen;
     int dev = 0;
     SORD_CUDA(cudaGetDevice(&dev));
+    if (seen.count({dev, func})) return;
     std::lock_guard<std::mutex> lock(m);
-    if (done.count({dev, func})) return;
-    SORD_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-    done.insert({dev, func});
+    if (!done.count({dev, func})) {
+        SORD_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        done.insert({dev, func});
+    }
+    seen.insert({dev, func});
+}
+
+// ------------------------------------------------------------ memory
+// Device memory of a handle comes from the device's default memory pool in
+// stream order (cudaMallocAsync / cudaFreeAsync on the handle's stream):
+// unlike cudaMalloc and cudaFree, neither call synchronises the device, so
+// handles that run concurrently (an ensemble) do not serialise each other's
+// setup and teardown.  While any handle is alive the pool keeps freed
+// memory for the next allocation; when the last one goes it is trimmed.
+static std::mutex g_mem_m;
+static std::map<int, int> g_live;  // device -> live handles
+
+void mem_attach(int device) {
+    std::lock_guard<std::mutex> lock(g_mem_m);
+    if (g_live[device]++ == 0) {
+        cudaMemPool_t pool;
+        SORD_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+        uint64_t keep = ~0ull;
+        SORD_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    }
+}
+
+void mem_detach(int device) {
+    std::lock_guard<std::mutex> lock(g_mem_m);
+    if (--g_live[device] == 0) {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+            uint64_t keep = 0;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+            cudaMemPoolTrimTo(pool, 0);
+        }
+    }
+}
+
+cudaError_t dev_malloc(Solver& s, void** p, size_t bytes) {
+    return cudaMallocAsync(p, bytes > 0 ? bytes : 4, s.stream);
+}
+
+void dev_free(Solver& s, void* p) {
+    if (p) cudaFreeAsync(p, s.stream);
+}
+
+// Pinned host buffers, kept for reuse by later handles: cudaMallocHost
+// synchronises the device, so a buffer is allocated only when no free one
+// is large enough.
+static std::multimap<size_t, void*> g_pin_free;
+static std::map<void*, size_t> g_pin_size;
+
+void* pinned_get(size_t bytes) {
+    std::lock_guard<std::mutex> lock(g_mem_m);
+    auto it = g_pin_free.lower_bound(bytes);
+    if (it != g_pin_free.end()) {
+        void* p = it->second;
+        g_pin_free.erase(it);
+        return p;
+    }
+    void* p = nullptr;
+    SORD_CUDA(cudaMallocHost(&p, bytes));
+    g_pin_size[p] = bytes;
+    return p;
+}
+
+void pinned_put(void* p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(g_mem_m);
+    auto it = g_pin_size.find(p);
+    if (it == g_pin_size.end()) return;
+    g_pin_free.insert({it->second, p});
 }
 
 }  // namespace sordgpu

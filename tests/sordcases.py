@@ -201,6 +201,42 @@ def interior_wave_inputs(path):
     wave_inputs(path, WAVE_INTERIOR)
 
 
+def case_fault_x(nt=20):
+    """x-normal slip-weakening fault with forced nucleation, PML on every
+    face (the fused step with its fault kernels), a moment point source and
+    fault outputs at every step."""
+    prm = {
+        'delta': [100.0, 100.0, 100.0, 0.008], 'shape': [44, 40, 30, nt],
+        'rho': [2670.0], 'vp': [6000.0], 'vs': [3464.0], 'gam': [0.2],
+        'hourglass': [1.0, 2.0], 'bc1': ['pml'] * 3, 'bc2': ['pml'] * 3, 'npml': 5,
+        'faultnormal': '+x', 'slipvector': [0.0, 1.0, 0.0], 'hypocenter': [21.5, 19.0, 14.0],
+        'vrup': 3000.0, 'rcrit': 1500.0,
+        'trelax': 0.05, 'mus': [1e4, ([[6, 34], [6, 24]], '=', 0.6)], 'mud': [0.5], 'dc': [0.2],
+        'tn': [-80e6], 'ts': [45e6, ([[16, 22], [11, 17]], '=', 50e6)],
+        'itstats': 3, 'itio': 7,
+        'mxy': [([30.3, 12.2, 20.6, []], '.', 1e14, 'brune', 0.05)],
+    }
+    for f in ('svm', 'sux', 'svy', 'tsm', 'trup', 'sam', 'tnm', 'psv', 'sl', 'tx', 'fr', 'tarr'):
+        prm[f] = [([], '=>', f + '.bin')]
+    prm['vx'] = [([[], [], 14, [None, None, 3]], '=>', 'vx.bin')]
+    prm['am2'] = [([21, [], [], -1], '=>', 'am2.bin')]
+    return prm
+
+
+def case_fault_noise(nt=16):
+    """z-normal spontaneous fault on a randomly perturbed (general) mesh."""
+    prm = case_fault_x(nt)
+    prm.update({'shape': [40, 36, 32, nt], 'faultnormal': '+z', 'slipvector': [1.0, 0.0, 0.0],
+                'hypocenter': [19.0, 17.0, 15.5],
+                'gridnoise': 0.05, 'vrup': -1.0,
+                'mus': [1e4, ([[5, 34], [5, 30]], '=', 0.6)],
+                'ts': [45e6, ([[15, 23], [13, 21]], '=', 50e6)]})
+    prm['vx'] = [([[], 17, [], [None, None, 4]], '=>', 'vx.bin')]
+    prm['am2'] = [([[], [], 16, -1], '=>', 'am2.bin')]
+    prm['mxy'] = [([10.3, 12.2, 25.6, []], '.', 1e14, 'brune', 0.05)]
+    return prm
+
+
 CASES = {
     'mpi': case_mpi,
     'pml': case_pml,
@@ -215,6 +251,8 @@ CASES = {
     'interior': case_interior,
     'interior_noise': case_interior_noise,
     'interior_wave': case_interior_wave,
+    'fault_x': case_fault_x,
+    'fault_noise': case_fault_noise,
 }
 INPUTS = {'wave': wave_inputs, 'interior_wave': interior_wave_inputs}
 
