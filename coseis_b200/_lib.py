@@ -15,7 +15,7 @@ SYMBOLS = [
     'sord_get_field', 'sord_info', 'sord_stats', 'sord_last_step_ms',
     'sord_kernel_launches', 'sord_set_profiling', 'sord_kernel_times',
     'sord_last_error', 'sord_error_string', 'sord_destroy',
-    'sord_vector_max_noalloc', 'sord_run_ensemble',
+    'sord_vector_max_noalloc', 'sord_run_ensemble', 'sord_adjoint_forward', 'sord_adjoint_backward',
 ]
 
 # return codes (enum in include/sordgpu.h)
@@ -72,6 +72,12 @@ def load():
     IP = ctypes.POINTER(ctypes.c_int)
     lib.sord_run_ensemble.argtypes = [ctypes.POINTER(ctypes.c_char_p), ctypes.c_int, ctypes.c_int, ctypes.c_int, IP]
     lib.sord_run_ensemble.restype = ctypes.c_int
+    lib.sord_adjoint_forward.argtypes = [P, ctypes.c_int]
+    lib.sord_adjoint_forward.restype = ctypes.c_int
+    FP = ctypes.POINTER(ctypes.c_float)
+    lib.sord_adjoint_backward.argtypes = [P, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(FP), IP,
+                                          FP, FP, FP, FP, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
+    lib.sord_adjoint_backward.restype = ctypes.c_int
     lib.sord_vector_max_noalloc.argtypes = [P, P, P, IP, IP, IP, P, P]
     lib.sord_vector_max_noalloc.restype = ctypes.c_int
     _lib = lib
@@ -126,6 +132,35 @@ class Solver(object):
 
     def step(self, n=1):
         _check(load().sord_step(self._h, n), self._h)
+
+    def adjoint_forward(self, segment):
+        """Whole forward run keeping a checkpoint every `segment` steps."""
+        _check(load().sord_adjoint_forward(self._h, segment), self._h)
+
+    def adjoint_backward(self, dtraces, nmoment):
+        """dtraces: {receiver file name: dL/d(samples)}.  Returns a dict of
+        numpy arrays: lam, mu, yy (real cells, shape (nx-1, ny-1, nz-1),
+        index [j, k, l]), mr (nodes, (nx, ny, nz)) and moment (nmoment)."""
+        import numpy as np
+        nn, it, nt = self.info()
+        files = list(dtraces)
+        arrs = [np.ascontiguousarray(dtraces[f], dtype=np.float32).ravel() for f in files]
+        n = len(files)
+        FP = ctypes.POINTER(ctypes.c_float)
+        fa = (ctypes.c_char_p * max(n, 1))(*[f.encode() for f in files])
+        ta = (FP * max(n, 1))(*[a.ctypes.data_as(FP) for a in arrs])
+        na = (ctypes.c_int * max(n, 1))(*[a.size for a in arrs])
+        nc = [max(x - 1, 1) for x in nn]
+        out = {k: np.zeros(nc[::-1], np.float32) for k in ('lam', 'mu', 'yy')}
+        out['mr'] = np.zeros(nn[::-1], np.float32)
+        gm = np.zeros(max(nmoment, 1), np.float64)
+        ptr = lambda a: a.ctypes.data_as(FP)
+        _check(load().sord_adjoint_backward(self._h, n, fa, ta, na, ptr(out['lam']), ptr(out['mu']), ptr(out['yy']),
+                                            ptr(out['mr']), gm.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                            nmoment), self._h)
+        res = {k: v.T for k, v in out.items()}
+        res['moment'] = gm[:nmoment]
+        return res
 
     def run(self):
         _check(load().sord_run(self._h), self._h)

@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, 'csrc')
 LIB = os.path.join(HERE, 'libsordgpu.so')
-SOURCES = ['api.cu', 'kernels.cu', 'fused.cu', 'setup.cu', 'fault.cu', 'fieldio.cu', 'util.cu', 'noalloc.cu']
+SOURCES = ['api.cu', 'kernels.cu', 'fused.cu', 'setup.cu', 'fault.cu', 'fieldio.cu', 'util.cu', 'noalloc.cu', 'adjoint.cu']
 HEADERS = ['sord.cuh', 'stencil.cuh', 'inject.cuh']
 NVCC = os.environ.get('NVCC', '/usr/local/cuda/bin/nvcc')
 FLAGS = [

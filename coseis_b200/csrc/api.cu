@@ -202,6 +202,32 @@ static InjectList upload(Solver& s, int slot, const std::vector<Inject>& e) {
     return l;
 }
 
+// One forward step n with no field-I/O hook: leapfrog update, then the
+// fused stress/force/acceleration step with the point sources of step n,
+// unfolded, so that u, v and w1n = a are the state after step n.  The
+// adjoint recomputes checkpointed segments with it; every step of such a run
+// is fusable, and the arithmetic is that of Solver::step.
+void bare_step(Solver& s, int n) {
+    s.it = n;
+    s.tm = s.prm.tm0 + s.g.dt * (float)(n - 1);
+    launch_time_update(s, false);
+    std::vector<Inject> pot, mom, frc;
+    tensor_point_ops(s, kPot, pot);
+    tensor_point_ops(s, kMom, mom);
+    InjectList lp = upload(s, 0, pot), lm = upload(s, 1, mom), lf = upload(s, 2, frc);
+    launch_fused(s, lp, lm, lf, pot, mom, frc, false, true, false);
+    s.folded = false;
+}
+
+// Injection entries of '.' moment op opi at step s.it (none if it does not fire).
+void moment_entries(Solver& s, int opi, std::vector<Inject>& out) {
+    IoOp& io = s.ops[opi];
+    int it1 = io.ii[3][0], it2 = io.ii[3][1], dit = io.ii[3][2];
+    if (io.op != "." || s.it > it2 || s.it < it1 || ((s.it - it1) % dit) != 0) return;
+    for (int c = 0; c < 6; c++)
+        if (io.field == kMom[c]) point_injection(s, io, vol(s, s.d.sd[0]), c, out);
+}
+
 static float read_max(Solver& s, int slot) {
     unsigned b;
     SORD_CUDA(cudaMemcpyAsync(&b, (unsigned*)s.d.red + slot, sizeof(unsigned), cudaMemcpyDeviceToHost, s.stream));
@@ -536,6 +562,7 @@ void Solver::destroy() {
     for (auto& io : ops) fr(io.dbuf);
     probes_free(*this);
     fused_free(*this);
+    adjoint_free(*this);
     for (auto& p : prof_ev) { cudaEventDestroy(p.second.first); cudaEventDestroy(p.second.second); }
     prof_ev.clear();
     pinned_put(hinj);
@@ -625,6 +652,45 @@ int sord_step(sord_handle* h, int nsteps) {
         if (nsteps < 0 || s.it + nsteps > s.nt) throw SordError(SORD_E_STATE, "step past nt");
         SORD_CUDA(cudaEventRecord(s.ev0, s.stream));
         for (int i = 0; i < nsteps; i++) s.step(i == nsteps - 1);
+        SORD_CUDA(cudaEventRecord(s.ev1, s.stream));
+        SORD_CUDA(cudaEventSynchronize(s.ev1));
+        float ms = 0;
+        SORD_CUDA(cudaEventElapsedTime(&ms, s.ev0, s.ev1));
+        s.last_step_ms = ms;
+    } catch (const std::exception& e) {
+        return fail(h, e);
+    }
+    return SORD_OK;
+}
+
+int sord_adjoint_forward(sord_handle* h, int segment) {
+    if (!h) return SORD_E_PARAM;
+    Solver& s = h->s;
+    try {
+        SORD_CUDA(cudaSetDevice(s.device));
+        adjoint_begin(s, segment);
+        const int seg = std::max(1, std::min(segment, std::max(s.nt, 1)));
+        while (s.it < s.nt) {
+            const int n = std::min(seg, s.nt - s.it);
+            for (int i = 0; i < n; i++) s.step(i == n - 1);
+            adjoint_checkpoint(s);
+        }
+        SORD_CUDA(cudaStreamSynchronize(s.stream));
+    } catch (const std::exception& e) {
+        return fail(h, e);
+    }
+    return SORD_OK;
+}
+
+int sord_adjoint_backward(sord_handle* h, int nrec, const char* const* files, const float* const* dtrace,
+                          const int* ntrace, float* grad_lam, float* grad_mu, float* grad_yy, float* grad_mr,
+                          double* grad_moment, int nmoment) {
+    if (!h || nrec < 0 || (nrec > 0 && (!files || !dtrace || !ntrace))) return SORD_E_PARAM;
+    Solver& s = h->s;
+    try {
+        SORD_CUDA(cudaSetDevice(s.device));
+        SORD_CUDA(cudaEventRecord(s.ev0, s.stream));
+        adjoint_backward(s, nrec, files, dtrace, ntrace, grad_lam, grad_mu, grad_yy, grad_mr, grad_moment, nmoment);
         SORD_CUDA(cudaEventRecord(s.ev1, s.stream));
         SORD_CUDA(cudaEventSynchronize(s.ev1));
         float ms = 0;

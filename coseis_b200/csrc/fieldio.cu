@@ -331,6 +331,17 @@ static int probe_id(Solver& s, size_t opi, const IoOp& io, const FieldView& f) {
     return T.id_of_op[opi];
 }
 
+// Probe of '.>' op opi (recorded when the op first fired): node or cell
+// indices and trilinear weights; returns the count, or 0 if the op never fired.
+int probe_of_op(const Solver& s, size_t opi, long long* idx, float* r) {
+    std::lock_guard<std::mutex> lock(g_probes_m);
+    auto it = g_probes.find(&s);
+    if (it == g_probes.end() || opi >= it->second.id_of_op.size() || it->second.id_of_op[opi] < 0) return 0;
+    const Probe& p = it->second.host[it->second.id_of_op[opi]];
+    for (int t = 0; t < p.n; t++) { idx[t] = p.idx[t]; r[t] = p.r[t]; }
+    return p.n;
+}
+
 void probes_free(Solver& s) {
     std::lock_guard<std::mutex> lock(g_probes_m);
     auto it = g_probes.find(&s);

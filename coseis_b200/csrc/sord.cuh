@@ -291,6 +291,7 @@ struct Solver {
     cudaEvent_t pin_ev[4] = {nullptr, nullptr, nullptr, nullptr};
     // work decomposition of the fused step kernels (fused.cu)
     FusedPlan* fplan = nullptr;
+    struct AdjointState* adj = nullptr;  // checkpoints and adjoint fields (adjoint.cu)
     bool mem_attached = false;  // holds a reference on the device's memory pool
     cudaEvent_t inj_done[kInjectSlots] = {};
     // fault bookkeeping
@@ -311,6 +312,11 @@ struct Solver {
 };
 
 void smem_limit(const void* func, int bytes);
+void adjoint_free(Solver& s);
+void adjoint_begin(Solver& s, int seg);
+void adjoint_checkpoint(Solver& s);
+void adjoint_backward(Solver& s, int nrec, const char* const* files, const float* const* dtrace, const int* ntrace,
+                      float* glam, float* gmu, float* gyy, float* gmr, double* gmom, int nmom);
 void mem_attach(int device);
 void mem_detach(int device);
 cudaError_t dev_malloc(Solver& s, void** p, size_t bytes);

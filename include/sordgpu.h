@@ -68,6 +68,32 @@ int sord_run_directory(const char* workdir, int device);
  * (cst/job.py:176-195), which the reference runs one job at a time. */
 int sord_run_ensemble(const char* const* workdirs, int n, int device, int nthreads, int* status);
 
+/* Adjoint (no reference counterpart: the reference computes no
+ * derivatives).  Gradients of a misfit of '.>' velocity or displacement
+ * receivers with respect to the per-cell moduli and node masses and to the
+ * value of every '.' moment op, for runs on a rectilinear mesh without PML
+ * or fault whose every step is a plain fused step (field-I/O outputs and '.'
+ * moment/potency ops only).
+ *
+ * sord_adjoint_forward runs the whole forward run of a fresh handle (it must
+ * be at step 0), writing its outputs as sord_run does, and keeps the state
+ * (u, v, a) every `segment` steps on the device.  Memory: about
+ * 36 B x (nt / segment + segment) per node. */
+int sord_adjoint_forward(sord_handle* h, int segment);
+
+/* Backward pass after sord_adjoint_forward: files[i] names the output file
+ * of a '.>' receiver op on vx/vy/vz/ux/uy/uz and dtrace[i] holds dL/d(sample)
+ * for its ntrace[i] samples (the file's layout).  Each segment is recomputed
+ * from its checkpoint and the transposed step kernels run backwards through
+ * it.  Outputs (any may be NULL): grad_lam, grad_mu, grad_yy per real cell
+ * ((nx-1)(ny-1)(nz-1), j fastest) = dL/d(lambda), dL/d(mu), dL/d(hourglass
+ * modulus yy); grad_mr per node (nx ny nz) = dL/d(mr), mr being the inverse
+ * nodal mass; grad_moment[m] = dL/d(value) of the m-th '.' moment op in
+ * sord.in order (nmoment must equal their count). */
+int sord_adjoint_backward(sord_handle* h, int nrec, const char* const* files, const float* const* dtrace,
+                          const int* ntrace, float* grad_lam, float* grad_mu, float* grad_yy, float* grad_mr,
+                          double* grad_moment, int nmoment);
+
 /* Copy a node or cell volume field to host memory (core region only, j
  * fastest; nn or nn-1 values per axis).  Names: vx vy vz ux uy uz ax ay az
  * (nodes; `a` holds the last acceleration) and lam mu yy vc (cells).

@@ -1,0 +1,139 @@
+"""Adjoint gradients of a receiver misfit (coseis_b200/adjoint.py,
+sord_adjoint_* in include/sordgpu.h) against central finite differences of
+the FP64 oracle forward run, along seeded random directions.
+
+The misfit is L = 1/2 sum (v_receiver - v_observed)^2 over 4 receivers x 3
+components x every step, the observed traces coming from a second seeded
+model.  FD step h = 1e-3 relative; the bound enforced is 1e-3 relative."""
+import math
+import os
+import shutil
+
+import numpy as np
+import pytest
+
+import sordcases as sc
+
+from coseis_b200 import adjoint
+
+SHAPE = (18, 16, 14)
+NT = 40
+H_FD = 1e-3
+TOL = 1e-3
+
+
+def problem(segment=7):
+    prm = {
+        'shape': list(SHAPE) + [NT], 'delta': [100.0, 100.0, 100.0, 0.008],
+        'bc1': ['free'] * 3, 'bc2': ['free'] * 3, 'npml': 0, 'hourglass': [1.0, 0.5], 'gam': [0.0],
+        'tm0': -0.15, 'itstats': 10, 'itio': 20,
+    }
+    src = {'x': [8.3, 7.6, 6.4], 'pulse': 'ricker2', 'tau': 0.05}
+    rng = np.random.default_rng(7)
+    rec = [[float(rng.uniform(2, SHAPE[0] - 3)), float(rng.uniform(2, SHAPE[1] - 3)), 0.0] for _ in range(4)]
+    return adjoint.Problem(prm, src, rec, segment=segment)
+
+
+def model(seed):
+    """Background 2700 / 6000 / 3464 with a 10 % Gaussian blob at a seeded place."""
+    rng = np.random.default_rng(seed)
+    nc = tuple(n - 1 for n in SHAPE)
+    j, k, l = np.meshgrid(*[np.arange(n) + 0.5 for n in nc], indexing='ij')
+    c = [rng.uniform(0.3, 0.7) * n for n in nc]
+    b = np.exp(-((j - c[0]) ** 2 + (k - c[1]) ** 2 + (l - c[2]) ** 2) / (2 * 3.0 ** 2))
+    amp = rng.uniform(-0.1, 0.1, 3)
+    m = rng.standard_normal(6)
+    m *= 1e15 / math.sqrt((m[:3] ** 2).sum() + 2 * (m[3:] ** 2).sum())
+    return (2700.0 * (1 + amp[0] * b), 6000.0 * (1 + amp[1] * b), 3464.0 * (1 + amp[2] * b), m)
+
+
+def oracle_traces(p, rho, vp, vs, mom, path, exe):
+    shutil.rmtree(path, ignore_errors=True)
+    p.stage(rho, vp, vs, mom, path, realsize=8)
+    sc.run_oracle(path, exe)
+    return p.read_traces(path, '<f8')
+
+
+def test_material_chain_matches_finite_differences():
+    """The chain rule of the material setup, against central differences of a
+    direct evaluation of lambda, mu, yy (cells) and mr (nodes)."""
+    rng = np.random.default_rng(3)
+    nc = (4, 3, 5)
+    rho = 2500 + 300 * rng.random(nc)
+    vp = 5500 + 800 * rng.random(nc)
+    vs = 3000 + 500 * rng.random(nc)
+    delta = [100.0, 80.0, 120.0]
+    g = {'lam': rng.standard_normal(nc), 'mu': rng.standard_normal(nc), 'yy': rng.standard_normal(nc),
+         'mr': rng.standard_normal(tuple(n + 1 for n in nc)) * 1e12}
+    s = math.sqrt(sum(d * d for d in delta) / 3) / 12
+    V = delta[0] * delta[1] * delta[2]
+
+    def F(r, a, b):
+        mu = r * b * b
+        lam = r * a * a - 2 * mu
+        yy = mu * (lam + mu) * s / (lam + 2 * mu)
+        S = np.zeros(tuple(n + 1 for n in nc))
+        for dj in (0, 1):
+            for dk in (0, 1):
+                for dl in (0, 1):
+                    S[dj:dj + nc[0], dk:dk + nc[1], dl:dl + nc[2]] += r * V
+        mr = 8.0 / S
+        return (g['lam'] * lam).sum() + (g['mu'] * mu).sum() + (g['yy'] * yy).sum() + (g['mr'] * mr).sum()
+
+    grads = adjoint.material_chain(rho, vp, vs, g, delta)
+    for x, gx in zip(range(3), grads):
+        d = rng.standard_normal(nc)
+        h = 1e-6
+        args = [rho, vp, vs]
+        ap = list(args); ap[x] = args[x] * (1 + h * d)
+        am = list(args); am[x] = args[x] * (1 - h * d)
+        fd = (F(*ap) - F(*am)) / (2 * h)
+        an = (gx * args[x] * d).sum()
+        assert abs(fd - an) <= 1e-6 * max(abs(fd), 1e-30), (x, fd, an)
+
+
+def test_problem_stages_moment_and_receivers(tmp_path):
+    p = problem()
+    rho, vp, vs, m = model(1)
+    p.stage(rho, vp, vs, m, str(tmp_path))
+    text = open(str(tmp_path / 'sord.in')).read()
+    assert sorted(adjoint.MOMENT[c] for c in p.moment_order(str(tmp_path))) == sorted(adjoint.MOMENT)
+    assert text.count('.>') == 12
+    assert os.path.getsize(str(tmp_path / 'rho.bin')) == 4 * np.prod([n - 1 for n in SHAPE])
+
+
+@pytest.mark.gpu
+def test_adjoint_gradient_vs_finite_differences(tmp_path, oracle_bins, gpu_lib):
+    import torch
+    exe = oracle_bins['f64']
+    p = problem()
+    rho0, vp0, vs0, m0 = model(11)
+    obs = oracle_traces(p, *model(12), str(tmp_path / 'obs'), exe)
+
+    rho = torch.tensor(rho0, dtype=torch.float32, requires_grad=True)
+    vp = torch.tensor(vp0, dtype=torch.float32, requires_grad=True)
+    vs = torch.tensor(vs0, dtype=torch.float32, requires_grad=True)
+    mom = torch.tensor(m0, dtype=torch.float32, requires_grad=True)
+    tr = adjoint.ReceiverTraces.apply(rho, vp, vs, mom, p)
+    # the forward traces are the oracle's within FP32 rounding
+    ref = oracle_traces(p, rho0, vp0, vs0, m0, str(tmp_path / 'fwd'), exe)
+    assert np.abs(tr.detach().numpy() - ref).max() <= 1e-4 * np.abs(ref).max()
+    loss = 0.5 * ((tr.double() - torch.as_tensor(obs)) ** 2).sum()
+    loss.backward()
+    G = [rho.grad.numpy().astype(np.float64), vp.grad.numpy().astype(np.float64),
+         vs.grad.numpy().astype(np.float64), mom.grad.numpy().astype(np.float64)]
+
+    def L(r, a, b, m, tag):
+        t = oracle_traces(p, r, a, b, m, str(tmp_path / tag), exe)
+        return 0.5 * ((t - obs) ** 2).sum()
+
+    rng = np.random.default_rng(2024)
+    base = [rho0, vp0, vs0, m0]
+    # one direction per variable (rho, vp, vs, moment), then all together
+    for k, group in enumerate([[0], [1], [2], [3], [0, 1, 2, 3]]):
+        d = [rng.standard_normal(x.shape) if i in group else np.zeros(np.shape(x)) for i, x in enumerate(base)]
+        plus = [x * (1 + H_FD * dx) for x, dx in zip(base, d)]
+        minus = [x * (1 - H_FD * dx) for x, dx in zip(base, d)]
+        fd = (L(*plus, tag='p%d' % k) - L(*minus, tag='m%d' % k)) / (2 * H_FD)
+        an = sum((g * x * dx).sum() for g, x, dx in zip(G, base, d))
+        assert abs(an - fd) <= TOL * abs(fd), (k, an, fd)
