@@ -245,6 +245,78 @@ def stage_scenarios(indices, root, seed=SEED, nt=ENS_NT, shape=None):
     return dirs
 
 
+# ------------------------------------------------------- adjoint
+def adjoint_problem(shape=(128, 128, 128), nt=1200, nrec=32, seed=SEED, segment=35):
+    """The adjoint workload: 128^3 nodes, dx 100 m, dt 0.008 s, 1200 steps;
+    rho / vp / vs 2700 / 6000 / 3464 with a 10 % seeded Gaussian blob
+    (2 km wide, seeded place and signs); seeded moment tensor (M0 1e16 N m)
+    at the centre with a Ricker wavelet of 2 Hz peak frequency ('ricker2',
+    tau = 1 / (sqrt(2) pi f0), start time -0.25 s); 32 seeded surface
+    receivers (vx, vy, vz every step); free surfaces on all faces (the
+    adjoint has no PML); checkpoints every 35 steps."""
+    from coseis_b200 import adjoint
+    nx, ny, nz = shape
+    rng = np.random.default_rng([seed, 3])
+    prm = {'shape': [nx, ny, nz, nt], 'delta': [100.0, 100.0, 100.0, 0.008], 'bc1': ['free'] * 3,
+           'bc2': ['free'] * 3, 'npml': 0, 'hourglass': [1.0, 1.0], 'gam': [0.0], 'tm0': -0.25,
+           'itstats': 10, 'itio': 100}
+    tau = 1.0 / (math.sqrt(2.0) * math.pi * 2.0)
+    src = {'x': [nx * 0.5 + 0.3, ny * 0.5 - 0.2, nz * 0.5 + 0.1], 'pulse': 'ricker2', 'tau': tau}
+    rec = [[float(rng.uniform(2, nx - 3)), float(rng.uniform(2, ny - 3)), 0.0] for _ in range(nrec)]
+    nc = (nx - 1, ny - 1, nz - 1)
+    j, k, l = np.meshgrid(*[np.arange(n, dtype=np.float32) + 0.5 for n in nc], indexing='ij', sparse=True)
+    c = [rng.uniform(0.3, 0.7) * n for n in nc]
+    blob = np.exp(-((j - c[0]) ** 2 + (k - c[1]) ** 2 + (l - c[2]) ** 2) / (2 * 10.0 ** 2)).astype(np.float32)
+    amp = rng.choice([-0.1, 0.1], 3)
+    m = rng.standard_normal(6)
+    m *= 1e16 / math.sqrt((m[:3] ** 2).sum() + 2 * (m[3:] ** 2).sum())
+    mat = [base * (1 + a * blob) for base, a in zip((2700.0, 6000.0, 3464.0), amp)]
+    return adjoint.Problem(prm, src, rec, segment=segment), mat[0], mat[1], mat[2], m
+
+
+def run_adjoint_bench(device, nt=1200):
+    """Cost of the misfit gradient against the forward run alone, all on the
+    device clock: (adjoint forward with checkpoints + backward) / plain
+    forward of the same problem; `value` with a checkpoint every 35 steps
+    (35 checkpoints, each segment recomputed), `stored` keeping every
+    state instead (no recomputation; 9.5 GB here)."""
+    from coseis_b200 import _lib
+    p, rho, vp, vs, m = adjoint_problem(nt=nt)
+    work = tempfile.mkdtemp(prefix='sord_adjb_')
+    try:
+        d = os.path.join(work, 'fwd')
+        p.stage(rho, vp, vs, m, d)
+        s = _lib.Solver(d, open(os.path.join(d, 'sord.in')).read(), device=device)
+        s.step(nt)
+        t_fwd = s.last_step_ms()
+        s.close()
+        res = {}
+        for tag, seg in (('checkpointed', 35), ('stored', 1)):
+            d = os.path.join(work, tag)
+            p.stage(rho, vp, vs, m, d)
+            s = _lib.Solver(d, open(os.path.join(d, 'sord.in')).read(), device=device)
+            try:
+                s.adjoint_forward(seg)
+                t_af = s.last_step_ms()
+                tr = p.read_traces(d)
+                # misfit against observed traces 0.9 x the computed ones
+                dtr = {f: 0.1 * tr[i // 3, i % 3] for i, f in enumerate(p.files())}
+                g = s.adjoint_backward(dtr, 6)
+                t_b = s.last_step_ms()
+            finally:
+                s.close()
+            ok = bool(np.isfinite(g['lam']).all() and np.abs(g['mu']).max() > 0)
+            res[tag] = {'ratio': (t_af + t_b) / t_fwd, 'adjoint_forward_ms': t_af, 'backward_ms': t_b,
+                        'segment': seg, 'finite_gradients': ok}
+        return {'metric': 'adjoint gradient cost / forward', 'value': res['checkpointed']['ratio'], 'unit': 'x',
+                'higher_is_better': False, 'forward_ms': t_fwd, 'checkpointed': res['checkpointed'],
+                'stored': res['stored'],
+                'workload': 'adjoint: 128^3 nodes, %d steps, seeded 10%% blob in rho/vp/vs, 32 receivers, '
+                            'moment tensor with 2 Hz Ricker, free surfaces' % nt}
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
 def pml_memberships(shape):
     """Node and cell PML slab memberships (one per node/cell per PML face)."""
     nn = np.array(shape)
@@ -448,6 +520,9 @@ def run_ours(args):
         ens = None
         if ws == 1 and args.ensemble > 0:
             ens = run_ensemble_bench(args.ensemble, args.ensemble_threads, local)
+        adj = None
+        if ws == 1 and args.adjoint_steps > 0:
+            adj = run_adjoint_bench(local, args.adjoint_steps)
     finally:
         shutil.rmtree(work, ignore_errors=True)
     if rank != 0:
@@ -484,6 +559,7 @@ def run_ours(args):
         'clocks': clocks,
         'e2e': e2e,
         'ensemble': ens,
+        'adjoint': adj,
     }
     if ws == 1 and not args.no_cpu:
         try:
@@ -588,6 +664,7 @@ def main():
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--ensemble', type=int, default=32, help='rupture-ensemble scenarios (0: skip)')
     ap.add_argument('--ensemble-threads', type=int, default=8)
+    ap.add_argument('--adjoint-steps', type=int, default=1200, help='adjoint workload steps (0: skip)')
     ap.add_argument('--hill', type=float, default=500.0, help='topography peak (m); 0 gives a rectilinear mesh')
     args = ap.parse_args()
     if args.impl == 'reference':

@@ -45,15 +45,17 @@ class Problem(object):
                pulse=time function name, tau=its parameter)
     receivers  list of [x, y, z] node positions; each records vx, vy, vz
                at every step ('.>' ops)
-    segment    steps between checkpoints (default about sqrt(nt))
+    segment    steps between checkpoints: 1 keeps every state (no
+               recomputation), 0 or None lets the library choose (1 when
+               the states fit in half of the free device memory, else about
+               sqrt(nt))
     """
 
     def __init__(self, prm, source, receivers, segment=None, device=0):
         self.prm = dict(prm)
         self.source = dict(source)
         self.receivers = [list(r) for r in receivers]
-        nt = self.prm['shape'][3]
-        self.segment = segment or max(1, int(math.ceil(math.sqrt(nt))))
+        self.segment = int(segment or 0)
         self.device = device
 
     @property

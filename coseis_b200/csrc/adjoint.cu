@@ -21,8 +21,11 @@
 // Memory: the forward stores (u, v, a) every `seg` steps; the backward pass
 // recomputes each segment from its checkpoint into a segment buffer and runs
 // the adjoint steps of the segment from it (uniform checkpointing:
-// 1 forward + 1 recomputation + the adjoint).
+// 1 forward + 1 recomputation + the adjoint).  With seg = 1 every state is
+// kept and nothing is recomputed; segment 0 picks that when all states fit
+// in half of the free device memory, else segments of about sqrt(nt).
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -49,6 +52,7 @@ struct MomEntry {
 
 struct AdjointState {
     int seg = 0;
+    int nck = 0;               // checkpoints stored
     std::vector<float*> ckpt;  // (u, v, a) at steps 0, seg, 2 seg, ...; 9 nv floats each
     float* segbuf = nullptr;   // seg states of 9 nv floats
     float* ub[3] = {};
@@ -129,6 +133,18 @@ __global__ void k_adj_cells(AdjArgs A) {
         long long cq[8];
 #pragma unroll
         for (int n = 0; n < 8; n++) cq[n] = q + (n & 1) + ((n >> 1) & 1) * g.sy + ((n >> 2) & 1) * g.sz;
+        // corner values, by corner id dj + 2 dk + 4 dl
+        float cu[3][8], cv[3][8], cf[3][8], cg[8];
+#pragma unroll
+        for (int n = 0; n < 8; n++) {
+            cg[n] = __ldg(A.gam + cq[n]);
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+                cu[i][n] = __ldg(A.u[i] + cq[n]);
+                cv[i][n] = __ldg(A.v[i] + cq[n]);
+                cf[i][n] = __ldg(A.fb[i] + cq[n]);
+            }
+        }
         // forward strain (stress.f90:251-282), w = u + g v at the corners
         float G[3][3];
 #pragma unroll
@@ -136,8 +152,8 @@ __global__ void k_adj_cells(AdjArgs A) {
             float W[8];
 #pragma unroll
             for (int t = 0; t < 8; t++) {
-                const long long c = cq[term_corner(t)];
-                W[t] = A.u[ic][c] + A.gam[c] * A.v[ic][c];
+                const int n = term_corner(t);
+                W[t] = cu[ic][n] + cg[n] * cv[ic][n];
             }
 #pragma unroll
             for (int id = 0; id < 3; id++) G[ic][id] = stencil8(W, A.br.bnc[id], h);
@@ -153,9 +169,9 @@ __global__ void k_adj_cells(AdjArgs A) {
 #pragma unroll
         for (int t = 0; t < 8; t++) {
             const int ct = t & 1, lt = (t >> 1) & 1, kt = (t >> 2) & 1;
-            const long long n = q + (1 - ct) + (1 - kt) * g.sy + (1 - lt) * g.sz;
+            const int n = (1 - ct) + 2 * (1 - kt) + 4 * (1 - lt);
 #pragma unroll
-            for (int i = 0; i < 3; i++) F[i][t] = A.fb[i][n];
+            for (int i = 0; i < 3; i++) F[i][t] = cf[i][n];
         }
         float sd[3], so[3];
 #pragma unroll
@@ -187,9 +203,9 @@ __global__ void k_adj_cells(AdjArgs A) {
                 float Hc[8], Fc[8];
 #pragma unroll
                 for (int t = 0; t < 8; t++) {
-                    const long long c = cq[hg_corner(t)];
-                    Hc[t] = A.hg1 * A.u[ic][c] + A.dh2 * A.v[ic][c];
-                    Fc[t] = A.fb[ic][c];
+                    const int n = hg_corner(t);
+                    Hc[t] = A.hg1 * cu[ic][n] + A.dh2 * cv[ic][n];
+                    Fc[t] = cf[ic][n];
                 }
 #pragma unroll
                 for (int iq = 0; iq < 4; iq++) {
@@ -213,18 +229,29 @@ __global__ void k_adj_nodes(AdjArgs A) {
         int j, k, l;
         node_jkl(g, q, j, k, l);
         float wb[3] = {0.f, 0.f, 0.f}, hb[3] = {0.f, 0.f, 0.f};
+        const float* __restrict__ cs = A.cs;
+        // cells at minus the corner offsets, by corner id dj + 2 dk + 4 dl
+        bool ok[8];
+        long long cc[8];
+#pragma unroll
+        for (int n = 0; n < 8; n++) {
+            const int dj = n & 1, dk = (n >> 1) & 1, dl = n >> 2;
+            ok[n] = in_cells(g, j - dj, k - dk, l - dl);
+            cc[n] = q - dj - dk * g.sy - dl * g.sz;
+        }
 #pragma unroll
         for (int t = 0; t < 8; t++) {
             const int n = term_corner(t);
-            const int dj = n & 1, dk = (n >> 1) & 1, dl = n >> 2;
-            if (!in_cells(g, j - dj, k - dk, l - dl)) continue;
-            const long long c = q - dj - dk * g.sy - dl * g.sz;
+            if (!ok[n]) continue;
+            float Gb[6];
+#pragma unroll
+            for (int m = 0; m < 6; m++) Gb[m] = __ldg(cs + m * nv + cc[n]);
 #pragma unroll
             for (int ic = 0; ic < 3; ic++)
 #pragma unroll
                 for (int id = 0; id < 3; id++) {
                     const int comp = ic == id ? ic : 3 + (3 - ic - id);
-                    wb[ic] = wb[ic] + h * A.br.bnc[id][t] * A.cs[comp * nv + c];
+                    wb[ic] = wb[ic] + h * A.br.bnc[id][t] * Gb[comp];
                 }
         }
         if (A.hourglass) {
@@ -236,10 +263,7 @@ __global__ void k_adj_nodes(AdjArgs A) {
 #pragma unroll
                     for (int t = 0; t < 8; t++) {
                         const int n = hg_corner(t);
-                        const int dj = n & 1, dk = (n >> 1) & 1, dl = n >> 2;
-                        S[t] = in_cells(g, j - dj, k - dk, l - dl)
-                                   ? A.cs[(6 + 3 * iq + ic) * nv + q - dj - dk * g.sy - dl * g.sz]
-                                   : 0.f;
+                        S[t] = ok[n] ? __ldg(cs + (6 + 3 * iq + ic) * nv + cc[n]) : 0.f;
                     }
                     hb[ic] = hb[ic] + hg_sum(S, iq);
                 }
@@ -346,13 +370,22 @@ static void load_state(Solver& s, const float* src) {
     }
 }
 
+int adjoint_segment(Solver& s, int seg) {
+    if (seg > 0) return std::max(1, std::min(seg, std::max(s.nt, 1)));
+    size_t fr = 0, tot = 0;
+    SORD_CUDA(cudaMemGetInfo(&fr, &tot));
+    const double all = 36.0 * (double)s.g.nv * (double)(s.nt + 1);
+    if (all < 0.5 * (double)fr) return 1;
+    return std::max(1, (int)std::ceil(std::sqrt((double)std::max(s.nt, 1))));
+}
+
 void adjoint_begin(Solver& s, int seg) {
     if (s.it != 0) throw SordError(SORD_E_STATE, "adjoint: the forward run must start at step 0");
     adjoint_check(s);
     adjoint_free(s);
     AdjointState* A = new AdjointState();
     s.adj = A;
-    A->seg = std::max(1, std::min(seg, std::max(s.nt, 1)));
+    A->seg = seg;
     for (size_t i = 0; i < s.ops.size(); i++) {
         const IoOp& io = s.ops[i];
         const std::string& f = io.field;
@@ -361,16 +394,19 @@ void adjoint_begin(Solver& s, int seg) {
         if (io.op == "." && f.size() == 3 && f[0] == 'm') A->mom_ops.push_back((int)i);
     }
     const size_t nv = (size_t)s.g.nv;
-    A->ckpt.push_back(dalloc(s, 9 * nv));
+    // seg = 1: the states after every step, the last included
+    const int nseg = A->seg == 1 ? s.nt + 1 : (s.nt + A->seg - 1) / A->seg;
+    for (int k = 0; k < std::max(nseg, 1); k++) A->ckpt.push_back(dalloc(s, 9 * nv));
+    A->nck = 1;
     save_state(s, A->ckpt[0]);
+    SORD_CUDA(cudaStreamSynchronize(s.stream));
 }
 
 // After each forward segment: the state at the end of step s.it.
 void adjoint_checkpoint(Solver& s) {
     AdjointState* A = s.adj;
-    if (!A || s.it >= s.nt) return;
-    A->ckpt.push_back(dalloc(s, 9 * (size_t)s.g.nv));
-    save_state(s, A->ckpt.back());
+    if (!A || (s.it >= s.nt && A->seg != 1) || A->nck >= (int)A->ckpt.size()) return;
+    save_state(s, A->ckpt[A->nck++]);
 }
 
 void bare_step(Solver& s, int n);
@@ -409,7 +445,7 @@ void adjoint_backward(Solver& s, int nrec, const char* const* files, const float
         for (int i = 0; i < 3; i++) { A->ub[i] = dalloc(s, nv); A->vb[i] = dalloc(s, nv); A->fb[i] = dalloc(s, nv); }
         A->cs = dalloc(s, 18 * nv);
         A->glam = dalloc(s, nv); A->gmu = dalloc(s, nv); A->gyy = dalloc(s, nv); A->gmr = dalloc(s, nv);
-        A->segbuf = dalloc(s, (size_t)A->seg * 9 * nv);
+        if (A->seg > 1) A->segbuf = dalloc(s, (size_t)A->seg * 9 * nv);
     } else {
         for (int i = 0; i < 3; i++) {
             SORD_CUDA(cudaMemsetAsync(A->ub[i], 0, sizeof(float) * nv, s.stream));
@@ -453,17 +489,19 @@ void adjoint_backward(Solver& s, int nrec, const char* const* files, const float
 
     const int seg = A->seg;
     const int nseg = (s.nt + seg - 1) / seg;
-    if ((int)A->ckpt.size() < nseg) throw SordError(SORD_E_STATE, "adjoint: missing checkpoints");
+    if (A->nck < (seg == 1 ? s.nt + 1 : nseg)) throw SordError(SORD_E_STATE, "adjoint: missing checkpoints");
     const unsigned gb = gsz((long long)nv);
     for (int k = nseg - 1; k >= 0; k--) {
         const int n0 = k * seg, n1 = std::min(s.nt, n0 + seg);
-        load_state(s, A->ckpt[k]);
-        for (int n = n0 + 1; n <= n1; n++) {
-            bare_step(s, n);
-            save_state(s, A->segbuf + (size_t)(n - n0 - 1) * 9 * nv);
+        if (seg > 1) {
+            load_state(s, A->ckpt[k]);
+            for (int n = n0 + 1; n <= n1; n++) {
+                bare_step(s, n);
+                save_state(s, A->segbuf + (size_t)(n - n0 - 1) * 9 * nv);
+            }
         }
         for (int n = n1; n >= n0 + 1; n--) {
-            const float* st = A->segbuf + (size_t)(n - n0 - 1) * 9 * nv;
+            const float* st = seg > 1 ? A->segbuf + (size_t)(n - n0 - 1) * 9 * nv : A->ckpt[n];
             for (int i = 0; i < 3; i++) { K.u[i] = st + i * nv; K.v[i] = st + (3 + i) * nv; K.a[i] = st + (6 + i) * nv; }
             k_adj_mass<<<gb, 256, 0, s.stream>>>(K, g.dt);
             k_adj_cells<<<gb, 256, 0, s.stream>>>(K);

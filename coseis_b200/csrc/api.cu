@@ -668,14 +668,19 @@ int sord_adjoint_forward(sord_handle* h, int segment) {
     Solver& s = h->s;
     try {
         SORD_CUDA(cudaSetDevice(s.device));
-        adjoint_begin(s, segment);
-        const int seg = std::max(1, std::min(segment, std::max(s.nt, 1)));
+        const int seg = adjoint_segment(s, segment);
+        adjoint_begin(s, seg);
+        SORD_CUDA(cudaEventRecord(s.ev0, s.stream));
         while (s.it < s.nt) {
             const int n = std::min(seg, s.nt - s.it);
             for (int i = 0; i < n; i++) s.step(i == n - 1);
             adjoint_checkpoint(s);
         }
-        SORD_CUDA(cudaStreamSynchronize(s.stream));
+        SORD_CUDA(cudaEventRecord(s.ev1, s.stream));
+        SORD_CUDA(cudaEventSynchronize(s.ev1));
+        float ms = 0;
+        SORD_CUDA(cudaEventElapsedTime(&ms, s.ev0, s.ev1));
+        s.last_step_ms = ms;
     } catch (const std::exception& e) {
         return fail(h, e);
     }

@@ -313,6 +313,7 @@ struct Solver {
 
 void smem_limit(const void* func, int bytes);
 void adjoint_free(Solver& s);
+int adjoint_segment(Solver& s, int seg);
 void adjoint_begin(Solver& s, int seg);
 void adjoint_checkpoint(Solver& s);
 void adjoint_backward(Solver& s, int nrec, const char* const* files, const float* const* dtrace, const int* ntrace,

@@ -78,7 +78,10 @@ int sord_run_ensemble(const char* const* workdirs, int n, int device, int nthrea
  * sord_adjoint_forward runs the whole forward run of a fresh handle (it must
  * be at step 0), writing its outputs as sord_run does, and keeps the state
  * (u, v, a) every `segment` steps on the device.  Memory: about
- * 36 B x (nt / segment + segment) per node. */
+ * 36 B x (nt / segment + segment) per node.  segment 1 keeps every state
+ * and the backward pass recomputes nothing; segment 0 chooses 1 when all
+ * states fit in half of the free device memory, else about sqrt(nt).  sord_last_step_ms gives the
+ * device time of the call (and of sord_adjoint_backward after that one). */
 int sord_adjoint_forward(sord_handle* h, int segment);
 
 /* Backward pass after sord_adjoint_forward: files[i] names the output file

@@ -103,10 +103,11 @@ def test_problem_stages_moment_and_receivers(tmp_path):
 
 
 @pytest.mark.gpu
-def test_adjoint_gradient_vs_finite_differences(tmp_path, oracle_bins, gpu_lib):
+@pytest.mark.parametrize('segment', [7, 1], ids=['recompute', 'stored'])
+def test_adjoint_gradient_vs_finite_differences(segment, tmp_path, oracle_bins, gpu_lib):
     import torch
     exe = oracle_bins['f64']
-    p = problem()
+    p = problem(segment)
     rho0, vp0, vs0, m0 = model(11)
     obs = oracle_traces(p, *model(12), str(tmp_path / 'obs'), exe)
 
