@@ -1479,26 +1479,25 @@ static FusedPlan& fused_plan(Solver& s) {
     FusedPlan* P = new FusedPlan();
     s.fplan = P;
     const Geom& g = s.g;
-    // node c along axis d is interior when both adjacent cells are
+    // Node c along axis d is interior when it is outside the PML and each
+    // adjacent cell is either a real cell outside the PML or a cell outside
+    // the mesh (a boundary without PML, whose coefficients are zero: the
+    // kernel then adds exactly zero for it, as the reference does).
     auto cin = [&](int d, int c) { return c > g.i1pml[d] && c < g.i2pml[d] - 1 && c >= g.i1cell[d] && c <= g.i2cell[d]; };
+    auto cellok = [&](int d, int c) { return c < g.i1cell[d] || c > g.i2cell[d] || cin(d, c); };
+    auto nodeok = [&](int d, int c) { return c >= g.i1pml[d] + 1 && c <= g.i2pml[d] - 1 && cellok(d, c - 1) && cellok(d, c); };
     auto range = [&](int d, int& a, int& b) {
         a = 0;
         b = -1;
         for (int c = g.i1node[d]; c <= g.i2node[d]; c++)
-            if (cin(d, c - 1) && cin(d, c)) {
+            if (nodeok(d, c)) {
                 if (b < a) a = c;
                 if (b == c - 1 || b < a) b = c;
             }
     };
     range(0, P->jf, P->jend);
     range(1, P->kf, P->kend);
-    // planes: cells l-1 and l interior, or outside the mesh's cells (free surface)
-    auto cellok = [&](int c) { return c < g.i1cell[2] || c > g.i2cell[2] || cin(2, c); };
-    for (int l = g.i1node[2]; l <= g.i2node[2]; l++) {
-        const bool f = l >= g.i1pml[2] + 1 && l <= g.i2pml[2] - 1 && cellok(l - 1) && cellok(l);
-        if (f && P->lf1 < P->lf0) P->lf0 = P->lf1 = l;
-        else if (f && P->lf1 == l - 1) P->lf1 = l;
-    }
+    range(2, P->lf0, P->lf1);
     const bool inner = P->jend >= P->jf && P->kend >= P->kf && P->lf1 >= P->lf0;
     const int L1 = g.i1node[2], L2 = g.i2node[2];
     int sms = 148;

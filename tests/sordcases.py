@@ -237,6 +237,25 @@ def case_fault_noise(nt=16):
     return prm
 
 
+def case_free(nt=24):
+    """Free surfaces on all six faces, no PML: interior tiles reach every
+    boundary (cells outside the mesh add zero); moment and force-free point
+    source, snapshots and receivers."""
+    prm = {
+        'delta': [100.0, 100.0, 100.0, 0.008], 'shape': [44, 38, 30, nt],
+        'rho': [2670.0], 'vp': [6000.0], 'vs': [3464.0], 'gam': [0.1], 'hourglass': [1.0, 0.7],
+        'bc1': ['free'] * 3, 'bc2': ['free'] * 3, 'npml': 0, 'tm0': -0.1,
+        'mxx': [([4.3, 5.6, 3.2, []], '.', 1e12, 'ricker2', 0.05)],
+        'myz': [([4.3, 5.6, 3.2, []], '.', -4e11, 'ricker2', 0.05)],
+        'itstats': 3, 'itio': 8,
+    }
+    prm['vx'] = [([[], [], 0, [None, None, 3]], '=>', 'vx-top.bin'), ([[], 0, [], -1], '=>', 'vx-side.bin')]
+    prm['vz'] = [([[], [], -1, -1], '=>', 'vz-bottom.bin'), ([0.0, 5.5, 3.25, []], '.>', 'vz-corner.bin')]
+    prm['uy'] = [([-1, [], [], -1], '=>', 'uy-far.bin')]
+    prm['am2'] = [([[], [], [], -1], '=>', 'am2.bin')]
+    return prm
+
+
 CASES = {
     'mpi': case_mpi,
     'pml': case_pml,
@@ -253,6 +272,7 @@ CASES = {
     'interior_wave': case_interior_wave,
     'fault_x': case_fault_x,
     'fault_noise': case_fault_noise,
+    'free': case_free,
 }
 INPUTS = {'wave': wave_inputs, 'interior_wave': interior_wave_inputs}
 
