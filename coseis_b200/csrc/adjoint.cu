@@ -55,10 +55,8 @@ struct AdjointState {
     int nck = 0;               // checkpoints stored
     std::vector<float*> ckpt;  // (u, v, a) at steps 0, seg, 2 seg, ...; 9 nv floats each
     float* segbuf = nullptr;   // seg states of 9 nv floats
-    float* ub[3] = {};
-    float* vb[3] = {};
-    float* fb[3] = {};
-    float* cs = nullptr;       // 18 nv cell values
+    float* ub[2][3] = {};      // adjoint state, double-buffered
+    float* vb[2][3] = {};
     float *glam = nullptr, *gmu = nullptr, *gyy = nullptr, *gmr = nullptr;
     RecvEntry* recv = nullptr;
     int nrecv = 0;
@@ -75,19 +73,15 @@ struct AdjArgs {
     Geom g;
     Brackets br;
     const float *u[3], *v[3], *a[3];  // forward state of step n
-    float *ub[3], *vb[3], *fb[3];
-    float* cs;
+    const float *ubi[3], *vbi[3];     // adjoint state of step n + 1
+    float *ubo[3], *vbo[3];           // adjoint state of step n
     const float *lam, *mu, *yy, *vc, *mr, *gam;
     float *glam, *gmu, *gyy, *gmr;
-    float hg1, dh2;
+    float hg1, dh2, dt;
     int hourglass;
+    int nbx, segl;                    // tiles along j, node planes per block
 };
 
-__device__ __forceinline__ void node_jkl(const Geom& g, long long q, int& j, int& k, int& l) {
-    j = (int)(q % g.sy) + 1;
-    k = (int)((q / g.sy) % g.nm[1]) + 1;
-    l = (int)(q / g.sz) + 1;
-}
 __device__ __forceinline__ bool in_nodes(const Geom& g, int j, int k, int l) {
     return j >= g.i1node[0] && j <= g.i2node[0] && k >= g.i1node[1] && k <= g.i2node[1] && l >= g.i1node[2] &&
            l <= g.i2node[2];
@@ -96,65 +90,99 @@ __device__ __forceinline__ bool in_cells(const Geom& g, int j, int k, int l) {
     return j >= g.i1cell[0] && j <= g.i2cell[0] && k >= g.i1cell[1] && k <= g.i2cell[1] && l >= g.i1cell[2] &&
            l <= g.i2cell[2];
 }
-
-// abar = dt (vbar + dt ubar); vbar <- vbar + dt ubar; fbar = mr abar on the
-// force nodes; dL/dmr += f . abar with f = a / mr.
-__global__ void k_adj_mass(AdjArgs A, float dt) {
-    const Geom& g = A.g;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < g.nv; q += (long long)gridDim.x * blockDim.x) {
-        int j, k, l;
-        node_jkl(g, q, j, k, l);
-        const bool act = in_nodes(g, j, k, l);
-        const float m = A.mr[q];
-        float gm = 0.f;
-#pragma unroll
-        for (int i = 0; i < 3; i++) {
-            const float vt = A.vb[i][q] + dt * A.ub[i][q];
-            A.vb[i][q] = vt;
-            const float ab = dt * vt;
-            A.fb[i][q] = act ? m * ab : 0.f;
-            if (act && m != 0.f) gm = gm + (A.a[i][q] / m) * ab;
-        }
-        if (act) A.gmr[q] = A.gmr[q] + gm;
-    }
+// fbar = mr dt (vbar + dt ubar) of node q, zero off the force nodes
+__device__ __forceinline__ float fbar(const AdjArgs& A, long long q, bool act, int i) {
+    return act ? A.mr[q] * (A.dt * (A.vbi[i][q] + A.dt * A.ubi[i][q])) : 0.f;
 }
 
-// Cell pass: forward strain of step n, sigmabar = vc Dcn^T fbar, the
-// transposed Hooke law, hourglass cell adjoints; per-cell gradients.
-// cs[0..2] = Gbar_ii, cs[3..5] = Gbar of the off-diagonal pairs (yz zx xy),
-// cs[6 + 3 q + i] = yy * sbar_q,i.
-__global__ void k_adj_cells(AdjArgs A) {
+// One adjoint step over a tile column, streaming along l like the forward
+// step kernel: a block of 32 x 8 threads owns node columns j0..j0+30 x
+// k0..k0+6 (outputs) and computes the cells j0-1..j0+30 x k0-1..k0+6 they
+// touch.  The raw node values of a plane (forward u, v, a, g, mr and the
+// adjoint ubar, vbar of step n + 1) are copied into a three-slot shared ring
+// with cp.async two planes ahead; cell planes (Gbar of the transposed
+// strain, yy sbar of the hourglass) sit in a two-slot ring.  Cell gradients
+// are written by the block that owns the cell (tx, ty >= 1), node gradients
+// and the adjoint state by the owner of the node; the adjoint state is
+// double-buffered (in: step n + 1, out: step n) because neighbouring blocks
+// read the in-state of their halo nodes.
+constexpr int AJ = 32, AK = 8, ANJ = AJ + 1, ANK = AK + 1, ANP = ANJ * ANK, ANC = AJ * AK;
+constexpr int ARF = 17, ACF = 18;  // raw floats per node, cell floats
+// raw node fields
+enum { RU = 0, RV = 3, RUB = 6, RVB = 9, RA = 12, RG = 15, RM = 16 };
+constexpr size_t kAdjSmem = sizeof(float) * (3 * ARF * ANP + 2 * ACF * ANC);
+
+__global__ void __launch_bounds__(AJ * AK, 2) k_adj_step(AdjArgs A) {
+    extern __shared__ float sm[];
+    float* sR = sm;                     // [slot][field][node]
+    float* sC = sm + 3 * ARF * ANP;     // [slot][field][cell]
     const Geom& g = A.g;
-    const float h = g.h;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < g.nv; q += (long long)gridDim.x * blockDim.x) {
-        int j, k, l;
-        node_jkl(g, q, j, k, l);
-        if (!in_cells(g, j, k, l)) continue;
-        long long cq[8];
+    const float h = g.h, dt = A.dt;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + AJ * ty;
+    const int bx = blockIdx.x % A.nbx, by = blockIdx.x / A.nbx;
+    const int j0 = g.i1node[0] + bx * (AJ - 1), k0 = g.i1node[1] + by * (AK - 1);
+    const int L0 = g.i1node[2] + blockIdx.y * A.segl, L1 = min(L0 + A.segl - 1, g.i2node[2]);
+    const int J = j0 - 1 + tx, K = k0 - 1 + ty;  // this thread's cell column
+
+    auto issue = [&](int p) {
+        float* d = sR + (p % 3) * (ARF * ANP);
+        for (int n = tid; n < ANP; n += AJ * AK) {
+            const int j = j0 - 1 + n % ANJ, k = k0 - 1 + n / ANJ;
+            if (j <= g.nm[0] && k <= g.nm[1] && p >= 1 && p <= g.nm[2]) {
+                const long long q = g.idx(j, k, p);
 #pragma unroll
-        for (int n = 0; n < 8; n++) cq[n] = q + (n & 1) + ((n >> 1) & 1) * g.sy + ((n >> 2) & 1) * g.sz;
-        // corner values, by corner id dj + 2 dk + 4 dl
-        float cu[3][8], cv[3][8], cf[3][8], cg[8];
+                for (int i = 0; i < 3; i++) {
+                    cp_async4(d + (RU + i) * ANP + n, A.u[i] + q);
+                    cp_async4(d + (RV + i) * ANP + n, A.v[i] + q);
+                    cp_async4(d + (RUB + i) * ANP + n, A.ubi[i] + q);
+                    cp_async4(d + (RVB + i) * ANP + n, A.vbi[i] + q);
+                    cp_async4(d + (RA + i) * ANP + n, A.a[i] + q);
+                }
+                cp_async4(d + RG * ANP + n, A.gam + q);
+                cp_async4(d + RM * ANP + n, A.mr + q);
+            } else {
 #pragma unroll
-        for (int n = 0; n < 8; n++) {
-            cg[n] = __ldg(A.gam + cq[n]);
-#pragma unroll
-            for (int i = 0; i < 3; i++) {
-                cu[i][n] = __ldg(A.u[i] + cq[n]);
-                cv[i][n] = __ldg(A.v[i] + cq[n]);
-                cf[i][n] = __ldg(A.fb[i] + cq[n]);
+                for (int f = 0; f < ARF; f++) d[f * ANP + n] = 0.f;
             }
         }
-        // forward strain (stress.f90:251-282), w = u + g v at the corners
+        cp_async_commit();
+    };
+
+    auto cells = [&](int l, bool own) {
+        float* o = sC + (l & 1) * (ACF * ANC) + tid;
+        if (!in_cells(g, J, K, l)) {
+#pragma unroll
+            for (int f = 0; f < ACF; f++) o[f * ANC] = 0.f;
+            return;
+        }
+        const long long q = g.idx(J, K, l);
+        const float r = A.vc[q], lm = A.lam[q], m2 = 2.0f * A.mu[q], yc = A.yy[q];
+        const float* r0 = sR + (l % 3) * (ARF * ANP);
+        const float* r1 = sR + ((l + 1) % 3) * (ARF * ANP);
+        // corner values by corner id dj + 2 dk + 4 dl: w = u + g v,
+        // hg1 u + dt hg2 v, fbar = mr dt (vbar + dt ubar) on force nodes
+        float cw[3][8], ch[3][8], cf[3][8];
+#pragma unroll
+        for (int n = 0; n < 8; n++) {
+            const int dj = n & 1, dk = (n >> 1) & 1, dl = n >> 2;
+            const float* b = (dl ? r1 : r0) + (tx + dj) + ANJ * (ty + dk);
+            const bool act = in_nodes(g, J + dj, K + dk, l + dl);
+            const float gm = b[RG * ANP], mm = b[RM * ANP];
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+                const float uu = b[(RU + i) * ANP], vv = b[(RV + i) * ANP];
+                cw[i][n] = uu + gm * vv;
+                ch[i][n] = A.hg1 * uu + A.dh2 * vv;
+                cf[i][n] = act ? mm * (dt * (b[(RVB + i) * ANP] + dt * b[(RUB + i) * ANP])) : 0.f;
+            }
+        }
+        // forward strain (stress.f90:251-282)
         float G[3][3];
 #pragma unroll
         for (int ic = 0; ic < 3; ic++) {
             float W[8];
 #pragma unroll
-            for (int t = 0; t < 8; t++) {
-                const int n = term_corner(t);
-                W[t] = cu[ic][n] + cg[n] * cv[ic][n];
-            }
+            for (int t = 0; t < 8; t++) W[t] = cw[ic][term_corner(t)];
 #pragma unroll
             for (int id = 0; id < 3; id++) G[ic][id] = stencil8(W, A.br.bnc[id], h);
         }
@@ -164,7 +192,7 @@ __global__ void k_adj_cells(AdjArgs A) {
         eo[0] = 0.5f * G[1][2] + 0.5f * G[2][1];
         eo[1] = 0.5f * G[0][2] + 0.5f * G[2][0];
         eo[2] = 0.5f * G[0][1] + 0.5f * G[1][0];
-        // sigmabar = Dcn^T fbar: node of diff_cn term t is c + (1-ct, 1-kt, 1-lt)
+        // sigmabar = vc Dcn^T fbar: the node of diff_cn term t is at cell corner (1-ct, 1-kt, 1-lt)
         float F[3][8];
 #pragma unroll
         for (int t = 0; t < 8; t++) {
@@ -175,77 +203,61 @@ __global__ void k_adj_cells(AdjArgs A) {
         }
         float sd[3], so[3];
 #pragma unroll
-        for (int i = 0; i < 3; i++) sd[i] = stencil8(F[i], A.br.bcn[i], h);
-        so[0] = stencil8(F[1], A.br.bcn[2], h) + stencil8(F[2], A.br.bcn[1], h);
-        so[1] = stencil8(F[0], A.br.bcn[2], h) + stencil8(F[2], A.br.bcn[0], h);
-        so[2] = stencil8(F[0], A.br.bcn[1], h) + stencil8(F[1], A.br.bcn[0], h);
-        const float r = A.vc[q];
-#pragma unroll
-        for (int i = 0; i < 3; i++) { sd[i] = sd[i] * r; so[i] = so[i] * r; }
-        // Hooke's law transposed; dL/dlam, dL/dmu
-        const float lm = A.lam[q], m2 = 2.0f * A.mu[q];
+        for (int i = 0; i < 3; i++) sd[i] = stencil8(F[i], A.br.bcn[i], h) * r;
+        so[0] = (stencil8(F[1], A.br.bcn[2], h) + stencil8(F[2], A.br.bcn[1], h)) * r;
+        so[1] = (stencil8(F[0], A.br.bcn[2], h) + stencil8(F[2], A.br.bcn[0], h)) * r;
+        so[2] = (stencil8(F[0], A.br.bcn[1], h) + stencil8(F[1], A.br.bcn[0], h)) * r;
+        // Hooke's law transposed
         const float tr = ed[0] + ed[1] + ed[2], st = sd[0] + sd[1] + sd[2];
-        A.glam[q] = A.glam[q] + st * tr;
-        A.gmu[q] = A.gmu[q] + 2.0f * (sd[0] * ed[0] + sd[1] * ed[1] + sd[2] * ed[2]) +
-                   2.0f * (so[0] * eo[0] + so[1] * eo[1] + so[2] * eo[2]);
-        float* cs = A.cs;
-        const long long nv = g.nv;
 #pragma unroll
         for (int i = 0; i < 3; i++) {
-            cs[i * nv + q] = m2 * sd[i] + lm * st;  // Gbar_ii
-            cs[(3 + i) * nv + q] = 0.5f * (m2 * so[i]);  // Gbar_ij = Gbar_ji
+            o[i * ANC] = m2 * sd[i] + lm * st;         // Gbar_ii
+            o[(3 + i) * ANC] = 0.5f * (m2 * so[i]);    // Gbar_jk = Gbar_kj
         }
+        float gy = 0.f;
         if (A.hourglass) {
-            const float yc = A.yy[q];
-            float gy = 0.f;
 #pragma unroll
             for (int ic = 0; ic < 3; ic++) {
                 float Hc[8], Fc[8];
 #pragma unroll
                 for (int t = 0; t < 8; t++) {
                     const int n = hg_corner(t);
-                    Hc[t] = A.hg1 * cu[ic][n] + A.dh2 * cv[ic][n];
+                    Hc[t] = ch[ic][n];
                     Fc[t] = cf[ic][n];
                 }
 #pragma unroll
                 for (int iq = 0; iq < 4; iq++) {
                     const float sb = -hg_sum(Fc, iq);
                     gy = gy + sb * hg_sum(Hc, iq);
-                    cs[(6 + 3 * iq + ic) * nv + q] = yc * sb;
+                    o[(6 + 3 * iq + ic) * ANC] = yc * sb;
                 }
             }
-            A.gyy[q] = A.gyy[q] + gy;
-        }
-    }
-}
-
-// Node pass: wbar = Dnc^T Gbar, hbar = sum_q Hcn_q(yy sbar_q);
-// ubar += wbar + hg1 hbar, vbar += g wbar + dt hg2 hbar.
-__global__ void k_adj_nodes(AdjArgs A) {
-    const Geom& g = A.g;
-    const float h = g.h;
-    const long long nv = g.nv;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nv; q += (long long)gridDim.x * blockDim.x) {
-        int j, k, l;
-        node_jkl(g, q, j, k, l);
-        float wb[3] = {0.f, 0.f, 0.f}, hb[3] = {0.f, 0.f, 0.f};
-        const float* __restrict__ cs = A.cs;
-        // cells at minus the corner offsets, by corner id dj + 2 dk + 4 dl
-        bool ok[8];
-        long long cc[8];
+        } else {
 #pragma unroll
-        for (int n = 0; n < 8; n++) {
-            const int dj = n & 1, dk = (n >> 1) & 1, dl = n >> 2;
-            ok[n] = in_cells(g, j - dj, k - dk, l - dl);
-            cc[n] = q - dj - dk * g.sy - dl * g.sz;
+            for (int f = 6; f < ACF; f++) o[f * ANC] = 0.f;
         }
+        if (own && tx >= 1 && ty >= 1) {
+            A.glam[q] = A.glam[q] + st * tr;
+            A.gmu[q] = A.gmu[q] + 2.0f * (sd[0] * ed[0] + sd[1] * ed[1] + sd[2] * ed[2]) +
+                       2.0f * (so[0] * eo[0] + so[1] * eo[1] + so[2] * eo[2]);
+            if (A.hourglass) A.gyy[q] = A.gyy[q] + gy;
+        }
+    };
+
+    auto nodes = [&](int l) {
+        const int jn = j0 + tx, kn = k0 + ty;
+        if (tx >= AJ - 1 || ty >= AK - 1 || jn > g.i2node[0] || kn > g.i2node[1]) return;
+        const float* c0 = sC + ((l - 1) & 1) * (ACF * ANC);  // cell plane l - 1
+        const float* c1 = sC + (l & 1) * (ACF * ANC);        // cell plane l
+        // cells at minus the corner offsets: smem cell (tx + 1 - dj, ty + 1 - dk)
+        float wb[3] = {0.f, 0.f, 0.f}, hb[3] = {0.f, 0.f, 0.f};
 #pragma unroll
         for (int t = 0; t < 8; t++) {
             const int n = term_corner(t);
-            if (!ok[n]) continue;
+            const float* b = ((n >> 2) ? c0 : c1) + (tx + 1 - (n & 1)) + AJ * (ty + 1 - ((n >> 1) & 1));
             float Gb[6];
 #pragma unroll
-            for (int m = 0; m < 6; m++) Gb[m] = __ldg(cs + m * nv + cc[n]);
+            for (int m = 0; m < 6; m++) Gb[m] = b[m * ANC];
 #pragma unroll
             for (int ic = 0; ic < 3; ic++)
 #pragma unroll
@@ -263,24 +275,49 @@ __global__ void k_adj_nodes(AdjArgs A) {
 #pragma unroll
                     for (int t = 0; t < 8; t++) {
                         const int n = hg_corner(t);
-                        S[t] = ok[n] ? __ldg(cs + (6 + 3 * iq + ic) * nv + cc[n]) : 0.f;
+                        S[t] = (((n >> 2) ? c0 : c1) + (tx + 1 - (n & 1)) + AJ * (ty + 1 - ((n >> 1) & 1)))[(6 + 3 * iq + ic) * ANC];
                     }
                     hb[ic] = hb[ic] + hg_sum(S, iq);
                 }
         }
-        const float gm = A.gam[q];
+        const float* b = sR + (l % 3) * (ARF * ANP) + (tx + 1) + ANJ * (ty + 1);
+        const long long q = g.idx(jn, kn, l);
+        const float m = b[RM * ANP], gm = b[RG * ANP];
+        float gmr = 0.f;
 #pragma unroll
         for (int i = 0; i < 3; i++) {
-            A.ub[i][q] = A.ub[i][q] + wb[i] + A.hg1 * hb[i];
-            A.vb[i][q] = A.vb[i][q] + gm * wb[i] + A.dh2 * hb[i];
+            const float ub = b[(RUB + i) * ANP];
+            const float vt = b[(RVB + i) * ANP] + dt * ub;
+            const float ab = dt * vt;
+            if (m != 0.f) gmr = gmr + (b[(RA + i) * ANP] / m) * ab;
+            A.ubo[i][q] = ub + wb[i] + A.hg1 * hb[i];
+            A.vbo[i][q] = vt + gm * wb[i] + A.dh2 * hb[i];
         }
+        A.gmr[q] = A.gmr[q] + gmr;
+    };
+
+    issue(L0 - 1);
+    issue(L0);
+    cp_async_wait_all();
+    __syncthreads();
+    issue(L0 + 1);
+    cells(L0 - 1, false);
+#pragma unroll 1
+    for (int l = L0; l <= L1; l++) {
+        cp_async_wait_all();
+        __syncthreads();  // raw plane l+1 landed; cell plane l-1 and nodes(l-1) complete
+        if (l + 1 <= L1) issue(l + 2);
+        cells(l, true);
+        __syncthreads();  // cell plane l complete
+        nodes(l);
     }
+    cp_async_wait_all();
 }
 
 // dL/d(moment op value) at the source cells of step n: vc * (Dcn^T fbar)
 // of the injected component times d(injection)/d(value).
-__global__ void k_adj_moment(Geom g, Brackets br, const MomEntry* e, int n, float* const* fb, const float* vc,
-                             double* gmom) {
+__global__ void k_adj_moment(AdjArgs A, const MomEntry* e, int n, double* gmom) {
+    const Geom& g = A.g;
     const float h = g.h;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const MomEntry E = e[i];
@@ -288,43 +325,44 @@ __global__ void k_adj_moment(Geom g, Brackets br, const MomEntry* e, int n, floa
         for (int t = 0; t < 8; t++) {
             const int ct = t & 1, lt = (t >> 1) & 1, kt = (t >> 2) & 1;
             const long long nd = E.idx + (1 - ct) + (1 - kt) * g.sy + (1 - lt) * g.sz;
-            for (int c = 0; c < 3; c++) F[c][t] = fb[c][nd];
+            const int j = (int)(nd % g.sy) + 1, k = (int)((nd / g.sy) % g.nm[1]) + 1, l = (int)(nd / g.sz) + 1;
+            const bool act = in_nodes(g, j, k, l);
+            for (int c = 0; c < 3; c++) F[c][t] = fbar(A, nd, act, c);
         }
         float s;
-        if (E.comp < 3) s = stencil8(F[E.comp], br.bcn[E.comp], h);
+        if (E.comp < 3) s = stencil8(F[E.comp], A.br.bcn[E.comp], h);
         else {
-            const int a = E.comp == 3 ? 1 : E.comp == 4 ? 0 : 0, b = E.comp == 3 ? 2 : E.comp == 4 ? 2 : 1;
-            s = stencil8(F[a], br.bcn[b], h) + stencil8(F[b], br.bcn[a], h);
+            const int a = E.comp == 5 ? 0 : E.comp == 4 ? 0 : 1, b = E.comp == 5 ? 1 : 2;
+            s = stencil8(F[a], A.br.bcn[b], h) + stencil8(F[b], A.br.bcn[a], h);
         }
-        atomicAdd(gmom + E.slot, (double)(s * vc[E.idx] * E.w));
+        atomicAdd(gmom + E.slot, (double)(s * A.vc[E.idx] * E.w));
     }
 }
 
 // Receiver misfit sources of step n: ubar/vbar += weight * dL/d(sample).
-__global__ void k_adj_recv(const RecvEntry* e, int n, int it, const float* trace, float* const* ub, float* const* vb) {
+struct Ptr3 {
+    float* p[3];
+};
+__global__ void k_adj_recv(const RecvEntry* e, int n, int it, const float* trace, Ptr3 ub, Ptr3 vb) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const RecvEntry E = e[i];
         if (it < E.it1 || (it - E.it1) % E.dit != 0) continue;
         const int sidx = (it - E.it1) / E.dit;
         if (sidx >= E.ns) continue;
-        float* dst = E.disp ? ub[E.comp] : vb[E.comp];
+        float* dst = E.disp ? ub.p[E.comp] : vb.p[E.comp];
         atomicAdd(dst + E.idx, E.r * trace[E.off + sidx]);
     }
 }
 
 // ------------------------------------------------------------ host
-static unsigned gsz(long long n) {
-    long long b = (n + 255) / 256;
-    return (unsigned)std::max(1LL, std::min(b, 148LL * 16));
-}
 
 void adjoint_free(Solver& s) {
     AdjointState* A = s.adj;
     if (!A) return;
     for (float* p : A->ckpt) dev_free(s, p);
     dev_free(s, A->segbuf);
-    for (int i = 0; i < 3; i++) { dev_free(s, A->ub[i]); dev_free(s, A->vb[i]); dev_free(s, A->fb[i]); }
-    dev_free(s, A->cs);
+    for (int b = 0; b < 2; b++)
+        for (int i = 0; i < 3; i++) { dev_free(s, A->ub[b][i]); dev_free(s, A->vb[b][i]); }
     dev_free(s, A->glam); dev_free(s, A->gmu); dev_free(s, A->gyy); dev_free(s, A->gmr);
     dev_free(s, A->recv); dev_free(s, A->trace); dev_free(s, A->mom); dev_free(s, A->gmom);
     delete A;
@@ -441,16 +479,17 @@ void adjoint_backward(Solver& s, int nrec, const char* const* files, const float
         for (int t = 0; t < np; t++)
             rec.push_back(RecvEntry{idx[t], comp, disp, r[t], off, io.ii[3][0], io.ii[3][2], ntrace[i]});
     }
-    if (!A->ub[0]) {
-        for (int i = 0; i < 3; i++) { A->ub[i] = dalloc(s, nv); A->vb[i] = dalloc(s, nv); A->fb[i] = dalloc(s, nv); }
-        A->cs = dalloc(s, 18 * nv);
+    if (!A->ub[0][0]) {
+        for (int b = 0; b < 2; b++)
+            for (int i = 0; i < 3; i++) { A->ub[b][i] = dalloc(s, nv); A->vb[b][i] = dalloc(s, nv); }
         A->glam = dalloc(s, nv); A->gmu = dalloc(s, nv); A->gyy = dalloc(s, nv); A->gmr = dalloc(s, nv);
         if (A->seg > 1) A->segbuf = dalloc(s, (size_t)A->seg * 9 * nv);
     } else {
-        for (int i = 0; i < 3; i++) {
-            SORD_CUDA(cudaMemsetAsync(A->ub[i], 0, sizeof(float) * nv, s.stream));
-            SORD_CUDA(cudaMemsetAsync(A->vb[i], 0, sizeof(float) * nv, s.stream));
-        }
+        for (int b = 0; b < 2; b++)
+            for (int i = 0; i < 3; i++) {
+                SORD_CUDA(cudaMemsetAsync(A->ub[b][i], 0, sizeof(float) * nv, s.stream));
+                SORD_CUDA(cudaMemsetAsync(A->vb[b][i], 0, sizeof(float) * nv, s.stream));
+            }
         for (float* p : {A->glam, A->gmu, A->gyy, A->gmr}) SORD_CUDA(cudaMemsetAsync(p, 0, sizeof(float) * nv, s.stream));
     }
     dev_free(s, A->recv); dev_free(s, A->trace); dev_free(s, A->gmom); dev_free(s, A->mom);
@@ -464,33 +503,53 @@ void adjoint_backward(Solver& s, int nrec, const char* const* files, const float
     if (!tr.empty()) SORD_CUDA(cudaMemcpyAsync(A->trace, tr.data(), sizeof(float) * tr.size(), cudaMemcpyHostToDevice, s.stream));
     SORD_CUDA(dev_malloc(s, (void**)&A->gmom, sizeof(double) * std::max(nmom, 1)));
     SORD_CUDA(cudaMemsetAsync(A->gmom, 0, sizeof(double) * std::max(nmom, 1), s.stream));
-    const int cap = 4096;
-    SORD_CUDA(dev_malloc(s, (void**)&A->mom, sizeof(MomEntry) * cap));
+    // moment-source entries of every step, uploaded once: me[moff[n] .. moff[n+1])
     std::vector<MomEntry> me;
-    MomEntry* hmom = (MomEntry*)pinned_get(sizeof(MomEntry) * cap);
-    cudaEvent_t mev = nullptr;
-    SORD_CUDA(cudaEventCreateWithFlags(&mev, cudaEventDisableTiming));
-    SORD_CUDA(cudaEventRecord(mev, s.stream));
+    std::vector<int> moff(s.nt + 2, 0);
+    for (int n = 1; n <= s.nt; n++) {
+        moff[n] = (int)me.size();
+        s.it = n;
+        s.tm = s.prm.tm0 + g.dt * (float)(n - 1);
+        for (size_t m = 0; m < A->mom_ops.size(); m++) {
+            const IoOp& io = s.ops[A->mom_ops[m]];
+            std::vector<Inject> e;
+            moment_entries(s, A->mom_ops[m], e);
+            for (const Inject& x : e)
+                if (io.val != 0.f) me.push_back(MomEntry{x.idx, x.comp, (int)m, x.inc / io.val});
+        }
+    }
+    moff[s.nt + 1] = (int)me.size();
+    SORD_CUDA(dev_malloc(s, (void**)&A->mom, sizeof(MomEntry) * std::max<size_t>(me.size(), 1)));
+    if (!me.empty())
+        SORD_CUDA(cudaMemcpyAsync(A->mom, me.data(), sizeof(MomEntry) * me.size(), cudaMemcpyHostToDevice, s.stream));
 
     AdjArgs K;
     K.g = g;
     K.br = s.br;
-    for (int i = 0; i < 3; i++) { K.ub[i] = A->ub[i]; K.vb[i] = A->vb[i]; K.fb[i] = A->fb[i]; }
-    K.cs = A->cs;
     K.lam = s.d.lam; K.mu = s.d.mu; K.yy = s.d.yy; K.vc = s.d.vc; K.mr = s.d.mr; K.gam = s.d.gam;
     K.glam = A->glam; K.gmu = A->gmu; K.gyy = A->gyy; K.gmr = A->gmr;
     K.hg1 = s.prm.hourglass[0];
     K.dh2 = g.dt * s.prm.hourglass[1];
+    K.dt = g.dt;
     K.hourglass = (s.prm.hourglass[0] > 0.f || s.prm.hourglass[1] > 0.f) ? 1 : 0;
-    float** dfb = nullptr;  // device copies of the three fbar / ubar / vbar pointers
-    SORD_CUDA(dev_malloc(s, (void**)&dfb, sizeof(float*) * 9));
-    float* hp[9] = {A->fb[0], A->fb[1], A->fb[2], A->ub[0], A->ub[1], A->ub[2], A->vb[0], A->vb[1], A->vb[2]};
-    SORD_CUDA(cudaMemcpyAsync(dfb, hp, sizeof hp, cudaMemcpyHostToDevice, s.stream));
+    // tiles over the force nodes; planes split so that each SM gets a few blocks
+    int sms = 148;
+    SORD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s.device));
+    K.nbx = (g.i2node[0] - g.i1node[0] + AJ - 1) / (AJ - 1);
+    const int nby = (g.i2node[1] - g.i1node[1] + AK - 1) / (AK - 1);
+    const int planes = g.i2node[2] - g.i1node[2] + 1;
+    const int nsg = std::max(1, std::min((4 * sms + K.nbx * nby - 1) / (K.nbx * nby), planes / 8));
+    K.segl = (planes + nsg - 1) / nsg;
+    const dim3 agrid((unsigned)(K.nbx * nby), (unsigned)((planes + K.segl - 1) / K.segl));
+    smem_limit((const void*)k_adj_step, (int)kAdjSmem);
+    int cur = 0;  // buffer holding the adjoint state of step n + 1
+    // device time of the backward pass (sord_last_step_ms), set-up and
+    // allocations excluded
+    SORD_CUDA(cudaEventRecord(s.ev0, s.stream));
 
     const int seg = A->seg;
     const int nseg = (s.nt + seg - 1) / seg;
     if (A->nck < (seg == 1 ? s.nt + 1 : nseg)) throw SordError(SORD_E_STATE, "adjoint: missing checkpoints");
-    const unsigned gb = gsz((long long)nv);
     for (int k = nseg - 1; k >= 0; k--) {
         const int n0 = k * seg, n1 = std::min(s.nt, n0 + seg);
         if (seg > 1) {
@@ -502,39 +561,30 @@ void adjoint_backward(Solver& s, int nrec, const char* const* files, const float
         }
         for (int n = n1; n >= n0 + 1; n--) {
             const float* st = seg > 1 ? A->segbuf + (size_t)(n - n0 - 1) * 9 * nv : A->ckpt[n];
-            for (int i = 0; i < 3; i++) { K.u[i] = st + i * nv; K.v[i] = st + (3 + i) * nv; K.a[i] = st + (6 + i) * nv; }
-            k_adj_mass<<<gb, 256, 0, s.stream>>>(K, g.dt);
-            k_adj_cells<<<gb, 256, 0, s.stream>>>(K);
+            for (int i = 0; i < 3; i++) {
+                K.u[i] = st + i * nv; K.v[i] = st + (3 + i) * nv; K.a[i] = st + (6 + i) * nv;
+                K.ubi[i] = A->ub[cur][i]; K.vbi[i] = A->vb[cur][i];
+                K.ubo[i] = A->ub[1 - cur][i]; K.vbo[i] = A->vb[1 - cur][i];
+            }
             // moment sources of step n
-            me.clear();
-            s.it = n;
-            s.tm = s.prm.tm0 + g.dt * (float)(n - 1);
-            for (size_t m = 0; m < A->mom_ops.size(); m++) {
-                const IoOp& io = s.ops[A->mom_ops[m]];
-                std::vector<Inject> e;
-                moment_entries(s, A->mom_ops[m], e);
-                for (const Inject& x : e)
-                    if (io.val != 0.f) me.push_back(MomEntry{x.idx, x.comp, (int)m, x.inc / io.val});
+            const int nme = moff[n + 1] - moff[n];
+            if (nme > 0) k_adj_moment<<<1, 128, 0, s.stream>>>(K, A->mom + moff[n], nme, A->gmom);
+            k_adj_step<<<agrid, dim3(AJ, AK), kAdjSmem, s.stream>>>(K);
+            cur = 1 - cur;
+            if (A->nrecv) {
+                Ptr3 pu{{A->ub[cur][0], A->ub[cur][1], A->ub[cur][2]}}, pv{{A->vb[cur][0], A->vb[cur][1], A->vb[cur][2]}};
+                k_adj_recv<<<std::max(1, (A->nrecv + 255) / 256), 256, 0, s.stream>>>(A->recv, A->nrecv, n, A->trace, pu, pv);
             }
-            if (!me.empty()) {
-                if ((int)me.size() > cap) throw SordError(SORD_E_PARAM, "adjoint: too many moment injections in one step");
-                SORD_CUDA(cudaEventSynchronize(mev));
-                std::memcpy(hmom, me.data(), sizeof(MomEntry) * me.size());
-                SORD_CUDA(cudaMemcpyAsync(A->mom, hmom, sizeof(MomEntry) * me.size(), cudaMemcpyHostToDevice, s.stream));
-                SORD_CUDA(cudaEventRecord(mev, s.stream));
-                k_adj_moment<<<1, 128, 0, s.stream>>>(g, s.br, A->mom, (int)me.size(), dfb, s.d.vc, A->gmom);
-            }
-            k_adj_nodes<<<gb, 256, 0, s.stream>>>(K);
-            if (A->nrecv)
-                k_adj_recv<<<std::max(1, (A->nrecv + 255) / 256), 256, 0, s.stream>>>(A->recv, A->nrecv, n, A->trace, dfb + 3, dfb + 6);
-            s.launches += 3 + (me.empty() ? 0 : 1) + (A->nrecv ? 1 : 0);
+            s.launches += 1 + (nme > 0 ? 1 : 0) + (A->nrecv ? 1 : 0);
             SORD_CUDA(cudaGetLastError());
         }
     }
     s.it = s.nt;
-    SORD_CUDA(cudaEventSynchronize(mev));
-    cudaEventDestroy(mev);
-    pinned_put(hmom);
+    SORD_CUDA(cudaEventRecord(s.ev1, s.stream));
+    SORD_CUDA(cudaEventSynchronize(s.ev1));
+    float ms = 0;
+    SORD_CUDA(cudaEventElapsedTime(&ms, s.ev0, s.ev1));
+    s.last_step_ms = ms;
     // gradients of the real cells and nodes, global order (j fastest)
     std::vector<float> buf(nv);
     auto out = [&](const float* d, float* host, bool cell) {
@@ -555,7 +605,6 @@ void adjoint_backward(Solver& s, int nrec, const char* const* files, const float
         SORD_CUDA(cudaMemcpyAsync(gmom, A->gmom, sizeof(double) * nmom, cudaMemcpyDeviceToHost, s.stream));
         SORD_CUDA(cudaStreamSynchronize(s.stream));
     }
-    dev_free(s, dfb);
     SORD_CUDA(cudaStreamSynchronize(s.stream));
 }
 

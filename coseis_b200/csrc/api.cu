@@ -190,16 +190,17 @@ static bool tensor_point_ops(Solver& s, const char* const* names, std::vector<In
 
 static InjectList upload(Solver& s, int slot, const std::vector<Inject>& e) {
     if ((int)e.size() > kMaxInject) throw SordError(SORD_E_PARAM, "too many point injections in one step");
-    InjectList l{s.d.inj + slot * kMaxInject, (int)e.size()};
-    if (!e.empty()) {
-        Inject* h = s.hinj + slot * kMaxInject;
-        // the previous step's copy from this slot must have completed
-        SORD_CUDA(cudaEventSynchronize(s.inj_done[slot]));
-        std::memcpy(h, e.data(), sizeof(Inject) * e.size());
-        SORD_CUDA(cudaMemcpyAsync(s.d.inj + slot * kMaxInject, h, sizeof(Inject) * e.size(), cudaMemcpyHostToDevice, s.stream));
-        SORD_CUDA(cudaEventRecord(s.inj_done[slot], s.stream));
-    }
-    return l;
+    if (e.empty()) return InjectList{s.d.inj + inj_off(slot, 0), 0};
+    // a ring of staging buffers per slot: the copy that last used buffer r
+    // (kInjectRing uploads ago) must have completed before it is refilled
+    const int r = s.inj_ring[slot];
+    s.inj_ring[slot] = (r + 1) % kInjectRing;
+    Inject* h = s.hinj + inj_off(slot, r);
+    SORD_CUDA(cudaEventSynchronize(s.inj_done[slot][r]));
+    std::memcpy(h, e.data(), sizeof(Inject) * e.size());
+    SORD_CUDA(cudaMemcpyAsync(s.d.inj + inj_off(slot, r), h, sizeof(Inject) * e.size(), cudaMemcpyHostToDevice, s.stream));
+    SORD_CUDA(cudaEventRecord(s.inj_done[slot][r], s.stream));
+    return InjectList{s.d.inj + inj_off(slot, r), (int)e.size()};
 }
 
 // One forward step n with no field-I/O hook: leapfrog update, then the
@@ -571,7 +572,8 @@ void Solver::destroy() {
         pinned_put(pin_io[i]);
         if (pin_ev[i]) cudaEventDestroy(pin_ev[i]);
     }
-    for (auto& e : inj_done) if (e) cudaEventDestroy(e);
+    for (auto& row : inj_done)
+        for (auto& e : row) if (e) cudaEventDestroy(e);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) {
@@ -631,7 +633,8 @@ int sord_create(const char* workdir, const char* sord_in_text, int device, sord_
         s.mem_attached = true;
         SORD_CUDA(cudaEventCreate(&s.ev0));
         SORD_CUDA(cudaEventCreate(&s.ev1));
-        for (auto& e : s.inj_done) SORD_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        for (auto& row : s.inj_done)
+            for (auto& e : row) SORD_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         s.prm = parse_sord_in(sord_in_text, s.ops);
         setup_all(s);
     } catch (const std::exception& e) {
@@ -694,13 +697,7 @@ int sord_adjoint_backward(sord_handle* h, int nrec, const char* const* files, co
     Solver& s = h->s;
     try {
         SORD_CUDA(cudaSetDevice(s.device));
-        SORD_CUDA(cudaEventRecord(s.ev0, s.stream));
         adjoint_backward(s, nrec, files, dtrace, ntrace, grad_lam, grad_mu, grad_yy, grad_mr, grad_moment, nmoment);
-        SORD_CUDA(cudaEventRecord(s.ev1, s.stream));
-        SORD_CUDA(cudaEventSynchronize(s.ev1));
-        float ms = 0;
-        SORD_CUDA(cudaEventElapsedTime(&ms, s.ev0, s.ev1));
-        s.last_step_ms = ms;
     } catch (const std::exception& e) {
         return fail(h, e);
     }

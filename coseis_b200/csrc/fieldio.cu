@@ -619,9 +619,9 @@ static void field_io_op(Solver& s, size_t opi, FieldView f, ProbeBatch& batch) {
             point_injection(s, io, f, 0, e);
             if (!e.empty()) {
                 if ((int)e.size() > kMaxInject) throw SordError(SORD_E_PARAM, "too many point injections");
-                Inject* h = s.hinj + 3 * kMaxInject;
+                Inject* h = s.hinj + inj_off(3, 0);
                 std::memcpy(h, e.data(), sizeof(Inject) * e.size());
-                Inject* dptr = s.d.inj + 3 * kMaxInject;
+                Inject* dptr = s.d.inj + inj_off(3, 0);
                 SORD_CUDA(cudaMemcpyAsync(dptr, h, sizeof(Inject) * e.size(), cudaMemcpyHostToDevice, s.stream));
                 float* F6[6] = {f.p, f.p, f.p, f.p, f.p, f.p};
                 InjectList l{dptr, (int)e.size()};

@@ -156,12 +156,6 @@ __device__ __forceinline__ long long slab_idx(const Geom& g, int axis, int t, in
 }
 
 // 4-byte asynchronous global -> shared copy (no register staging).
-__device__ __forceinline__ void cp_async4(float* smem, const float* gmem) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // Shared-memory layout of the PML-shell kernel: plain per-field planes
 // (node ring: w(3), hourglass input(3), coordinates; cell ring: stress(6),

@@ -104,6 +104,8 @@ struct Inject {
 };
 static const int kMaxInject = 256;
 static const int kInjectSlots = 4;  // 0 potency, 1 moment, 2 force, 3 field-I/O '.' ops
+static const int kInjectRing = 16;  // uploads in flight per slot (the host runs that far ahead)
+inline size_t inj_off(int slot, int r) { return ((size_t)slot * kInjectRing + (size_t)r) * kMaxInject; }
 
 // Layout of the reduction scratch Device::red (16384 floats):
 static const int kRedBad = 15;        // unsigned index: rectilinear check flag
@@ -155,6 +157,16 @@ struct StepArgs {
     int fax, firup;
     float* fout[3];
 };
+
+#ifdef __CUDACC__
+// 4-byte asynchronous global -> shared copies (cp.async) and their groups
+__device__ __forceinline__ void cp_async4(float* smem, const float* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+#endif
 
 // Device state of one handle.
 struct Device {
@@ -293,7 +305,8 @@ struct Solver {
     FusedPlan* fplan = nullptr;
     struct AdjointState* adj = nullptr;  // checkpoints and adjoint fields (adjoint.cu)
     bool mem_attached = false;  // holds a reference on the device's memory pool
-    cudaEvent_t inj_done[kInjectSlots] = {};
+    cudaEvent_t inj_done[kInjectSlots][kInjectRing] = {};
+    int inj_ring[kInjectSlots] = {};
     // fault bookkeeping
     int fn3[3] = {0, 0, 0};
     float* fa(int a) const { return d.fp + (long long)a * d.np; }
