@@ -354,6 +354,18 @@ __global__ void k_adj_recv(const RecvEntry* e, int n, int it, const float* trace
     }
 }
 
+// Leapfrog update of time_integration.f90:32-35 from state p (u, v, a; 9 nv
+// floats) into state q, whose a is then written by the fused step.
+__global__ void k_adj_advance(const float* __restrict__ p, float* __restrict__ q, long long nv, float dt) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv; i += (long long)gridDim.x * blockDim.x)
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const float a = p[(3 + c) * nv + i] + dt * p[(6 + c) * nv + i];
+            q[(3 + c) * nv + i] = a;
+            q[c * nv + i] = p[c * nv + i] + dt * a;
+        }
+}
+
 // ------------------------------------------------------------ host
 
 void adjoint_free(Solver& s) {
@@ -391,21 +403,22 @@ void adjoint_check(Solver& s) {
     if (P.nsource != 0) throw SordError(SORD_E_PARAM, "adjoint: finite source files are not supported");
 }
 
-static void save_state(Solver& s, float* dst) {
-    const size_t nv = (size_t)s.g.nv, b = sizeof(float) * nv;
-    for (int i = 0; i < 3; i++) {
-        SORD_CUDA(cudaMemcpyAsync(dst + (0 + i) * nv, s.d.u[i], b, cudaMemcpyDeviceToDevice, s.stream));
-        SORD_CUDA(cudaMemcpyAsync(dst + (3 + i) * nv, s.d.v[i], b, cudaMemcpyDeviceToDevice, s.stream));
-        SORD_CUDA(cudaMemcpyAsync(dst + (6 + i) * nv, s.d.w1n[i], b, cudaMemcpyDeviceToDevice, s.stream));
-    }
+// (u, v, a) of the solver into one state record of 9 nv floats, one kernel
+struct State9 {
+    const float* p[9];
+};
+__global__ void k_adj_save(State9 src, float* __restrict__ dst, long long nv) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv; i += (long long)gridDim.x * blockDim.x)
+#pragma unroll
+        for (int c = 0; c < 9; c++) dst[c * nv + i] = src.p[c][i];
 }
-static void load_state(Solver& s, const float* src) {
-    const size_t nv = (size_t)s.g.nv, b = sizeof(float) * nv;
-    for (int i = 0; i < 3; i++) {
-        SORD_CUDA(cudaMemcpyAsync(s.d.u[i], src + (0 + i) * nv, b, cudaMemcpyDeviceToDevice, s.stream));
-        SORD_CUDA(cudaMemcpyAsync(s.d.v[i], src + (3 + i) * nv, b, cudaMemcpyDeviceToDevice, s.stream));
-        SORD_CUDA(cudaMemcpyAsync(s.d.w1n[i], src + (6 + i) * nv, b, cudaMemcpyDeviceToDevice, s.stream));
-    }
+static void save_state(Solver& s, float* dst) {
+    const long long nv = s.g.nv;
+    State9 src;
+    for (int i = 0; i < 3; i++) { src.p[i] = s.d.u[i]; src.p[3 + i] = s.d.v[i]; src.p[6 + i] = s.d.w1n[i]; }
+    k_adj_save<<<(unsigned)std::max(1LL, std::min((nv + 255) / 256, 148LL * 16)), 256, 0, s.stream>>>(src, dst, nv);
+    s.launches++;
+    SORD_CUDA(cudaGetLastError());
 }
 
 int adjoint_segment(Solver& s, int seg) {
@@ -447,7 +460,7 @@ void adjoint_checkpoint(Solver& s) {
     save_state(s, A->ckpt[A->nck++]);
 }
 
-void bare_step(Solver& s, int n);
+void bare_step(Solver& s, int n, bool update);
 void moment_entries(Solver& s, int opi, std::vector<Inject>& out);
 int probe_of_op(const Solver& s, size_t opi, long long* idx, float* r);
 
@@ -543,6 +556,19 @@ void adjoint_backward(Solver& s, int nrec, const char* const* files, const float
     const dim3 agrid((unsigned)(K.nbx * nby), (unsigned)((planes + K.segl - 1) / K.segl));
     smem_limit((const void*)k_adj_step, (int)kAdjSmem);
     int cur = 0;  // buffer holding the adjoint state of step n + 1
+    // the solver's own state arrays: recomputation points u, v, w1n into the
+    // segment buffer; this guard puts them back on every exit
+    struct Live {
+        Solver& s;
+        float* p[9];
+        explicit Live(Solver& s_) : s(s_) {
+            for (int i = 0; i < 3; i++) { p[i] = s.d.u[i]; p[3 + i] = s.d.v[i]; p[6 + i] = s.d.w1n[i]; }
+        }
+        void restore() {
+            for (int i = 0; i < 3; i++) { s.d.u[i] = p[i]; s.d.v[i] = p[3 + i]; s.d.w1n[i] = p[6 + i]; }
+        }
+        ~Live() { restore(); }
+    } live(s);
     // device time of the backward pass (sord_last_step_ms), set-up and
     // allocations excluded
     SORD_CUDA(cudaEventRecord(s.ev0, s.stream));
@@ -553,11 +579,20 @@ void adjoint_backward(Solver& s, int nrec, const char* const* files, const float
     for (int k = nseg - 1; k >= 0; k--) {
         const int n0 = k * seg, n1 = std::min(s.nt, n0 + seg);
         if (seg > 1) {
-            load_state(s, A->ckpt[k]);
+            // recompute the segment from its checkpoint straight into the
+            // segment buffer: the leapfrog update reads state n - 1 and
+            // writes state n, then the fused step runs on state n in place
+            const float* prev = A->ckpt[k];
             for (int n = n0 + 1; n <= n1; n++) {
-                bare_step(s, n);
-                save_state(s, A->segbuf + (size_t)(n - n0 - 1) * 9 * nv);
+                float* st = A->segbuf + (size_t)(n - n0 - 1) * 9 * nv;
+                k_adj_advance<<<std::max(1LL, std::min((long long)(nv + 255) / 256, 148LL * 16)), 256, 0, s.stream>>>(
+                    prev, st, (long long)nv, g.dt);
+                for (int i = 0; i < 3; i++) { s.d.u[i] = st + i * nv; s.d.v[i] = st + (3 + i) * nv; s.d.w1n[i] = st + (6 + i) * nv; }
+                bare_step(s, n, false);
+                s.launches++;
+                prev = st;
             }
+            live.restore();
         }
         for (int n = n1; n >= n0 + 1; n--) {
             const float* st = seg > 1 ? A->segbuf + (size_t)(n - n0 - 1) * 9 * nv : A->ckpt[n];

@@ -203,15 +203,16 @@ static InjectList upload(Solver& s, int slot, const std::vector<Inject>& e) {
     return InjectList{s.d.inj + inj_off(slot, r), (int)e.size()};
 }
 
-// One forward step n with no field-I/O hook: leapfrog update, then the
-// fused stress/force/acceleration step with the point sources of step n,
-// unfolded, so that u, v and w1n = a are the state after step n.  The
+// One forward step n with no field-I/O hook: leapfrog update (unless the
+// caller has done it), then the fused stress/force/acceleration step with
+// the point sources of step n, unfolded, so that u, v and w1n = a are the
+// state after step n.  The
 // adjoint recomputes checkpointed segments with it; every step of such a run
 // is fusable, and the arithmetic is that of Solver::step.
-void bare_step(Solver& s, int n) {
+void bare_step(Solver& s, int n, bool update) {
     s.it = n;
     s.tm = s.prm.tm0 + s.g.dt * (float)(n - 1);
-    launch_time_update(s, false);
+    if (update) launch_time_update(s, false);
     std::vector<Inject> pot, mom, frc;
     tensor_point_ops(s, kPot, pot);
     tensor_point_ops(s, kMom, mom);
