@@ -138,3 +138,24 @@ def test_adjoint_gradient_vs_finite_differences(segment, tmp_path, oracle_bins, 
         fd = (L(*plus, tag='p%d' % k) - L(*minus, tag='m%d' % k)) / (2 * H_FD)
         an = sum((g * x * dx).sum() for g, x, dx in zip(G, base, d))
         assert abs(an - fd) <= TOL * abs(fd), (k, an, fd)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize('change,msg', [({'bc1': ['pml'] * 3, 'bc2': ['pml'] * 3, 'npml': 3}, 'no PML'),
+                                        ({'gridnoise': 0.05}, 'rectilinear')])
+def test_adjoint_rejects_unsupported_runs(change, msg, tmp_path, gpu_lib):
+    """PML and non-rectilinear meshes stay forward-only: the adjoint forward
+    refuses them with SORD_E_PARAM before running."""
+    from coseis_b200 import _lib
+    p = problem()
+    p.prm.update(change)
+    rho, vp, vs, m = model(1)
+    d = str(tmp_path)
+    p.stage(rho, vp, vs, m, d)
+    s = _lib.Solver(d, open(os.path.join(d, 'sord.in')).read())
+    try:
+        with pytest.raises(_lib.SordError) as e:
+            s.adjoint_forward(1)
+        assert e.value.code == _lib.SORD_E_PARAM and msg in str(e.value)
+    finally:
+        s.close()

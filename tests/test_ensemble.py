@@ -70,3 +70,23 @@ def test_ensemble_matches_oracle_and_serial(tmp_path, oracle_bins, gpu_lib):
         assert np.fromfile(os.path.join(a, 'trup.bin'), '<f4').min() < 1e8, 'no rupture'
         _check(sc.compare(a, b))
         _check(sc.compare(c, b))
+
+
+def test_front_end_run_ensemble_stages_every_case(tmp_path):
+    """coseis_b200.sord.run_ensemble stages each parameter dict in its own
+    directory before the single library call; without a device that call
+    fails with the CUDA error, with the directories staged."""
+    from coseis_b200 import _lib, sord
+    cases = [sc.case_explosion(n=15, nt=2, npml=3), sc.case_pml(n=14, nt=2)]
+    dirs = [str(tmp_path / 'a'), str(tmp_path / 'b')]
+    try:
+        metas = sord.run_ensemble(cases, dirs, nthreads=2)
+    except _lib.SordError as e:
+        assert e.code == _lib.SORD_E_CUDA
+    else:
+        assert len(metas) == 2
+    for d in dirs:
+        assert os.path.exists(os.path.join(d, 'sord.in'))
+        assert os.path.exists(os.path.join(d, 'meta.json'))
+    with pytest.raises(ValueError):
+        sord.run_ensemble(cases, dirs[:1])
