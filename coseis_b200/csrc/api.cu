@@ -569,7 +569,7 @@ void Solver::destroy() {
     prof_ev.clear();
     pinned_put(hinj);
     fr(d_stage);
-    for (int i = 0; i < 4; i++) {
+    for (int i = 0; i < (int)(sizeof(pin_io) / sizeof(pin_io[0])); i++) {
         pinned_put(pin_io[i]);
         if (pin_ev[i]) cudaEventDestroy(pin_ev[i]);
     }

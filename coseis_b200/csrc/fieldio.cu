@@ -386,7 +386,7 @@ static void magnitude(Solver& s, const std::string& fl) {
 // 8 M floats with pread into their own pinned buffer and copy it to the
 // device on the solver's stream; a thread waits for its previous copy before
 // reusing its buffer.
-static constexpr int kReaders = 4;
+static constexpr int kReaders = 8;
 static constexpr size_t kChunk = (size_t)8 << 20;
 static void read_to_device(Solver& s, const std::string& fn, size_t off, size_t count, float* dst) {
     static_assert(kReaders <= (int)(sizeof(s.pin_io) / sizeof(s.pin_io[0])), "pinned buffers");

@@ -200,8 +200,11 @@ __global__ void k_ref_brackets(Geom g, const float* x0, const float* x1, const f
     for (int a = 0; a < 3; a++) brackets_cn(XN, a, out + 24 + 8 * a);
 }
 
+// Mismatch bits are gathered per thread (a direction already found to differ
+// is not tested again) and merged with one atomic per warp.
 __global__ void k_rect_check(Geom g, const float* x0, const float* x1, const float* x2, const float* ref, unsigned* bad) {
     const float* X_[3] = {x0, x1, x2};
+    unsigned m = 0;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < g.nv; q += (long long)gridDim.x * blockDim.x) {
         int p[3] = {(int)(q % g.sy) + 1, (int)((q / g.sy) % g.nm[1]) + 1, (int)(q / g.sz) + 1};
         // cell test
@@ -213,10 +216,11 @@ __global__ void k_rect_check(Geom g, const float* x0, const float* x1, const flo
             for (int c = 0; c < 3; c++)
                 for (int n = 0; n < 8; n++) X[c][n] = X_[c][q + (n & 1) + ((n >> 1) & 1) * g.sy + ((n >> 2) & 1) * g.sz];
             for (int a = 0; a < 3; a++) {
+                if (m & (1u << a)) continue;
                 float B[8];
                 brackets_nc(X, a, B);
                 for (int t = 0; t < 8; t++)
-                    if (!(B[t] == ref[8 * a + t])) atomicOr(bad, 1u << a);
+                    if (!(B[t] == ref[8 * a + t])) m |= 1u << a;
             }
         }
         // node test: terms whose cell is real and off the fault plane
@@ -229,6 +233,7 @@ __global__ void k_rect_check(Geom g, const float* x0, const float* x1, const flo
             };
             const int ct[8] = {-1, 0, -1, 0, -1, 0, -1, 0}, kt[8] = {-1, -1, -1, -1, 0, 0, 0, 0}, lt[8] = {-1, -1, 0, 0, -1, -1, 0, 0};
             for (int a = 0; a < 3; a++) {
+                if (m & (8u << a)) continue;
                 float B[8];
                 brackets_cn(XN, a, B);
                 for (int t = 0; t < 8; t++) {
@@ -236,19 +241,24 @@ __global__ void k_rect_check(Geom g, const float* x0, const float* x1, const flo
                     bool real = true;
                     for (int d = 0; d < 3; d++) real = real && c[d] >= g.i1cell[d] && c[d] <= g.i2cell[d];
                     if (g.ifn && c[g.ifn - 1] == g.irup) real = false;
-                    if (real && !(B[t] == ref[24 + 8 * a + t])) atomicOr(bad, 8u << a);
+                    if (real && !(B[t] == ref[24 + 8 * a + t])) m |= 8u << a;
                 }
             }
         }
     }
+    m = __reduce_or_sync(0xffffffffu, m);
+    if ((threadIdx.x & 31) == 0 && m) atomicOr(bad, m);
 }
 
 // terrain mesh test: x depends on j only and y on k only (bit 64 if not)
 __global__ void k_terrain_check(Geom g, const float* x0, const float* x1, const float* x1d, const float* y1d, unsigned* bad) {
+    unsigned m = 0;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < g.nv; q += (long long)gridDim.x * blockDim.x) {
         int j = (int)(q % g.sy) + 1, k = (int)((q / g.sy) % g.nm[1]) + 1;
-        if (!(x0[q] == x1d[j - 1]) || !(x1[q] == y1d[k - 1])) atomicOr(bad, 64u);
+        if (!(x0[q] == x1d[j - 1]) || !(x1[q] == y1d[k - 1])) m = 64u;
     }
+    m = __reduce_or_sync(0xffffffffu, m);
+    if ((threadIdx.x & 31) == 0 && m) atomicOr(bad, m);
 }
 __global__ void k_line(const float* src, float* dst, int n, long long stride, long long base) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;

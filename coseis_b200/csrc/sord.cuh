@@ -299,8 +299,8 @@ struct Solver {
     // pinned chunk buffers for the file reads
     float* d_stage = nullptr;
     size_t stage_cap = 0;
-    float* pin_io[4] = {nullptr, nullptr, nullptr, nullptr};
-    cudaEvent_t pin_ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    float* pin_io[8] = {};     // pinned chunks of the whole-volume input readers
+    cudaEvent_t pin_ev[8] = {};
     // work decomposition of the fused step kernels (fused.cu)
     FusedPlan* fplan = nullptr;
     struct AdjointState* adj = nullptr;  // checkpoints and adjoint fields (adjoint.cu)
