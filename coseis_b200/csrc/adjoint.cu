@@ -63,7 +63,6 @@ struct AdjointState {
     float* trace = nullptr;
     MomEntry* mom = nullptr;
     double* gmom = nullptr;
-    int nmomslot = 0;
     std::vector<int> recv_ops;  // op indices of '.>' receivers, recorded before the forward run
     std::vector<int> mom_ops;   // op indices of '.' moment ops
 };
