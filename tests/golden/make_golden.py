@@ -17,6 +17,9 @@ files.
   pulse), sampled on the solver's output times, unfiltered and after the
   lowpass of scripts/Explosion-plot.py:54-58 (cst/dsp.py:107-142), plus a
   probe vector through the same filter to pin its restatement.
+* srf.json -- a small synthetic SRF rupture read and written by the
+  reference (cst/srf.py:13-194) and the fault geometry of its points
+  (cst/coord.py:190-202 slip_vectors, 336-351 potency_tensor).
 * frontend.json -- for several parameter sets, the sord.in text and the
   metadata (indices, shapes, deltas) that the reference front end produces:
   cst/sord.py:prepare (cst/sord.py:296-468) followed by the sord.in
@@ -187,6 +190,58 @@ def make_explosion(ref):
                 plot_analytic_first=float(va[0]))
 
 
+# A small synthetic SRF rupture (one plane of 3 x 2 points) for the SRF
+# reader / writer / geometry fixtures; all numbers are made up here.
+SRF_TEXT = """1.0
+PLANE 1
+-118.0 34.0 3 2 3.0 2.0
+30.0 60.0 0.5 1.0 0.8
+POINTS 6
+-118.01 34.00 1.0 30.0 60.0 100000000.0 0.10 0.01
+90.0 20.0 3 5.0 2 0.0 0
+1.0 2.0 3.0 4.0 5.0
+-118.00 34.00 1.0 30.0 60.0 100000000.0 0.15 0.01
+45.0 30.0 4 0.0 0 10.0 1
+0.5 1.5 2.5 3.5 7.0
+-117.99 34.00 1.0 31.0 61.0 100000000.0 0.20 0.02
+0.0 10.0 2 0.0 0 0.0 0
+6.0 8.0
+-118.01 34.01 1.9 30.0 60.0 100000000.0 0.30 0.01
+-30.0 0.0 0 12.0 3 0.0 0
+1.0 1.0 1.0
+-118.00 34.01 1.9 29.0 59.0 100000000.0 0.35 0.01
+170.0 15.0 1 15.0 1 1.0 1
+2.0 3.0 4.0
+-117.99 34.01 1.9 30.0 60.0 100000000.0 0.40 0.01
+90.0 0.0 0 0.0 0 0.0 0
+
+"""
+
+
+def make_srf(ref):
+    """Reference SRF read of SRF_TEXT, its write, and the fault geometry of
+    every point (cst/srf.py:13-194, cst/coord.py:190-202, 336-351)."""
+    import io
+    sys.path.insert(0, ref)
+    from cst import coord, srf
+    fh = io.StringIO(SRF_TEXT)
+    fh.name = 'synthetic.srf'
+    meta, data = srf.read(fh)
+    # the reference writer indexes the arrays by point, so it needs them in
+    # file order (read reshapes single-plane files to the plane grid)
+    fdata = {k: (np.asarray(v).T.ravel() if np.ndim(v) > 1 else v) for k, v in data.items()}
+    out = io.StringIO()
+    srf.write(out, (meta, fdata))
+    flat = {k: np.asarray(v).T.ravel().tolist() for k, v in data.items() if not k.startswith('sv')}
+    R = coord.slip_vectors(np.asarray(flat['stk']), np.asarray(flat['dip']), np.asarray(flat['rake']))
+    R = np.asarray([[np.asarray(c, dtype=float) for c in row] for row in R])
+    pot = [coord.potency_tensor(R[2], R[0]), coord.potency_tensor(R[2], R[1]), coord.potency_tensor(R[2], R[2])]
+    return {'text': SRF_TEXT, 'meta': meta, 'data': flat,
+            'sv': [np.asarray(data['sv%d' % c]).tolist() for c in (1, 2, 3)],
+            'written': out.getvalue(), 'slip_vectors': R.tolist(),
+            'potency': [[np.asarray(a, dtype=float).tolist() for a in part] for p_ in pot for part in p_]}
+
+
 def main():
     ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('COSEIS_REFERENCE', '')
     if not ref or not os.path.isdir(os.path.join(ref, 'cst')):
@@ -198,6 +253,8 @@ def main():
         json.dump(make_kostrov(ref), fh, indent=1, sort_keys=True)
     with open(os.path.join(HERE, 'explosion.json'), 'w') as fh:
         json.dump(make_explosion(ref), fh, indent=1, sort_keys=True)
+    with open(os.path.join(HERE, 'srf.json'), 'w') as fh:
+        json.dump(make_srf(ref), fh, indent=1, sort_keys=True, default=lambda o: o.item())
 
 
 if __name__ == '__main__':
