@@ -54,7 +54,7 @@ struct AdjointState {
     int seg = 0;
     int nck = 0;               // checkpoints stored
     std::vector<float*> ckpt;  // (u, v, a) at steps 0, seg, 2 seg, ...; 9 nv floats each
-    float* segbuf = nullptr;   // seg states of 9 nv floats
+    float* segbuf[2] = {};     // two segment buffers of seg states (9 nv floats each)
     float* ub[2][3] = {};      // adjoint state, double-buffered
     float* vb[2][3] = {};
     float *glam = nullptr, *gmu = nullptr, *gyy = nullptr, *gmr = nullptr;
@@ -371,7 +371,8 @@ void adjoint_free(Solver& s) {
     AdjointState* A = s.adj;
     if (!A) return;
     for (float* p : A->ckpt) dev_free(s, p);
-    dev_free(s, A->segbuf);
+    dev_free(s, A->segbuf[0]);
+    dev_free(s, A->segbuf[1]);
     for (int b = 0; b < 2; b++)
         for (int i = 0; i < 3; i++) { dev_free(s, A->ub[b][i]); dev_free(s, A->vb[b][i]); }
     dev_free(s, A->glam); dev_free(s, A->gmu); dev_free(s, A->gyy); dev_free(s, A->gmr);
@@ -459,7 +460,7 @@ void adjoint_checkpoint(Solver& s) {
     save_state(s, A->ckpt[A->nck++]);
 }
 
-void bare_step(Solver& s, int n, bool update);
+void bare_step(Solver& s, int n, bool update, bool fold);
 void moment_entries(Solver& s, int opi, std::vector<Inject>& out);
 int probe_of_op(const Solver& s, size_t opi, long long* idx, float* r);
 
@@ -495,7 +496,8 @@ void adjoint_backward(Solver& s, int nrec, const char* const* files, const float
         for (int b = 0; b < 2; b++)
             for (int i = 0; i < 3; i++) { A->ub[b][i] = dalloc(s, nv); A->vb[b][i] = dalloc(s, nv); }
         A->glam = dalloc(s, nv); A->gmu = dalloc(s, nv); A->gyy = dalloc(s, nv); A->gmr = dalloc(s, nv);
-        if (A->seg > 1) A->segbuf = dalloc(s, (size_t)A->seg * 9 * nv);
+        if (A->seg > 1)
+            for (int b = 0; b < 2; b++) A->segbuf[b] = dalloc(s, (size_t)A->seg * 9 * nv);
     } else {
         for (int b = 0; b < 2; b++)
             for (int i = 0; i < 3; i++) {
@@ -559,12 +561,16 @@ void adjoint_backward(Solver& s, int nrec, const char* const* files, const float
     // segment buffer; this guard puts them back on every exit
     struct Live {
         Solver& s;
-        float* p[9];
+        float* p[15];
         explicit Live(Solver& s_) : s(s_) {
-            for (int i = 0; i < 3; i++) { p[i] = s.d.u[i]; p[3 + i] = s.d.v[i]; p[6 + i] = s.d.w1n[i]; }
+            for (int i = 0; i < 3; i++) {
+                p[i] = s.d.u[i]; p[3 + i] = s.d.v[i]; p[6 + i] = s.d.w1n[i]; p[9 + i] = s.d.ub[i]; p[12 + i] = s.d.vb[i];
+            }
         }
         void restore() {
-            for (int i = 0; i < 3; i++) { s.d.u[i] = p[i]; s.d.v[i] = p[3 + i]; s.d.w1n[i] = p[6 + i]; }
+            for (int i = 0; i < 3; i++) {
+                s.d.u[i] = p[i]; s.d.v[i] = p[3 + i]; s.d.w1n[i] = p[6 + i]; s.d.ub[i] = p[9 + i]; s.d.vb[i] = p[12 + i];
+            }
         }
         ~Live() { restore(); }
     } live(s);
@@ -575,26 +581,56 @@ void adjoint_backward(Solver& s, int nrec, const char* const* files, const float
     const int seg = A->seg;
     const int nseg = (s.nt + seg - 1) / seg;
     if (A->nck < (seg == 1 ? s.nt + 1 : nseg)) throw SordError(SORD_E_STATE, "adjoint: missing checkpoints");
+    // The adjoint steps run on their own stream, so that the recomputation of
+    // segment k - 1 (on the solver's stream, into the other segment buffer)
+    // overlaps the adjoint pass over segment k.
+    struct Streams {
+        cudaStream_t as = nullptr;
+        cudaEvent_t ev[5] = {};  // rec_done[2], adj_done[2], start
+        ~Streams() {
+            for (auto e : ev) if (e) cudaEventDestroy(e);
+            if (as) cudaStreamDestroy(as);
+        }
+    } S;
+    SORD_CUDA(cudaStreamCreateWithFlags(&S.as, cudaStreamNonBlocking));
+    for (auto& e : S.ev) SORD_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    cudaEvent_t* rec_done = S.ev;
+    cudaEvent_t* adj_done = S.ev + 2;
+    SORD_CUDA(cudaEventRecord(S.ev[4], s.stream));
+    SORD_CUDA(cudaStreamWaitEvent(S.as, S.ev[4], 0));
+    auto recompute = [&](int k) {
+        const int n0 = k * seg, n1 = std::min(s.nt, n0 + seg);
+        float* base = A->segbuf[k & 1];
+        // the buffer was last read by the adjoint pass over segment k + 2
+        SORD_CUDA(cudaStreamWaitEvent(s.stream, adj_done[k & 1], 0));
+        // from the checkpoint straight into the segment buffer: the leapfrog
+        // update of the first step reads the checkpoint, then each fused step
+        // runs on state n in place and writes u, v of step n + 1 into the
+        // next state (the folded update)
+        k_adj_advance<<<std::max(1LL, std::min((long long)(nv + 255) / 256, 148LL * 16)), 256, 0, s.stream>>>(
+            A->ckpt[k], base, (long long)nv, g.dt);
+        s.launches++;
+        for (int n = n0 + 1; n <= n1; n++) {
+            float* st = base + (size_t)(n - n0 - 1) * 9 * nv;
+            const bool fold = n < n1;
+            for (int i = 0; i < 3; i++) {
+                s.d.u[i] = st + i * nv; s.d.v[i] = st + (3 + i) * nv; s.d.w1n[i] = st + (6 + i) * nv;
+                if (fold) { s.d.ub[i] = st + (9 + i) * nv; s.d.vb[i] = st + (12 + i) * nv; }
+            }
+            bare_step(s, n, false, fold);
+        }
+        live.restore();
+        SORD_CUDA(cudaEventRecord(rec_done[k & 1], s.stream));
+    };
+    if (seg > 1) recompute(nseg - 1);
     for (int k = nseg - 1; k >= 0; k--) {
         const int n0 = k * seg, n1 = std::min(s.nt, n0 + seg);
         if (seg > 1) {
-            // recompute the segment from its checkpoint straight into the
-            // segment buffer: the leapfrog update reads state n - 1 and
-            // writes state n, then the fused step runs on state n in place
-            const float* prev = A->ckpt[k];
-            for (int n = n0 + 1; n <= n1; n++) {
-                float* st = A->segbuf + (size_t)(n - n0 - 1) * 9 * nv;
-                k_adj_advance<<<std::max(1LL, std::min((long long)(nv + 255) / 256, 148LL * 16)), 256, 0, s.stream>>>(
-                    prev, st, (long long)nv, g.dt);
-                for (int i = 0; i < 3; i++) { s.d.u[i] = st + i * nv; s.d.v[i] = st + (3 + i) * nv; s.d.w1n[i] = st + (6 + i) * nv; }
-                bare_step(s, n, false);
-                s.launches++;
-                prev = st;
-            }
-            live.restore();
+            if (k > 0) recompute(k - 1);
+            SORD_CUDA(cudaStreamWaitEvent(S.as, rec_done[k & 1], 0));
         }
         for (int n = n1; n >= n0 + 1; n--) {
-            const float* st = seg > 1 ? A->segbuf + (size_t)(n - n0 - 1) * 9 * nv : A->ckpt[n];
+            const float* st = seg > 1 ? A->segbuf[k & 1] + (size_t)(n - n0 - 1) * 9 * nv : A->ckpt[n];
             for (int i = 0; i < 3; i++) {
                 K.u[i] = st + i * nv; K.v[i] = st + (3 + i) * nv; K.a[i] = st + (6 + i) * nv;
                 K.ubi[i] = A->ub[cur][i]; K.vbi[i] = A->vb[cur][i];
@@ -602,17 +638,21 @@ void adjoint_backward(Solver& s, int nrec, const char* const* files, const float
             }
             // moment sources of step n
             const int nme = moff[n + 1] - moff[n];
-            if (nme > 0) k_adj_moment<<<1, 128, 0, s.stream>>>(K, A->mom + moff[n], nme, A->gmom);
-            k_adj_step<<<agrid, dim3(AJ, AK), kAdjSmem, s.stream>>>(K);
+            if (nme > 0) k_adj_moment<<<1, 128, 0, S.as>>>(K, A->mom + moff[n], nme, A->gmom);
+            k_adj_step<<<agrid, dim3(AJ, AK), kAdjSmem, S.as>>>(K);
             cur = 1 - cur;
             if (A->nrecv) {
                 Ptr3 pu{{A->ub[cur][0], A->ub[cur][1], A->ub[cur][2]}}, pv{{A->vb[cur][0], A->vb[cur][1], A->vb[cur][2]}};
-                k_adj_recv<<<std::max(1, (A->nrecv + 255) / 256), 256, 0, s.stream>>>(A->recv, A->nrecv, n, A->trace, pu, pv);
+                k_adj_recv<<<std::max(1, (A->nrecv + 255) / 256), 256, 0, S.as>>>(A->recv, A->nrecv, n, A->trace, pu, pv);
             }
             s.launches += 1 + (nme > 0 ? 1 : 0) + (A->nrecv ? 1 : 0);
             SORD_CUDA(cudaGetLastError());
         }
+        SORD_CUDA(cudaEventRecord(adj_done[k & 1], S.as));
     }
+    // join the adjoint stream back into the solver's
+    SORD_CUDA(cudaEventRecord(S.ev[4], S.as));
+    SORD_CUDA(cudaStreamWaitEvent(s.stream, S.ev[4], 0));
     s.it = s.nt;
     SORD_CUDA(cudaEventRecord(s.ev1, s.stream));
     SORD_CUDA(cudaEventSynchronize(s.ev1));

@@ -205,11 +205,12 @@ static InjectList upload(Solver& s, int slot, const std::vector<Inject>& e) {
 
 // One forward step n with no field-I/O hook: leapfrog update (unless the
 // caller has done it), then the fused stress/force/acceleration step with
-// the point sources of step n, unfolded, so that u, v and w1n = a are the
-// state after step n.  The
+// the point sources of step n, so that u, v and w1n = a are the state after
+// step n; folded, the step also writes u, v of step n + 1 into ub, vb (which
+// launch_fused then swaps in).  The
 // adjoint recomputes checkpointed segments with it; every step of such a run
 // is fusable, and the arithmetic is that of Solver::step.
-void bare_step(Solver& s, int n, bool update) {
+void bare_step(Solver& s, int n, bool update, bool fold) {
     s.it = n;
     s.tm = s.prm.tm0 + s.g.dt * (float)(n - 1);
     if (update) launch_time_update(s, false);
@@ -217,8 +218,8 @@ void bare_step(Solver& s, int n, bool update) {
     tensor_point_ops(s, kPot, pot);
     tensor_point_ops(s, kMom, mom);
     InjectList lp = upload(s, 0, pot), lm = upload(s, 1, mom), lf = upload(s, 2, frc);
-    launch_fused(s, lp, lm, lf, pot, mom, frc, false, true, false);
-    s.folded = false;
+    launch_fused(s, lp, lm, lf, pot, mom, frc, fold, true, false);
+    s.folded = fold;
 }
 
 // Injection entries of '.' moment op opi at step s.it (none if it does not fire).
