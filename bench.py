@@ -16,6 +16,12 @@ every input resident in HBM; `e2e` is the same metric for the user call
 (staged files on the host -> setup -> K steps -> outputs written); the
 reference arm (--impl reference) runs the CPU oracle, the restatement of the
 Fortran solver, on a bounded sample of the same workload.
+
+The interior step kernel runs in fast arithmetic by default (--arithmetic
+fast: fused multiply-adds and fewer operations, relative L2 error ~1e-6
+against the FP64 oracle, tested to <= 1e-4); the same handle then times the
+reference-order kernel (bit-identical to the FP32 oracle), reported as
+`reference_order`.
 """
 import argparse
 import json
@@ -287,6 +293,9 @@ def run_adjoint_bench(device, nt=1200):
         d = os.path.join(work, 'fwd')
         p.stage(rho, vp, vs, m, d)
         s = _lib.Solver(d, open(os.path.join(d, 'sord.in')).read(), device=device)
+        # the adjoint kernels transpose the reference-order step; forward and
+        # recomputation use that arithmetic here, so the ratio compares like with like
+        s.set_arithmetic('reference')
         s.step(nt)
         t_fwd = s.last_step_ms()
         s.close()
@@ -295,6 +304,7 @@ def run_adjoint_bench(device, nt=1200):
             d = os.path.join(work, tag)
             p.stage(rho, vp, vs, m, d)
             s = _lib.Solver(d, open(os.path.join(d, 'sord.in')).read(), device=device)
+            s.set_arithmetic('reference')
             try:
                 s.adjoint_forward(seg)
                 t_af = s.last_step_ms()
@@ -309,7 +319,8 @@ def run_adjoint_bench(device, nt=1200):
             res[tag] = {'ratio': (t_af + t_b) / t_fwd, 'adjoint_forward_ms': t_af, 'backward_ms': t_b,
                         'segment': seg, 'finite_gradients': ok}
         return {'metric': 'adjoint gradient cost / forward', 'value': res['checkpointed']['ratio'], 'unit': 'x',
-                'higher_is_better': False, 'forward_ms': t_fwd, 'checkpointed': res['checkpointed'],
+                'higher_is_better': False, 'forward_ms': t_fwd, 'arithmetic': 'reference',
+                'checkpointed': res['checkpointed'],
                 'stored': res['stored'],
                 'workload': 'adjoint: 128^3 nodes, %d steps, seeded 10%% blob in rho/vp/vs, 32 receivers, '
                             'moment tensor with 2 Hz Ricker, free surfaces' % nt}
@@ -481,6 +492,8 @@ def run_ours(args):
     from coseis_b200 import build as cb
     cb.build()
     from coseis_b200 import _lib
+    # read by every handle this process creates (timed run, e2e, ensemble, adjoint)
+    os.environ['SORD_ARITHMETIC'] = args.arithmetic
     ws, rank, local, pg = dist_init()
     shape = tuple(args.shape)
     nodes = float(np.prod(shape))
@@ -489,7 +502,10 @@ def run_ours(args):
         make_inputs(shape, inputs, hill=args.hill)
     barrier(pg)
     prof_steps = 6
-    nt = args.warmup + args.steps + prof_steps
+    # with fast arithmetic the same handle then times the reference-order
+    # kernel too (2 warm-up steps + the same number of timed steps)
+    other = args.arithmetic == 'fast' and not args.no_reference_order
+    nt = args.warmup + args.steps + prof_steps + ((2 + args.steps) if other else 0)
     work = tempfile.mkdtemp(prefix='sord_bench_%d_' % rank)
     try:
         text = stage_in(wave_prm(shape, nt), work, inputs)
@@ -512,6 +528,14 @@ def run_ours(args):
         s.step(prof_steps)
         kt = s.kernel_times()
         s.set_profiling(False)
+        ref_order = None
+        if other:
+            s.set_arithmetic('reference')
+            s.step(2)
+            barrier(pg)
+            s.step(args.steps)
+            r_ms = reduce_max(pg, s.last_step_ms())
+            ref_order = {'ms_per_step': r_ms / args.steps, 'value': job_rate(ws, nodes, args.steps, r_ms)}
         s.close()
         e2e = None
         if not args.no_e2e:
@@ -547,6 +571,7 @@ def run_ours(args):
         'config': {'workload': 'wave226: %dx%dx%d nodes curvilinear terrain, layered von Karman medium, '
                                '12-node PML on 5 faces, moment-tensor source, 64 receivers' % shape,
                    'nodes': int(nodes), 'dx_m': DX, 'dt_s': DT, 'parallelism': 'replicas' if ws > 1 else 'single',
+                   'arithmetic': args.arithmetic,
                    'l2': 'inputs larger than L2 (%.1f GB resident)' % (nodes * 100 / 1e9),
                    'setup_s': round(setup_s, 2), 'host_wall_s': round(wall, 4)},
         'roofline': {'bound': 'hbm', 'kernel': kernel, 'launch_ms': launch_ms,
@@ -555,6 +580,7 @@ def run_ours(args):
                      'algorithmic_bytes_per_launch': alg * nodes,
                      'traffic': (tr * nodes if tr else None)},
         'kernels_ms_per_step': {k: v[0] / prof_steps for k, v in kt.items() if v[1]},
+        'reference_order': ref_order,
         'gpu_launches': int(launches),
         'clocks': clocks,
         'e2e': e2e,
@@ -622,6 +648,7 @@ def run_ensemble_bench(n, nthreads, device, nt=ENS_NT, seed=SEED):
                 'one_at_a_time': n / t_ser, 'speedup': t_ser / t_ens, 'scenarios': n,
                 'concurrent': nthreads, 'steps': nt, 'wall_s': round(t_ens, 3), 'serial_wall_s': round(t_ser, 3),
                 'node_updates_per_s': float(sum(nodes)) * nt / t_ens, 'outputs_identical': bool(same),
+                'arithmetic': os.environ.get('SORD_ARITHMETIC', 'reference'),
                 'workload': 'rupture ensemble: seeded grids 64x64x64..192x96x96, dx 100 m, dt 0.008 s, '
                             'slip-weakening +z fault, seeded friction / stresses (scenarios 0..%d)' % (n - 1)}
     finally:
@@ -666,6 +693,10 @@ def main():
     ap.add_argument('--ensemble-threads', type=int, default=8)
     ap.add_argument('--adjoint-steps', type=int, default=1200, help='adjoint workload steps (0: skip)')
     ap.add_argument('--hill', type=float, default=500.0, help='topography peak (m); 0 gives a rectilinear mesh')
+    ap.add_argument('--arithmetic', choices=['reference', 'fast'], default='fast',
+                    help='interior step kernel arithmetic (sord_set_arithmetic)')
+    ap.add_argument('--no-reference-order', action='store_true',
+                    help='with --arithmetic fast, skip timing the reference-order kernel on the same handle')
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)

@@ -16,11 +16,15 @@ SYMBOLS = [
     'sord_kernel_launches', 'sord_set_profiling', 'sord_kernel_times',
     'sord_last_error', 'sord_error_string', 'sord_destroy',
     'sord_vector_max_noalloc', 'sord_run_ensemble', 'sord_adjoint_forward', 'sord_adjoint_backward',
+    'sord_set_arithmetic', 'sord_get_arithmetic',
 ]
 
 # return codes (enum in include/sordgpu.h)
 SORD_OK, SORD_E_PARAM, SORD_E_CFL, SORD_E_NEGVOL, SORD_E_NANINF = 0, -1, -2, -3, -4
 SORD_E_IO, SORD_E_CUDA, SORD_E_STATE, SORD_E_NOMEM = -5, -6, -7, -8
+
+# sord_set_arithmetic modes
+ARITHMETIC = {'reference': 0, 'fast': 1}
 
 _lib = None
 
@@ -61,6 +65,10 @@ def load():
     lib.sord_kernel_launches.restype = ctypes.c_longlong
     lib.sord_set_profiling.argtypes = [P, ctypes.c_int]
     lib.sord_set_profiling.restype = ctypes.c_int
+    lib.sord_set_arithmetic.argtypes = [P, ctypes.c_int]
+    lib.sord_set_arithmetic.restype = ctypes.c_int
+    lib.sord_get_arithmetic.argtypes = [P]
+    lib.sord_get_arithmetic.restype = ctypes.c_int
     lib.sord_kernel_times.argtypes = [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
     lib.sord_kernel_times.restype = ctypes.c_int
     lib.sord_last_error.argtypes = [P]
@@ -189,6 +197,15 @@ class Solver(object):
 
     def last_step_ms(self):
         return load().sord_last_step_ms(self._h)
+
+    def set_arithmetic(self, mode):
+        """'reference' (bit-identical to the reference's FP32 arithmetic) or
+        'fast' (fused multiply-adds and fewer operations in the interior step
+        kernel; equal in exact arithmetic)."""
+        _check(load().sord_set_arithmetic(self._h, ARITHMETIC[mode]), self._h)
+
+    def arithmetic(self):
+        return {v: k for k, v in ARITHMETIC.items()}[load().sord_get_arithmetic(self._h)]
 
     def set_profiling(self, on=True):
         _check(load().sord_set_profiling(self._h, 1 if on else 0), self._h)

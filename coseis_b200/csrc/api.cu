@@ -828,6 +828,18 @@ int sord_set_profiling(sord_handle* h, int on) {
     return SORD_OK;
 }
 
+int sord_set_arithmetic(sord_handle* h, int mode) {
+    if (!h) return SORD_E_PARAM;
+    if (mode != 0 && mode != 1) {
+        h->s.err = "sord_set_arithmetic: mode must be 0 or 1";
+        return SORD_E_PARAM;
+    }
+    h->s.arith = mode;
+    return SORD_OK;
+}
+
+int sord_get_arithmetic(const sord_handle* h) { return h ? h->s.arith : SORD_E_PARAM; }
+
 int sord_kernel_times(sord_handle* h, double* ms, long long* count, int n) {
     if (!h) return SORD_E_PARAM;
     try {

@@ -111,6 +111,7 @@ __device__ __forceinline__ float fmaxn(float m, float c) { return (c != c || c >
 // fault keeps its force: the rupture step adds the fault traction to it,
 // divides by the mass and, when the step is folded, advances its v and u;
 // the fold copies its v and u into the new buffers.
+template <bool FM = false>
 __device__ __forceinline__ void finish_node(const StepArgs& A, long long q, int jn, int kn, int l, float (&f)[3],
                                             float m, const float (&uv)[6], float dt, float& st_a, float& st_v,
                                             float& st_u) {
@@ -143,9 +144,15 @@ __device__ __forceinline__ void finish_node(const StepArgs& A, long long q, int 
         for (int i = 0; i < 3; i++) A.aout[i][q] = f[i];
     if (A.fold) {
         float a, b;
-        a = v0 + dt * f[0]; b = u0 + dt * a; A.vout[0][q] = a; A.uout[0][q] = b;
-        a = v1 + dt * f[1]; b = u1 + dt * a; A.vout[1][q] = a; A.uout[1][q] = b;
-        a = v2 + dt * f[2]; b = u2 + dt * a; A.vout[2][q] = a; A.uout[2][q] = b;
+        if (FM) {
+            a = fmaf(dt, f[0], v0); b = fmaf(dt, a, u0); A.vout[0][q] = a; A.uout[0][q] = b;
+            a = fmaf(dt, f[1], v1); b = fmaf(dt, a, u1); A.vout[1][q] = a; A.uout[1][q] = b;
+            a = fmaf(dt, f[2], v2); b = fmaf(dt, a, u2); A.vout[2][q] = a; A.uout[2][q] = b;
+        } else {
+            a = v0 + dt * f[0]; b = u0 + dt * a; A.vout[0][q] = a; A.uout[0][q] = b;
+            a = v1 + dt * f[1]; b = u1 + dt * a; A.vout[1][q] = a; A.uout[1][q] = b;
+            a = v2 + dt * f[2]; b = u2 + dt * a; A.vout[2][q] = a; A.uout[2][q] = b;
+        }
     }
 }
 
@@ -694,7 +701,11 @@ __global__ void __launch_bounds__(SJ * SK, GEOM == GEOM_GENERAL ? 1 : 2) k_shell
 
 // Interior kernel: tiles of 31 x 7 nodes from (A.jf, A.kf), planes A.lf0..A.lf1,
 // strictly inside the non-PML region, with no PML or boundary terms.
-template <int GEOM, bool FASTK>
+// FM (fast arithmetic): fused multiply-adds, brackets scaled by h once per
+// cell, divergence brackets taken as the negated gradient brackets and, on
+// terrain meshes, the closed-form brackets of stencil.cuh; equal to the
+// reference-order kernel in exact arithmetic, not bit for bit.
+template <int GEOM, bool FASTK, bool FM>
 __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(StepArgs A) {
     using L = Lay<GEOM>;
     constexpr int NGN = L::NGN, NGC = L::NGC, NDIR = L::NDIR;
@@ -726,6 +737,8 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
         tya = A.y1d[K - 1];
         tyb = A.y1d[K];
     }
+    // fast arithmetic on terrain meshes: the bracket spacings times h
+    const float hdx = h * (txb - txa), hdy = h * (tyb - tya);
 
     // point injections that fall inside this block (cells / nodes it computes)
     __shared__ Inject lpot[kLocalInject], lmom[kLocalInject], lfrc[kLocalInject];
@@ -783,8 +796,8 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
 #pragma unroll
                 for (int c = 0; c < 3; c++) {
                     const float u = RAW(c, n), v = RAW(3 + c, n);
-                    w[c] = u + gm * v;
-                    hh[c] = A.hg1 * u + A.dh2 * v;
+                    w[c] = FM ? fmaf(gm, v, u) : u + gm * v;
+                    hh[c] = FM ? fmaf(A.dh2, v, A.hg1 * u) : A.hg1 * u + A.dh2 * v;
                 }
                 const float c0 = L::NCOORD > 0 ? RAW(7, n) : 0.f;
                 const float c1 = L::NCOORD > 1 ? RAW(8, n) : 0.f;
@@ -875,7 +888,32 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
         // support-operator brackets; directions 0 and 1 in the two lanes
         float B[3][8];
         float cnb[NDIR > 0 ? NDIR : 1][8];
-        if (GEOM == GEOM_RECT) {
+        if constexpr (FM) {
+            // brackets scaled by h; divergence brackets = negated gradient brackets
+            if (GEOM == GEOM_RECT) {
+#pragma unroll
+                for (int a = 0; a < 3; a++)
+#pragma unroll
+                    for (int t = 0; t < 8; t++) B[a][t] = A.brh.bnc[a][t];
+            } else if (GEOM == GEOM_TERRAIN) {
+                terrain_brackets_0(hdy, X2, B[0]);
+                terrain_brackets_1(hdx, X2, B[1]);
+#pragma unroll
+                for (int t = 0; t < 8; t++) B[2][t] = A.brh.bnc[2][t];
+            } else {
+                brackets_nc_g<float>(X1, X2, B[0]);
+                brackets_nc_g<float>(X2, X0, B[1]);
+                brackets_nc_g<float>(X0, X1, B[2]);
+#pragma unroll
+                for (int a = 0; a < 3; a++)
+#pragma unroll
+                    for (int t = 0; t < 8; t++) B[a][t] = h * B[a][t];
+            }
+#pragma unroll
+            for (int a = 0; a < NDIR; a++)
+#pragma unroll
+                for (int t = 0; t < 8; t++) cnb[a][t] = -B[a][cn_of_nc(t)];
+        } else if (GEOM == GEOM_RECT) {
 #pragma unroll
             for (int a = 0; a < 3; a++)
 #pragma unroll
@@ -920,7 +958,24 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
 #pragma unroll
         for (int i = 0; i < 12; i++) he[i] = 0.f;
         const bool own = owncol && l >= L0;
-        if constexpr (F && !kPaired) {
+        if constexpr (F && FM) {
+            // gradients; the off-diagonal pairs are summed here and halved
+            // with the modulus below
+            float sg[3][3];
+#pragma unroll
+            for (int ic = 0; ic < 3; ic++) {
+                float W[8];
+#pragma unroll
+                for (int t = 0; t < 8; t++) W[t] = Wc[ic][term_corner(t)];
+#pragma unroll
+                for (int id = 0; id < 3; id++) sg[ic][id] = dot8(W, B[id]);
+            }
+#pragma unroll
+            for (int i = 0; i < 3; i++) ed[i] = sg[i][i];
+            eo[0] = sg[1][2] + sg[2][1];
+            eo[1] = sg[0][2] + sg[2][0];
+            eo[2] = sg[0][1] + sg[1][0];
+        } else if constexpr (F && !kPaired) {
 #pragma unroll
             for (int ic = 0; ic < 3; ic++) {
                 float W[8];
@@ -1054,17 +1109,25 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
             }
             apply_inject(lpot, npot, A.pot, q, ed, eo);
         }
-        {
-            const float lm = cur[0], m2 = 2.0f * cur[1];
-            const float s1v = lm * (ed[0] + ed[1] + ed[2]);
+        if constexpr (FM) {
+            // (2 mu e + lam tr e) / V; the off-diagonal sums carry the 1/2
+            const float r = cur[2], mur = cur[1] * r, m2r = mur + mur;
+            const float s1r = (cur[0] * r) * (ed[0] + ed[1] + ed[2]);
 #pragma unroll
-            for (int i = 0; i < 3; i++) { ed[i] = m2 * ed[i] + s1v; eo[i] = m2 * eo[i]; }
-        }
-        if constexpr (!F) apply_inject(lmom, nmom, A.mom, q, ed, eo);
-        {
-            const float r = cur[2];
+            for (int i = 0; i < 3; i++) { ed[i] = fmaf(m2r, ed[i], s1r); eo[i] = mur * eo[i]; }
+        } else {
+            {
+                const float lm = cur[0], m2 = 2.0f * cur[1];
+                const float s1v = lm * (ed[0] + ed[1] + ed[2]);
 #pragma unroll
-            for (int i = 0; i < 3; i++) { ed[i] = ed[i] * r; eo[i] = eo[i] * r; }
+                for (int i = 0; i < 3; i++) { ed[i] = m2 * ed[i] + s1v; eo[i] = m2 * eo[i]; }
+            }
+            if constexpr (!F) apply_inject(lmom, nmom, A.mom, q, ed, eo);
+            {
+                const float r = cur[2];
+#pragma unroll
+                for (int i = 0; i < 3; i++) { ed[i] = ed[i] * r; eo[i] = eo[i] * r; }
+            }
         }
         if (A.stats && own)
             st_w = fmaxn(st_w, (ed[0] * ed[0] + ed[1] * ed[1] + ed[2] * ed[2]) + 2.0f * (eo[0] * eo[0] + eo[1] * eo[1] + eo[2] * eo[2]));
@@ -1141,11 +1204,26 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
             if (NDIR == 3) Bc[2][t] = reinterpret_cast<const float*>(cp + (9 + t / 4) * NCL)[t % 4];
             if (GEOM == GEOM_RECT)
 #pragma unroll
-                for (int id = 0; id < 3; id++) Bc[id][t] = A.br.bcn[id][t];
-            if (GEOM == GEOM_TERRAIN) Bc[2][t] = A.br.bcn[2][t];
+                for (int id = 0; id < 3; id++) Bc[id][t] = FM ? A.brh.bcn[id][t] : A.br.bcn[id][t];
+            if (GEOM == GEOM_TERRAIN) Bc[2][t] = FM ? A.brh.bcn[2][t] : A.br.bcn[2][t];
         }
         float f[3];
-        if constexpr (F && !kPaired) {
+        if constexpr (F && FM) {
+            // one fused multiply-add chain per component over its 24 terms
+#pragma unroll
+            for (int ic = 0; ic < 3; ic++) {
+                float acc = S[ic][0] * Bc[ic][0];
+#pragma unroll
+                for (int t = 1; t < 8; t++) acc = fmaf(S[ic][t], Bc[ic][t], acc);
+#pragma unroll
+                for (int iid = 1; iid < 3; iid++) {
+                    const int id = (ic + iid) % 3, comp = 3 + (3 - ic - id);
+#pragma unroll
+                    for (int t = 0; t < 8; t++) acc = fmaf(S[comp][t], Bc[id][t], acc);
+                }
+                f[ic] = acc;
+            }
+        } else if constexpr (F && !kPaired) {
 #pragma unroll
             for (int ic = 0; ic < 3; ic++)
 #pragma unroll
@@ -1359,7 +1437,77 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
                     else f[2] = f[2] + inc;
                 }
         }
-        finish_node(A, q, jn, kn, l, f, cur[4], uv, dt, st_a, st_v, st_u);
+        finish_node<FM>(A, q, jn, kn, l, f, cur[4], uv, dt, st_a, st_v, st_u);
+    };
+
+    // ------------------------------------------------- node phase, fast arithmetic
+    // Each cell plane is read once: at node plane l a thread takes the four
+    // cells of plane l around its node column, adds their terms to node l
+    // (cells above it) and keeps their terms for node l + 1 (cells below it)
+    // in fc for the next plane.
+    float fc[3] = {0.f, 0.f, 0.f};
+    auto hg_term = [](int c) {  // hourglass term t with hg_corner(t) == c
+        int r = 0;
+#pragma unroll
+        for (int t = 0; t < 8; t++)
+            if (hg_corner(t) == c) r = t;
+        return r;
+    };
+    auto nodes_fm = [&](int l, bool finish) {
+        if (!outcol) return;
+        const float4* c1 = sC + (l & 1) * (NGC * NCL) + tid;
+        float fu[3] = {fc[0], fc[1], fc[2]}, fl[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int cj = q & 1, ck = q >> 1;
+            const float4* cp = c1 + cj + FJ * ck;
+            const float4 a = cp[0], b = cp[NCL], g2 = cp[2 * NCL], g3 = cp[3 * NCL], g4 = cp[4 * NCL];
+            const float S[6] = {a.x, a.y, a.z, a.w, b.x, b.y};
+            const float H[4][3] = {{b.z, b.w, g3.z}, {g2.x, g2.y, g3.w}, {g2.z, g2.w, g4.x}, {g3.x, g3.y, g4.y}};
+            // diff_cn terms of this cell for node l (above it: cl = 1) and node l + 1 (cl = 0)
+            const int tu = cj + 2 + 4 * ck, tl = cj + 4 * ck;
+            float Bu[3], Bl[3];
+            if constexpr (NDIR >= 2) {
+                const float4 xu = cp[(6 + 2 * ck) * NCL], xl = cp[(5 + 2 * ck) * NCL];
+                Bu[0] = cj ? xu.z : xu.x;
+                Bu[1] = cj ? xu.w : xu.y;
+                Bl[0] = cj ? xl.z : xl.x;
+                Bl[1] = cj ? xl.w : xl.y;
+            }
+            if constexpr (NDIR == 3) {
+                const float4 x2 = cp[(9 + ck) * NCL];
+                Bu[2] = cj ? x2.w : x2.z;
+                Bl[2] = cj ? x2.y : x2.x;
+            }
+#pragma unroll
+            for (int id = NDIR; id < 3; id++) {
+                Bu[id] = A.brh.bcn[id][tu];
+                Bl[id] = A.brh.bcn[id][tl];
+            }
+#pragma unroll
+            for (int ic = 0; ic < 3; ic++)
+#pragma unroll
+                for (int iid = 0; iid < 3; iid++) {
+                    const int id = (ic + iid) % 3, comp = ic == id ? ic : 3 + (3 - ic - id);
+                    fu[ic] = fmaf(S[comp], Bu[id], fu[ic]);
+                    fl[ic] = fmaf(S[comp], Bl[id], fl[ic]);
+                }
+            // hourglass_cn: f - sum over the node's cells of -+ H by the sign of
+            // the cell's term (cell position p is hourglass term hg_term(7 - p))
+            if (A.hourglass) {
+                const int hu = hg_term(7 - (q + 4)), hl = hg_term(7 - q);
+#pragma unroll
+                for (int iq = 0; iq < 4; iq++)
+#pragma unroll
+                    for (int ic = 0; ic < 3; ic++) {
+                        fu[ic] = hg_neg(iq, hu) ? fu[ic] + H[iq][ic] : fu[ic] - H[iq][ic];
+                        fl[ic] = hg_neg(iq, hl) ? fl[ic] + H[iq][ic] : fl[ic] - H[iq][ic];
+                    }
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 3; i++) fc[i] = fl[i];
+        if (finish) finish_node<FM>(A, g.idx(jn, kn, l), jn, kn, l, fu, cur[4], uv, dt, st_a, st_v, st_u);
     };
 
     // ---------------------------------------------------------------- stream
@@ -1377,6 +1525,10 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
     stat_load(L0 - 1, cur);
     uv_load(L0, uv);
     cells(L0 - 1, path);
+    if constexpr (FM) {
+        __syncthreads();  // cell plane L0-1 complete: its terms for node L0
+        nodes_fm(L0 - 1, false);
+    }
     stat_load(L0, cur);
 #pragma unroll 1
     for (int l = L0; l <= L1; l++) {
@@ -1386,7 +1538,8 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
         cp_async_wait_all();
         __syncthreads();  // cell plane l complete, staged plane l+2 landed
         store((l + 2) % 3);
-        nodes(l, path);
+        if constexpr (FM) nodes_fm(l, true);
+        else nodes(l, path);
         uv_load(l + 1, nuv);
         __syncthreads();  // ring slot l+2 complete, staging and cell slot l-1 free
         fetch(l + 3);
@@ -1559,10 +1712,16 @@ static void source_tiles(const Solver& s, const FusedPlan& P, const std::vector<
 template <int GEOM, bool FASTK>
 static void launch_mode(Solver& s, const StepArgs& A, dim3 grid, cudaStream_t st) {
     const size_t bytes = FASTK ? Lay<GEOM>::bytes : LayS<GEOM, (SJ + 1) * (SK + 1), SJ * SK>::bytes;
-    if (FASTK) smem_limit((const void*)k_interior<GEOM, true>, (int)bytes);
-    else smem_limit((const void*)k_shell<GEOM>, (int)bytes);
-    if (FASTK) k_interior<GEOM, true><<<grid, dim3(FJ, FK), bytes, st>>>(A);
-    else k_shell<GEOM><<<grid, dim3(SJ, SK), bytes, st>>>(A);
+    if (FASTK && s.arith) {
+        smem_limit((const void*)k_interior<GEOM, true, true>, (int)bytes);
+        k_interior<GEOM, true, true><<<grid, dim3(FJ, FK), bytes, st>>>(A);
+    } else if (FASTK) {
+        smem_limit((const void*)k_interior<GEOM, true, false>, (int)bytes);
+        k_interior<GEOM, true, false><<<grid, dim3(FJ, FK), bytes, st>>>(A);
+    } else {
+        smem_limit((const void*)k_shell<GEOM>, (int)bytes);
+        k_shell<GEOM><<<grid, dim3(SJ, SK), bytes, st>>>(A);
+    }
     s.launches++;
     SORD_CUDA(cudaGetLastError());
 }
@@ -1582,6 +1741,11 @@ void launch_fused(Solver& s, const InjectList& pot, const InjectList& mom, const
     StepArgs A;
     A.g = s.g;
     A.br = s.br;
+    for (int a = 0; a < 3; a++)
+        for (int t = 0; t < 8; t++) {
+            A.brh.bnc[a][t] = s.g.h * s.br.bnc[a][t];
+            A.brh.bcn[a][t] = s.g.h * s.br.bcn[a][t];
+        }
     A.x1d = d.x1d;
     A.y1d = d.y1d;
     for (int i = 0; i < 3; i++) {

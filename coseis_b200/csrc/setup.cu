@@ -357,6 +357,8 @@ static void allocate_arrays(Solver& s) {
     for (int i = 0; i < 3; i++) { alloc(s, &d.vb[i], nv); alloc(s, &d.ub[i], nv); }
     const char* fz = getenv("SORD_FUSED");
     s.use_fused = !(fz && fz[0] == '0');
+    const char* ar = getenv("SORD_ARITHMETIC");
+    s.arith = (ar && std::strcmp(ar, "fast") == 0) ? 1 : 0;
     SORD_CUDA(dev_malloc(s, (void**)&d.inj, sizeof(Inject) * kInjectSlots * kInjectRing * kMaxInject));
     s.hinj = (Inject*)pinned_get(sizeof(Inject) * kInjectSlots * kInjectRing * kMaxInject);
 }

@@ -128,6 +128,7 @@ enum { GEOM_RECT = 0, GEOM_TERRAIN = 1, GEOM_GENERAL = 2 };
 struct StepArgs {
     Geom g;
     Brackets br;
+    Brackets brh;      // br scaled by h (fast arithmetic)
     const float* x1d;  // terrain: x at nodes j = 1..nm0
     const float* y1d;  // terrain: y at nodes k = 1..nm1
     const float* x[3];
@@ -257,6 +258,7 @@ struct Solver {
     bool rect = false;        // rectilinear fast path verified
     int geom = GEOM_GENERAL;  // mesh class of the fused kernel
     bool use_fused = true;    // fused step kernel allowed (SORD_FUSED=0 disables)
+    int arith = 0;            // interior step arithmetic: 0 reference order, 1 fast (SORD_ARITHMETIC=fast)
     bool folded = false;      // previous step already applied this step's leapfrog update
     std::string workdir;
     int device = 0;

@@ -5,6 +5,8 @@
 // separately, exactly like the reference's (and the oracle's) FP32 code.
 #pragma once
 
+#include <math.h>
+
 #ifdef __CUDACC__
 #define SORD_HD __host__ __device__ __forceinline__
 #else
@@ -182,6 +184,59 @@ SORD_HD void cell_cn_brackets_g(const T* xb, const T* xc, const T nc[8], T cn[8]
 }
 SORD_HD void cell_cn_brackets(const float (*X)[8], int a, const float nc[8], float cn[8]) {
     cell_cn_brackets_g<float>(X[(a + 1) % 3], X[(a + 2) % 3], nc, cn, 0.0f);
+}
+
+// ---------------------------------------------------------------------------
+// Fast arithmetic: the same operators with fused multiply-adds and fewer
+// operations, equal to the reference's values in exact arithmetic (not bit
+// for bit; the rounding differs).
+//
+// In exact arithmetic every divergence bracket of a cell is the negated
+// gradient bracket of the same cell and corner: cn[t] = -nc[cn_of_nc(t)]
+// (the support operators are adjoint, diff_cn_op.f90 / diff_nc_op.f90).
+SORD_HD int cn_of_nc(int t) { return (int)((0x01452376u >> (4 * t)) & 0xFu); }
+
+// On a terrain mesh x depends on j only and y on k only, so the diff_nc
+// brackets (diff_nc_op.f90:19-70) of the two z-dependent directions reduce
+// to one spacing times small integer combinations of the corner z values
+// (corner n = dj + 2 dk + 4 dl).  Direction 0 (xb = y, xc = z), s = dy:
+//   B0 = s (2 (z1 - z4) + (z3 - z6)), B2 = s ((z1 - z4) + 2 (z3 - z6)),
+//   B1 = s (2 (z5 - z0) + (z7 - z2)), B3 = s ((z5 - z0) + 2 (z7 - z2)),
+//   B4 = -B1, B5 = -B0, B6 = -B2, B7 = -B3.
+// Direction 1 (xb = z, xc = x), s = dx:
+//   B0 = s (2 (z2 - z4) + (z3 - z5)), B1 = s ((z2 - z4) + 2 (z3 - z5)),
+//   B2 = s (2 (z6 - z0) + (z7 - z1)), B3 = s ((z6 - z0) + 2 (z7 - z1)),
+//   B4 = -B2, B5 = -B3, B6 = -B1, B7 = -B0.
+// s carries any common factor (the kernels pass h dy and h dx).
+SORD_HD void terrain_brackets_0(float s, const float z[8], float B[8]) {
+    const float a = z[1] - z[4], b = z[3] - z[6], c = z[5] - z[0], d = z[7] - z[2];
+    B[0] = s * fmaf(2.0f, a, b);
+    B[1] = s * fmaf(2.0f, c, d);
+    B[2] = s * fmaf(2.0f, b, a);
+    B[3] = s * fmaf(2.0f, d, c);
+    B[4] = -B[1];
+    B[5] = -B[0];
+    B[6] = -B[2];
+    B[7] = -B[3];
+}
+SORD_HD void terrain_brackets_1(float s, const float z[8], float B[8]) {
+    const float a = z[2] - z[4], b = z[3] - z[5], c = z[6] - z[0], d = z[7] - z[1];
+    B[0] = s * fmaf(2.0f, a, b);
+    B[1] = s * fmaf(2.0f, b, a);
+    B[2] = s * fmaf(2.0f, c, d);
+    B[3] = s * fmaf(2.0f, d, c);
+    B[4] = -B[2];
+    B[5] = -B[3];
+    B[6] = -B[1];
+    B[7] = -B[0];
+}
+
+// F . B with fused multiply-adds (B already scaled by h).
+SORD_HD float dot8(const float F[8], const float B[8]) {
+    float d = F[0] * B[0];
+#pragma unroll
+    for (int t = 1; t < 8; t++) d = fmaf(F[t], B[t], d);
+    return d;
 }
 
 }  // namespace sordgpu

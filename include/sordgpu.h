@@ -115,6 +115,22 @@ int sord_stats(const sord_handle* h, double* out, int n);
  * handle's stream, step kernels and I/O hooks included). */
 double sord_last_step_ms(const sord_handle* h);
 
+/* Arithmetic of the interior fused step kernel (no reference counterpart).
+ * Mode 0 (the default): every operation of the reference in its order and
+ * without fused multiply-adds, so outputs are bit-identical to a serial FP32
+ * build of the reference's arithmetic (sord/diff_nc_op.f90, diff_cn_op.f90,
+ * stress.f90, acceleration.f90, time_integration.f90).  Mode 1 (fast): fused
+ * multiply-adds, the support-operator brackets scaled by h once per cell,
+ * each divergence bracket taken as the negated gradient bracket of the same
+ * cell and corner, and on terrain meshes (x = x(j), y = y(k)) the closed
+ * form of the two z-dependent bracket sets; equal to mode 0 in exact
+ * arithmetic, FP32 rounding apart.  The PML shell, fault, source and
+ * separate-kernel paths keep mode 0.  New handles start in mode 1 when the
+ * environment variable SORD_ARITHMETIC is "fast".  May be called between any
+ * two steps.  sord_get_arithmetic returns the mode. */
+int sord_set_arithmetic(sord_handle* h, int mode);
+int sord_get_arithmetic(const sord_handle* h);
+
 /* Per-kernel device timing for performance reports.  With profiling on,
  * CUDA events are recorded around each step kernel on the handle's stream
  * and accumulated per class: 0 time update, 1 stress, 2 acceleration,

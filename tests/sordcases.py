@@ -296,19 +296,22 @@ def run_oracle(path, exe, threads=4):
     return json.loads(r.stdout.strip().splitlines()[-1])
 
 
-def run_gpu(path, fused=True):
-    """Run the CUDA solver through the C ABI; SORD_FUSED (read when a handle
-    is created) selects the fused step kernel or the per-stage kernels."""
+def run_gpu(path, fused=True, arithmetic='reference'):
+    """Run the CUDA solver through the C ABI; SORD_FUSED and SORD_ARITHMETIC
+    (read when a handle is created) select the fused step kernel or the
+    per-stage kernels, and the interior kernel's arithmetic."""
     from coseis_b200 import _lib
-    old = os.environ.get('SORD_FUSED')
-    os.environ['SORD_FUSED'] = '1' if fused else '0'
+    env = {'SORD_FUSED': '1' if fused else '0', 'SORD_ARITHMETIC': arithmetic}
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
     try:
         _lib.run_directory(path)
     finally:
-        if old is None:
-            del os.environ['SORD_FUSED']
-        else:
-            os.environ['SORD_FUSED'] = old
+        for k, v in old.items():
+            if v is None:
+                del os.environ[k]
+            else:
+                os.environ[k] = v
 
 
 def outputs(path):

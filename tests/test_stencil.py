@@ -15,3 +15,18 @@ def test_cell_cn_brackets_match_diff_cn(tmp_path):
     tot, bad = map(int, out.stdout.split())
     assert tot == 20000 * 24
     assert bad == 0, out.stdout
+
+
+def test_fast_brackets_match_reference_forms(tmp_path):
+    """The fast-arithmetic interior kernel (sord_set_arithmetic mode 1) uses
+    closed-form terrain brackets and the negated gradient brackets as
+    divergence brackets: both equal the reference's forms to rounding."""
+    exe = str(tmp_path / 'fast')
+    subprocess.check_call(['g++', '-std=c++17', '-O2', '-ffp-contract=off', '-o', exe,
+                           os.path.join(HERE, 'fast_brackets.cpp')])
+    out = subprocess.run([exe, '20000'], capture_output=True, text=True, check=True)
+    eterr, ecn = map(float, out.stdout.split())
+    # FP32 closed form against the double reference form: a few ulp
+    assert eterr < 1e-6, eterr
+    # the identity holds in exact arithmetic; double rounding only
+    assert ecn < 1e-12, ecn
