@@ -71,6 +71,7 @@ struct AdjointState {
 struct AdjArgs {
     Geom g;
     Brackets br;
+    Brackets brh;                     // br scaled by h
     const float *u[3], *v[3], *a[3];  // forward state of step n
     const float *ubi[3], *vbi[3];     // adjoint state of step n + 1
     float *ubo[3], *vbo[3];           // adjoint state of step n
@@ -104,7 +105,9 @@ __device__ __forceinline__ float fbar(const AdjArgs& A, long long q, bool act, i
 // are written by the block that owns the cell (tx, ty >= 1), node gradients
 // and the adjoint state by the owner of the node; the adjoint state is
 // double-buffered (in: step n + 1, out: step n) because neighbouring blocks
-// read the in-state of their halo nodes.
+// read the in-state of their halo nodes.  The transposed operators use fused
+// multiply-adds with the brackets scaled by h: the gradients are those of
+// the reference-order forward step to FP32 rounding.
 constexpr int AJ = 32, AK = 8, ANJ = AJ + 1, ANK = AK + 1, ANP = ANJ * ANK, ANC = AJ * AK;
 constexpr int ARF = 17, ACF = 18;  // raw floats per node, cell floats
 // raw node fields
@@ -116,7 +119,7 @@ __global__ void __launch_bounds__(AJ * AK, 2) k_adj_step(AdjArgs A) {
     float* sR = sm;                     // [slot][field][node]
     float* sC = sm + 3 * ARF * ANP;     // [slot][field][cell]
     const Geom& g = A.g;
-    const float h = g.h, dt = A.dt;
+    const float dt = A.dt;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + AJ * ty;
     const int bx = blockIdx.x % A.nbx, by = blockIdx.x / A.nbx;
     const int j0 = g.i1node[0] + bx * (AJ - 1), k0 = g.i1node[1] + by * (AK - 1);
@@ -170,9 +173,9 @@ __global__ void __launch_bounds__(AJ * AK, 2) k_adj_step(AdjArgs A) {
 #pragma unroll
             for (int i = 0; i < 3; i++) {
                 const float uu = b[(RU + i) * ANP], vv = b[(RV + i) * ANP];
-                cw[i][n] = uu + gm * vv;
-                ch[i][n] = A.hg1 * uu + A.dh2 * vv;
-                cf[i][n] = act ? mm * (dt * (b[(RVB + i) * ANP] + dt * b[(RUB + i) * ANP])) : 0.f;
+                cw[i][n] = fmaf(gm, vv, uu);
+                ch[i][n] = fmaf(A.dh2, vv, A.hg1 * uu);
+                cf[i][n] = act ? mm * (dt * fmaf(dt, b[(RUB + i) * ANP], b[(RVB + i) * ANP])) : 0.f;
             }
         }
         // forward strain (stress.f90:251-282)
@@ -183,7 +186,7 @@ __global__ void __launch_bounds__(AJ * AK, 2) k_adj_step(AdjArgs A) {
 #pragma unroll
             for (int t = 0; t < 8; t++) W[t] = cw[ic][term_corner(t)];
 #pragma unroll
-            for (int id = 0; id < 3; id++) G[ic][id] = stencil8(W, A.br.bnc[id], h);
+            for (int id = 0; id < 3; id++) G[ic][id] = dot8(W, A.brh.bnc[id]);
         }
         float ed[3], eo[3];
 #pragma unroll
@@ -202,10 +205,10 @@ __global__ void __launch_bounds__(AJ * AK, 2) k_adj_step(AdjArgs A) {
         }
         float sd[3], so[3];
 #pragma unroll
-        for (int i = 0; i < 3; i++) sd[i] = stencil8(F[i], A.br.bcn[i], h) * r;
-        so[0] = (stencil8(F[1], A.br.bcn[2], h) + stencil8(F[2], A.br.bcn[1], h)) * r;
-        so[1] = (stencil8(F[0], A.br.bcn[2], h) + stencil8(F[2], A.br.bcn[0], h)) * r;
-        so[2] = (stencil8(F[0], A.br.bcn[1], h) + stencil8(F[1], A.br.bcn[0], h)) * r;
+        for (int i = 0; i < 3; i++) sd[i] = dot8(F[i], A.brh.bcn[i]) * r;
+        so[0] = (dot8(F[1], A.brh.bcn[2]) + dot8(F[2], A.brh.bcn[1])) * r;
+        so[1] = (dot8(F[0], A.brh.bcn[2]) + dot8(F[2], A.brh.bcn[0])) * r;
+        so[2] = (dot8(F[0], A.brh.bcn[1]) + dot8(F[1], A.brh.bcn[0])) * r;
         // Hooke's law transposed
         const float tr = ed[0] + ed[1] + ed[2], st = sd[0] + sd[1] + sd[2];
 #pragma unroll
@@ -262,7 +265,7 @@ __global__ void __launch_bounds__(AJ * AK, 2) k_adj_step(AdjArgs A) {
 #pragma unroll
                 for (int id = 0; id < 3; id++) {
                     const int comp = ic == id ? ic : 3 + (3 - ic - id);
-                    wb[ic] = wb[ic] + h * A.br.bnc[id][t] * Gb[comp];
+                    wb[ic] = fmaf(A.brh.bnc[id][t], Gb[comp], wb[ic]);
                 }
         }
         if (A.hourglass) {
@@ -540,6 +543,11 @@ void adjoint_backward(Solver& s, int nrec, const char* const* files, const float
     AdjArgs K;
     K.g = g;
     K.br = s.br;
+    for (int a = 0; a < 3; a++)
+        for (int t = 0; t < 8; t++) {
+            K.brh.bnc[a][t] = s.g.h * s.br.bnc[a][t];
+            K.brh.bcn[a][t] = s.g.h * s.br.bcn[a][t];
+        }
     K.lam = s.d.lam; K.mu = s.d.mu; K.yy = s.d.yy; K.vc = s.d.vc; K.mr = s.d.mr; K.gam = s.d.gam;
     K.glam = A->glam; K.gmu = A->gmu; K.gyy = A->gyy; K.gmr = A->gmr;
     K.hg1 = s.prm.hourglass[0];

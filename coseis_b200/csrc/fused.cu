@@ -185,7 +185,8 @@ struct LayS {
 // at most 15 x 15 nodes), with every PML, boundary and point-source term of
 // the step.
 constexpr int SJ = 16, SK = 16;  // shell tile (cells = threads)
-template <int GEOM>
+// FM: the fast arithmetic of k_interior for the support-operator sums.
+template <int GEOM, bool FM>
 __global__ void __launch_bounds__(SJ * SK, GEOM == GEOM_GENERAL ? 1 : 2) k_shell(StepArgs A) {
     constexpr int FJ = SJ, FK = SK, FNJ = FJ + 1, FNK = FK + 1, FOJ = FJ - 1, FOK = FK - 1;
     constexpr int NPL = FNJ * FNK, NCL = FJ * FK, NTH = FJ * FK;
@@ -219,6 +220,7 @@ __global__ void __launch_bounds__(SJ * SK, GEOM == GEOM_GENERAL ? 1 : 2) k_shell
         tya = A.y1d[K - 1];
         tyb = A.y1d[K];
     }
+    const float hdx = h * (txb - txa), hdy = h * (tyb - tya);
 
     // point injections that fall inside this block (cells / nodes it computes)
     __shared__ Inject lpot[kLocalInject], lmom[kLocalInject], lfrc[kLocalInject];
@@ -274,8 +276,8 @@ __global__ void __launch_bounds__(SJ * SK, GEOM == GEOM_GENERAL ? 1 : 2) k_shell
 #pragma unroll
                 for (int c = 0; c < 3; c++) {
                     const float u = RAW(c, n), v = RAW(3 + c, n);
-                    NODE(slot, c, n) = u + gm * v;
-                    NODE(slot, L::HG + c, n) = A.hg1 * u + A.dh2 * v;
+                    NODE(slot, c, n) = FM ? fmaf(gm, v, u) : u + gm * v;
+                    NODE(slot, L::HG + c, n) = FM ? fmaf(A.dh2, v, A.hg1 * u) : A.hg1 * u + A.dh2 * v;
                 }
 #pragma unroll
                 for (int f = 0; f < L::NCOORD; f++) NODE(slot, L::CO + f, n) = RAW(7 + f, n);
@@ -332,7 +334,31 @@ __global__ void __launch_bounds__(SJ * SK, GEOM == GEOM_GENERAL ? 1 : 2) k_shell
 #pragma unroll
                 for (int a = 0; a < 3; a++)
 #pragma unroll
-                    for (int t = 0; t < 8; t++) B[a][t] = A.br.bnc[a][t];
+                    for (int t = 0; t < 8; t++) B[a][t] = FM ? A.brh.bnc[a][t] : A.br.bnc[a][t];
+            } else if constexpr (FM) {
+                // brackets scaled by h; divergence brackets = negated gradient brackets
+                float X[3][8];
+#pragma unroll
+                for (int n = 0; n < 8; n++)
+#pragma unroll
+                    for (int c = 0; c < L::NCOORD; c++) X[3 - L::NCOORD + c][n] = NODE(ns[n], L::CO + c, ni[n]);
+                if (GEOM == GEOM_TERRAIN) {
+                    terrain_brackets_0(hdy, X[2], B[0]);
+                    terrain_brackets_1(hdx, X[2], B[1]);
+#pragma unroll
+                    for (int t = 0; t < 8; t++) B[2][t] = A.brh.bnc[2][t];
+                } else {
+#pragma unroll
+                    for (int a = 0; a < 3; a++) {
+                        brackets_nc(X, a, B[a]);
+#pragma unroll
+                        for (int t = 0; t < 8; t++) B[a][t] = h * B[a][t];
+                    }
+                }
+#pragma unroll
+                for (int a = 0; a < L::NDIR; a++)
+#pragma unroll
+                    for (int t = 0; t < 8; t++) cnb[a][t] = -B[a][cn_of_nc(t)];
             } else {
                 float X[3][8];
                 if (GEOM == GEOM_TERRAIN) {
@@ -429,7 +455,7 @@ __global__ void __launch_bounds__(SJ * SK, GEOM == GEOM_GENERAL ? 1 : 2) k_shell
                         const int id = (ic + iid + 1) % 3;
                         float s;
                         if (nearS[id] || farS[id]) {
-                            const float raw = stencil8(V, B[id], h);
+                            const float raw = FM ? dot8(V, B[id]) : stencil8(V, B[id], h);
                             s = raw;
                             const int c = cc[id];
                             if (nearS[id]) {
@@ -445,9 +471,9 @@ __global__ void __launch_bounds__(SJ * SK, GEOM == GEOM_GENERAL ? 1 : 2) k_shell
                                 if (own) A.gout[3 + id][gi] = s;
                             }
                         } else if (anyS) {
-                            s = stencil8(U, B[id], h);
+                            s = FM ? dot8(U, B[id]) : stencil8(U, B[id], h);
                         } else {
-                            s = stencil8(W, B[id], h);
+                            s = FM ? dot8(W, B[id]) : stencil8(W, B[id], h);
                         }
                         if (ic == id) ed[ic] = s;
                         else if (ic < id) eo[3 - ic - id] = 0.5f * s;
@@ -533,10 +559,10 @@ __global__ void __launch_bounds__(SJ * SK, GEOM == GEOM_GENERAL ? 1 : 2) k_shell
 #pragma unroll
                 for (int t = 0; t < 8; t++) {
                     Fv[t] = CELL(cs[t], comp, ci[t]);
-                    if (GEOM == GEOM_RECT || (GEOM == GEOM_TERRAIN && id == 2)) B[t] = A.br.bcn[id][t];
+                    if (GEOM == GEOM_RECT || (GEOM == GEOM_TERRAIN && id == 2)) B[t] = FM ? A.brh.bcn[id][t] : A.br.bcn[id][t];
                     else B[t] = CELL(cs[t], 18 + 8 * id + t, ci[t]);
                 }
-                float s = stencil8(Fv, B, h);
+                float s = FM ? dot8(Fv, B) : stencil8(Fv, B, h);
                 if constexpr (!F) {
                     const int c = id == 0 ? jn : id == 1 ? kn : l;
                     if (c <= g.i1pml[id]) {
@@ -652,7 +678,7 @@ __global__ void __launch_bounds__(SJ * SK, GEOM == GEOM_GENERAL ? 1 : 2) k_shell
                     else f[2] = f[2] + inc;
                 }
         }
-        finish_node(A, q, jn, kn, l, f, cur[4], uv, dt, st_a, st_v, st_u);
+        finish_node<FM>(A, q, jn, kn, l, f, cur[4], uv, dt, st_a, st_v, st_u);
     };
 
     // ---------------------------------------------------------------- stream
@@ -842,10 +868,18 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
         cw_[2 * NCL] = make_float4(he[3], he[4], he[6], he[7]);                                            \
         cw_[3 * NCL] = make_float4(he[9], he[10], he[2], he[5]);                                           \
         cw_[4 * NCL] = make_float4(he[8], he[11], 0.f, 0.f);                                               \
-        if (NDIR >= 2)                                                                                     \
+        if (NDIR >= 2 && FM)                                                                               \
+            _Pragma("unroll") for (int q2 = 0; q2 < 4; q2++) {                                             \
+                const int tu_ = (q2 & 1) + 2 + 4 * (q2 >> 1), tl_ = (q2 & 1) + 4 * (q2 >> 1);               \
+                cw_[(5 + q2) * NCL] = make_float4(cnb[0][tu_], cnb[1][tu_], cnb[0][tl_], cnb[1][tl_]);      \
+            }                                                                                              \
+        else if (NDIR >= 2)                                                                                \
             _Pragma("unroll") for (int q2 = 0; q2 < 4; q2++) cw_[(5 + q2) * NCL] =                         \
                 make_float4(cnb[0][2 * q2], cnb[1][2 * q2], cnb[0][2 * q2 + 1], cnb[1][2 * q2 + 1]);        \
-        if (NDIR == 3) {                                                                                   \
+        if (NDIR == 3 && FM) {                                                                             \
+            cw_[9 * NCL] = make_float4(cnb[NDIR - 1][2], cnb[NDIR - 1][0], cnb[NDIR - 1][3], cnb[NDIR - 1][1]); \
+            cw_[10 * NCL] = make_float4(cnb[NDIR - 1][6], cnb[NDIR - 1][4], cnb[NDIR - 1][7], cnb[NDIR - 1][5]); \
+        } else if (NDIR == 3) {                                                                            \
             cw_[9 * NCL] = make_float4(cnb[NDIR - 1][0], cnb[NDIR - 1][1], cnb[NDIR - 1][2], cnb[NDIR - 1][3]); \
             cw_[10 * NCL] = make_float4(cnb[NDIR - 1][4], cnb[NDIR - 1][5], cnb[NDIR - 1][6], cnb[NDIR - 1][7]); \
         }                                                                                                  \
@@ -1467,17 +1501,18 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
             // diff_cn terms of this cell for node l (above it: cl = 1) and node l + 1 (cl = 0)
             const int tu = cj + 2 + 4 * ck, tl = cj + 4 * ck;
             float Bu[3], Bl[3];
+            // the cell keeps the brackets of each of its four node columns together
             if constexpr (NDIR >= 2) {
-                const float4 xu = cp[(6 + 2 * ck) * NCL], xl = cp[(5 + 2 * ck) * NCL];
-                Bu[0] = cj ? xu.z : xu.x;
-                Bu[1] = cj ? xu.w : xu.y;
-                Bl[0] = cj ? xl.z : xl.x;
-                Bl[1] = cj ? xl.w : xl.y;
+                const float4 xb = cp[(5 + q) * NCL];
+                Bu[0] = xb.x;
+                Bu[1] = xb.y;
+                Bl[0] = xb.z;
+                Bl[1] = xb.w;
             }
             if constexpr (NDIR == 3) {
                 const float4 x2 = cp[(9 + ck) * NCL];
-                Bu[2] = cj ? x2.w : x2.z;
-                Bl[2] = cj ? x2.y : x2.x;
+                Bu[2] = cj ? x2.z : x2.x;
+                Bl[2] = cj ? x2.w : x2.y;
             }
 #pragma unroll
             for (int id = NDIR; id < 3; id++) {
@@ -1718,9 +1753,12 @@ static void launch_mode(Solver& s, const StepArgs& A, dim3 grid, cudaStream_t st
     } else if (FASTK) {
         smem_limit((const void*)k_interior<GEOM, true, false>, (int)bytes);
         k_interior<GEOM, true, false><<<grid, dim3(FJ, FK), bytes, st>>>(A);
+    } else if (s.arith) {
+        smem_limit((const void*)k_shell<GEOM, true>, (int)bytes);
+        k_shell<GEOM, true><<<grid, dim3(SJ, SK), bytes, st>>>(A);
     } else {
-        smem_limit((const void*)k_shell<GEOM>, (int)bytes);
-        k_shell<GEOM><<<grid, dim3(SJ, SK), bytes, st>>>(A);
+        smem_limit((const void*)k_shell<GEOM, false>, (int)bytes);
+        k_shell<GEOM, false><<<grid, dim3(SJ, SK), bytes, st>>>(A);
     }
     s.launches++;
     SORD_CUDA(cudaGetLastError());
