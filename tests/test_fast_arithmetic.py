@@ -37,6 +37,12 @@ def floor_of(path, f, dtype):
         if f.startswith(pre):
             return max([np.sqrt(np.mean(load(path, m, dtype) ** 2)) for m in mags
                         if os.path.exists(os.path.join(path, m))] + [0.0])
+    # volume and receiver components ('snap-vx', 'snap-vy', 'snap-vz'): the
+    # RMS of the largest component of the same output
+    if len(f) > 6 and f[-5] in 'xyz' and f[-6] in 'vua':
+        comps = [f[:-5] + c + '.bin' for c in 'xyz']
+        return max([np.sqrt(np.mean(load(path, m, dtype) ** 2)) for m in comps
+                    if os.path.exists(os.path.join(path, m))] + [0.0])
     return 0.0
 
 
