@@ -16,7 +16,11 @@ import sordcases as sc
 TOL_L2 = 1e-4
 # interior tiles on rectilinear, general and terrain meshes, all-free
 # boundaries, and a fault
-CASES = ['interior', 'interior_noise', 'interior_wave', 'free', 'fault_x']
+# and meshes without interior tiles (the shell kernel alone)
+CASES = ['interior', 'interior_noise', 'interior_wave', 'free', 'fault_x', 'fault_noise', 'explosion', 'visc',
+         'noise', 'wave']
+# cases whose output steps read stress (separate-kernel path there)
+MIXED = {'explosion'}
 
 
 def rel_l2(a, b, floor=0.0):
@@ -97,7 +101,7 @@ def test_fast_arithmetic_accuracy(name, tmp_path, oracle_bins, gpu_lib):
         assert e_fast <= max(10 * e_o32, 1e-6), (f, e_fast, e_o32)
         assert rel_l2(a, load(o32, f, '<f4'), fl) <= TOL_L2, f
     # the fast kernel ran: its outputs are not the reference-order ones
-    assert differs, 'fast arithmetic gave bit-identical outputs'
+    assert differs or name in MIXED, 'fast arithmetic gave bit-identical outputs'
     print(name, {f: ('%.2e' % e[0], '%.2e' % e[1]) for f, e in sorted(worst.items())})
     # statistics maxima within the same bound, or no worse than the FP32
     # oracle's by more than a small factor (the fault traction maxima are
