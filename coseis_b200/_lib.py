@@ -16,7 +16,7 @@ SYMBOLS = [
     'sord_kernel_launches', 'sord_set_profiling', 'sord_kernel_times',
     'sord_last_error', 'sord_error_string', 'sord_destroy',
     'sord_vector_max_noalloc', 'sord_run_ensemble', 'sord_adjoint_forward', 'sord_adjoint_backward',
-    'sord_set_arithmetic', 'sord_get_arithmetic',
+    'sord_set_arithmetic', 'sord_get_arithmetic', 'sord_trim_memory',
 ]
 
 # return codes (enum in include/sordgpu.h)
@@ -65,6 +65,8 @@ def load():
     lib.sord_kernel_launches.restype = ctypes.c_longlong
     lib.sord_set_profiling.argtypes = [P, ctypes.c_int]
     lib.sord_set_profiling.restype = ctypes.c_int
+    lib.sord_trim_memory.argtypes = [ctypes.c_int]
+    lib.sord_trim_memory.restype = ctypes.c_int
     lib.sord_set_arithmetic.argtypes = [P, ctypes.c_int]
     lib.sord_set_arithmetic.restype = ctypes.c_int
     lib.sord_get_arithmetic.argtypes = [P]
@@ -120,6 +122,12 @@ def run_ensemble(paths, device=0, nthreads=8):
     st = (ctypes.c_int * max(n, 1))()
     _check(lib.sord_run_ensemble(arr, n, device, nthreads, st))
     return list(st)[:n]
+
+
+def trim_memory(device=0):
+    """Wait for the device memory of destroyed handles to go back to the
+    driver (it is returned on a helper thread)."""
+    _check(load().sord_trim_memory(device))
 
 
 def run_directory(path, device=0):

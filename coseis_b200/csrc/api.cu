@@ -840,6 +840,19 @@ int sord_set_arithmetic(sord_handle* h, int mode) {
 
 int sord_get_arithmetic(const sord_handle* h) { return h ? h->s.arith : SORD_E_PARAM; }
 
+int sord_trim_memory(int device) {
+    try {
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n)
+            throw SordError(SORD_E_CUDA, "sord_trim_memory: no CUDA device " + std::to_string(device));
+        SORD_CUDA(cudaSetDevice(device));
+        mem_trim(device);
+    } catch (const std::exception& e) {
+        return fail(nullptr, e);
+    }
+    return SORD_OK;
+}
+
 int sord_kernel_times(sord_handle* h, double* ms, long long* count, int n) {
     if (!h) return SORD_E_PARAM;
     try {

@@ -335,6 +335,7 @@ void adjoint_backward(Solver& s, int nrec, const char* const* files, const float
                       float* glam, float* gmu, float* gyy, float* gmr, double* gmom, int nmom);
 void mem_attach(int device);
 void mem_detach(int device);
+void mem_trim(int device);
 cudaError_t dev_malloc(Solver& s, void** p, size_t bytes);
 void dev_free(Solver& s, void* p);
 void* pinned_get(size_t bytes);

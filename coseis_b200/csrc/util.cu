@@ -2,9 +2,11 @@
 // (utilities.f90:103-117), region reductions, vector/tensor norms
 // (utilities.f90:120-165) and rinvert (utilities.f90:40-49).
 #include <cstdint>
+#include <cstdlib>
 #include <map>
 #include <mutex>
 #include <set>
+#include <thread>
 #include <utility>
 
 #include "sord.cuh"
@@ -215,11 +217,29 @@ void smem_limit(const void* func, int bytes) {
 // handles that run concurrently (an ensemble) do not serialise each other's
 // setup and teardown.  While any handle is alive the pool keeps freed
 // memory for the next allocation; when the last one goes it is trimmed.
+// Returning tens of GB to the driver takes up to seconds, so the trim runs
+// on a helper thread and the destroying call returns at once; the next
+// handle created on that device, and the exit of the process (an atexit
+// handler, registered after the CUDA runtime's own and so run before it),
+// wait for it.
 static std::mutex g_mem_m;
-static std::map<int, int> g_live;  // device -> live handles
+static std::map<int, int> g_live;             // device -> live handles
+static std::map<int, std::thread> g_trim;     // device -> trim in progress
+
+static void trim_join_locked(int device) {
+    auto it = g_trim.find(device);
+    if (it != g_trim.end() && it->second.joinable()) it->second.join();
+}
+
+static void trim_join_all() {
+    std::lock_guard<std::mutex> lock(g_mem_m);
+    for (auto& t : g_trim)
+        if (t.second.joinable()) t.second.join();
+}
 
 void mem_attach(int device) {
     std::lock_guard<std::mutex> lock(g_mem_m);
+    trim_join_locked(device);
     if (g_live[device]++ == 0) {
         cudaMemPool_t pool;
         SORD_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
@@ -228,14 +248,32 @@ void mem_attach(int device) {
     }
 }
 
+// Wait for a pending trim on `device`; with no live handle there, return
+// the pool's unused memory to the driver now.
+void mem_trim(int device) {
+    std::lock_guard<std::mutex> lock(g_mem_m);
+    trim_join_locked(device);
+    if (g_live[device] == 0) {
+        cudaMemPool_t pool;
+        SORD_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+        SORD_CUDA(cudaMemPoolTrimTo(pool, 0));
+    }
+}
+
 void mem_detach(int device) {
+    static std::once_flag at_exit;
     std::lock_guard<std::mutex> lock(g_mem_m);
     if (--g_live[device] == 0) {
         cudaMemPool_t pool;
         if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
             uint64_t keep = 0;
             cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-            cudaMemPoolTrimTo(pool, 0);
+            std::call_once(at_exit, [] { std::atexit(trim_join_all); });
+            trim_join_locked(device);
+            g_trim[device] = std::thread([device, pool] {
+                cudaSetDevice(device);
+                cudaMemPoolTrimTo(pool, 0);
+            });
         }
     }
 }

@@ -97,6 +97,16 @@ int sord_adjoint_backward(sord_handle* h, int nrec, const char* const* files, co
                           const int* ntrace, float* grad_lam, float* grad_mu, float* grad_yy, float* grad_mr,
                           double* grad_moment, int nmoment);
 
+/* Device memory of the handles comes from the device's default memory
+ * pool; when the last handle on a device is destroyed the pool's memory is
+ * returned to the driver on a helper thread, so sord_destroy and
+ * sord_run_directory return without waiting for it.  sord_trim_memory
+ * waits for that, and with no live handle on `device` returns the pool's
+ * unused memory now: call it before allocating the memory elsewhere in the
+ * same process.  No reference counterpart (the reference frees its arrays
+ * at process exit). */
+int sord_trim_memory(int device);
+
 /* Copy a node or cell volume field to host memory (core region only, j
  * fastest; nn or nn-1 values per axis).  Names: vx vy vz ux uy uz ax ay az
  * (nodes; `a` holds the last acceleration) and lam mu yy vc (cells).

@@ -6,6 +6,8 @@ import os
 import re
 import subprocess
 
+import numpy as np
+
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -88,6 +90,41 @@ def test_no_device_fails_loudly(tmp_path):
         _lib.run_directory(str(tmp_path))
     assert e.value.code == -6
     assert not [f for f in os.listdir(str(tmp_path)) if f.startswith('stats-')]
+
+
+def test_trim_memory_without_device(lib):
+    """sord_trim_memory names the missing device instead of doing anything on the CPU."""
+    import torch
+    from coseis_b200 import _lib
+    if torch.cuda.is_available():
+        pytest.skip('a device is present')
+    assert lib.sord_trim_memory(0) == _lib.SORD_E_CUDA
+    assert b'no CUDA device 0' in lib.sord_last_error(None)
+    assert lib.sord_trim_memory(-1) == _lib.SORD_E_CUDA
+
+
+@pytest.mark.gpu
+def test_trim_memory_after_destroy(tmp_path, gpu_lib):
+    """Handles on one device one after another: each destroy starts the
+    return of the pool's memory on a helper thread; sord_trim_memory and the
+    next create wait for it, and the runs are unaffected."""
+    from coseis_b200 import _lib, sord
+    for i in range(3):
+        d = str(tmp_path / str(i))
+        os.makedirs(d)
+        cwd = os.getcwd()
+        os.chdir(d)
+        try:
+            sord.stage({'shape': [21, 21, 21, 4], 'npml': 4, 'bc1': ['pml'] * 3, 'bc2': ['pml'] * 3,
+                        'mxx': [([10, 10, 10, []], '.', 1e16, 'brune', 0.1)],
+                        'vx': [([[], 10, [], -1], '=>', 'vx.bin')]})
+        finally:
+            os.chdir(cwd)
+        _lib.run_directory(d)
+        if i == 1:
+            _lib.trim_memory(0)
+        assert np.abs(np.fromfile(os.path.join(d, 'vx.bin'), '<f4')).max() > 0
+    _lib.trim_memory(0)
 
 
 def test_noalloc_argument_checks(lib):
