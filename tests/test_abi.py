@@ -1,13 +1,13 @@
 """The C ABI library on a machine without a GPU: it loads, exports every
 symbol include/sordgpu.h declares, and fails loudly (an error code, no CPU
-fallback) when there is no device.  No compute is launched here."""
+fallback) when there is no device.  No compute is launched by the tests
+not marked gpu."""
 import ctypes
 import os
 import re
 import subprocess
 
 import numpy as np
-
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
