@@ -79,6 +79,13 @@ struct Lay {
     static constexpr int NDIR = GEOM == GEOM_RECT ? 0 : GEOM == GEOM_TERRAIN ? 2 : 3;
     static constexpr int NGC = GEOM == GEOM_RECT ? 5 : GEOM == GEOM_TERRAIN ? 9 : 11;  // float4 groups per cell
     static constexpr size_t bytes = sizeof(float) * (size_t)RAWSZ + sizeof(float4) * (size_t)(3 * NPL * NGN + 2 * NCL * NGC);
+    // fast arithmetic: one cell plane (each node plane reads only the cells
+    // above it); groups: (e11 e22 e33 e23), (e31 e12) as float2, then per
+    // reading node column q: its hourglass sums for the node above and
+    // below, and its divergence brackets (NQ groups)
+    static constexpr int NQ = NDIR >= 2 ? 3 : 2;
+    static constexpr int NGCF = 2 + 4 * NQ;
+    static constexpr size_t bytes_fm = sizeof(float) * (size_t)RAWSZ + sizeof(float4) * (size_t)(3 * NPL * NGN + NCL * NGCF);
 };
 // scalar field numbers of the node and cell groups
 __host__ __device__ constexpr int nf_co(int c) { return c == 0 ? 3 : c == 1 ? 7 : 8; }
@@ -738,7 +745,8 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
     extern __shared__ float4 sm4[];
     float* sR = reinterpret_cast<float*>(sm4);  // [RAWF][NPL] staged plane
     float4* sN = sm4 + L::RAWSZ / 4;            // [3 slots][NGN][NPL]
-    float4* sC = sN + 3 * NGN * NPL;            // [2 slots][NGC][NCL]
+    float4* sC = sN + 3 * NGN * NPL;            // [2 slots][NGC][NCL]; fast arithmetic [NGCF][NCL]
+    constexpr int NQ = L::NQ, NGCF = L::NGCF;
 #define RAW(f, i) sR[(f) * NPL + (i)]
     const Geom& g = A.g;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + FJ * ty;
@@ -868,18 +876,10 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
         cw_[2 * NCL] = make_float4(he[3], he[4], he[6], he[7]);                                            \
         cw_[3 * NCL] = make_float4(he[9], he[10], he[2], he[5]);                                           \
         cw_[4 * NCL] = make_float4(he[8], he[11], 0.f, 0.f);                                               \
-        if (NDIR >= 2 && FM)                                                                               \
-            _Pragma("unroll") for (int q2 = 0; q2 < 4; q2++) {                                             \
-                const int tu_ = (q2 & 1) + 2 + 4 * (q2 >> 1), tl_ = (q2 & 1) + 4 * (q2 >> 1);               \
-                cw_[(5 + q2) * NCL] = make_float4(cnb[0][tu_], cnb[1][tu_], cnb[0][tl_], cnb[1][tl_]);      \
-            }                                                                                              \
-        else if (NDIR >= 2)                                                                                \
+        if (NDIR >= 2)                                                                                     \
             _Pragma("unroll") for (int q2 = 0; q2 < 4; q2++) cw_[(5 + q2) * NCL] =                         \
                 make_float4(cnb[0][2 * q2], cnb[1][2 * q2], cnb[0][2 * q2 + 1], cnb[1][2 * q2 + 1]);        \
-        if (NDIR == 3 && FM) {                                                                             \
-            cw_[9 * NCL] = make_float4(cnb[NDIR - 1][2], cnb[NDIR - 1][0], cnb[NDIR - 1][3], cnb[NDIR - 1][1]); \
-            cw_[10 * NCL] = make_float4(cnb[NDIR - 1][6], cnb[NDIR - 1][4], cnb[NDIR - 1][7], cnb[NDIR - 1][5]); \
-        } else if (NDIR == 3) {                                                                            \
+        if (NDIR == 3) {                                                                                   \
             cw_[9 * NCL] = make_float4(cnb[NDIR - 1][0], cnb[NDIR - 1][1], cnb[NDIR - 1][2], cnb[NDIR - 1][3]); \
             cw_[10 * NCL] = make_float4(cnb[NDIR - 1][4], cnb[NDIR - 1][5], cnb[NDIR - 1][6], cnb[NDIR - 1][7]); \
         }                                                                                                  \
@@ -888,12 +888,12 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
     // ---------------------------------------------------------------- cell phase
     auto cells = [&](int l, auto fast_tag) {
         constexpr bool F = decltype(fast_tag)::value;
-        const int cs = l & 1;
+        const int cs = FM ? 0 : l & 1;
         const bool valid = (F || cellcol) && l >= g.i1cell[2] && l <= g.i2cell[2];
         if (!valid) {
             float4* cw = sC + cs * (NGC * NCL) + tid;
 #pragma unroll
-            for (int i = 0; i < NGC; i++) cw[i * NCL] = make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int i = 0; i < (FM ? NGCF : NGC); i++) cw[i * NCL] = make_float4(0.f, 0.f, 0.f, 0.f);
             return;
         }
         const long long q = g.idx(J, K, l);
@@ -1202,7 +1202,42 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
                 }
             }
         }
-        WRITE_CELL(cs, ed, eo, he, cnb);
+        if constexpr (FM) {
+            // fast layout: for each node column q that reads this cell, the
+            // hourglass sum it adds to the node above the cell (u) and below
+            // it (l) -- the signs of hourglass_cn terms hg_term(7 - p) at cell
+            // position p -- and its divergence brackets
+            float4* cw = sC + tid;
+            cw[0] = make_float4(ed[0], ed[1], ed[2], eo[0]);
+            reinterpret_cast<float2*>(sC + NCL)[tid] = make_float2(eo[1], eo[2]);
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int hu = hg_term(7 - (q + 4)), hl = hg_term(7 - q);
+                float yu[3], yl[3];
+#pragma unroll
+                for (int ic = 0; ic < 3; ic++) {
+                    yu[ic] = hg_neg(0, hu) ? he[ic] : -he[ic];
+                    yl[ic] = hg_neg(0, hl) ? he[ic] : -he[ic];
+#pragma unroll
+                    for (int iq = 1; iq < 4; iq++) {
+                        yu[ic] = hg_neg(iq, hu) ? yu[ic] + he[3 * iq + ic] : yu[ic] - he[3 * iq + ic];
+                        yl[ic] = hg_neg(iq, hl) ? yl[ic] + he[3 * iq + ic] : yl[ic] - he[3 * iq + ic];
+                    }
+                }
+                float4* cq = cw + (2 + NQ * q) * NCL;
+                cq[0] = make_float4(yu[0], yu[1], yu[2], yl[0]);
+                if constexpr (NDIR >= 2) {
+                    const int tu = (q & 1) + 2 + 4 * (q >> 1), tl = (q & 1) + 4 * (q >> 1);
+                    cq[NCL] = make_float4(yl[1], yl[2], cnb[0][tu], cnb[1][tu]);
+                    cq[2 * NCL] = make_float4(cnb[0][tl], cnb[1][tl], NDIR == 3 ? cnb[NDIR - 1][tu] : 0.f,
+                                              NDIR == 3 ? cnb[NDIR - 1][tl] : 0.f);
+                } else {
+                    cq[NCL] = make_float4(yl[1], yl[2], 0.f, 0.f);
+                }
+            }
+        } else {
+            WRITE_CELL(cs, ed, eo, he, cnb);
+        }
     };
 
     // ---------------------------------------------------------------- node phase
@@ -1480,39 +1515,31 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
     // (cells above it) and keeps their terms for node l + 1 (cells below it)
     // in fc for the next plane.
     float fc[3] = {0.f, 0.f, 0.f};
-    auto hg_term = [](int c) {  // hourglass term t with hg_corner(t) == c
-        int r = 0;
-#pragma unroll
-        for (int t = 0; t < 8; t++)
-            if (hg_corner(t) == c) r = t;
-        return r;
-    };
     auto nodes_fm = [&](int l, bool finish) {
         if (!outcol) return;
-        const float4* c1 = sC + (l & 1) * (NGC * NCL) + tid;
         float fu[3] = {fc[0], fc[1], fc[2]}, fl[3] = {0.f, 0.f, 0.f};
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             const int cj = q & 1, ck = q >> 1;
-            const float4* cp = c1 + cj + FJ * ck;
-            const float4 a = cp[0], b = cp[NCL], g2 = cp[2 * NCL], g3 = cp[3 * NCL], g4 = cp[4 * NCL];
-            const float S[6] = {a.x, a.y, a.z, a.w, b.x, b.y};
-            const float H[4][3] = {{b.z, b.w, g3.z}, {g2.x, g2.y, g3.w}, {g2.z, g2.w, g4.x}, {g3.x, g3.y, g4.y}};
+            const int ci = tid + cj + FJ * ck;  // the cell (J + cj, K + ck)
+            const float4 a = sC[ci];
+            const float2 e = reinterpret_cast<const float2*>(sC + NCL)[ci];
+            const float S[6] = {a.x, a.y, a.z, a.w, e.x, e.y};
+            const float4* cq = sC + (2 + NQ * q) * NCL + ci;
+            const float4 y0 = cq[0], y1 = cq[NCL];
             // diff_cn terms of this cell for node l (above it: cl = 1) and node l + 1 (cl = 0)
             const int tu = cj + 2 + 4 * ck, tl = cj + 4 * ck;
             float Bu[3], Bl[3];
-            // the cell keeps the brackets of each of its four node columns together
             if constexpr (NDIR >= 2) {
-                const float4 xb = cp[(5 + q) * NCL];
-                Bu[0] = xb.x;
-                Bu[1] = xb.y;
-                Bl[0] = xb.z;
-                Bl[1] = xb.w;
-            }
-            if constexpr (NDIR == 3) {
-                const float4 x2 = cp[(9 + ck) * NCL];
-                Bu[2] = cj ? x2.z : x2.x;
-                Bl[2] = cj ? x2.w : x2.y;
+                const float4 y2 = cq[2 * NCL];
+                Bu[0] = y1.z;
+                Bu[1] = y1.w;
+                Bl[0] = y2.x;
+                Bl[1] = y2.y;
+                if constexpr (NDIR == 3) {
+                    Bu[2] = y2.z;
+                    Bl[2] = y2.w;
+                }
             }
 #pragma unroll
             for (int id = NDIR; id < 3; id++) {
@@ -1527,17 +1554,14 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
                     fu[ic] = fmaf(S[comp], Bu[id], fu[ic]);
                     fl[ic] = fmaf(S[comp], Bl[id], fl[ic]);
                 }
-            // hourglass_cn: f - sum over the node's cells of -+ H by the sign of
-            // the cell's term (cell position p is hourglass term hg_term(7 - p))
+            // hourglass_cn: the cell's signed sums for the nodes above and below it
             if (A.hourglass) {
-                const int hu = hg_term(7 - (q + 4)), hl = hg_term(7 - q);
-#pragma unroll
-                for (int iq = 0; iq < 4; iq++)
-#pragma unroll
-                    for (int ic = 0; ic < 3; ic++) {
-                        fu[ic] = hg_neg(iq, hu) ? fu[ic] + H[iq][ic] : fu[ic] - H[iq][ic];
-                        fl[ic] = hg_neg(iq, hl) ? fl[ic] + H[iq][ic] : fl[ic] - H[iq][ic];
-                    }
+                fu[0] = fu[0] + y0.x;
+                fu[1] = fu[1] + y0.y;
+                fu[2] = fu[2] + y0.z;
+                fl[0] = fl[0] + y0.w;
+                fl[1] = fl[1] + y1.x;
+                fl[2] = fl[2] + y1.y;
             }
         }
 #pragma unroll
@@ -1563,6 +1587,7 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
     if constexpr (FM) {
         __syncthreads();  // cell plane L0-1 complete: its terms for node L0
         nodes_fm(L0 - 1, false);
+        __syncthreads();  // one cell slot: read before cells(L0) overwrites it
     }
     stat_load(L0, cur);
 #pragma unroll 1
@@ -1746,7 +1771,8 @@ static void source_tiles(const Solver& s, const FusedPlan& P, const std::vector<
 
 template <int GEOM, bool FASTK>
 static void launch_mode(Solver& s, const StepArgs& A, dim3 grid, cudaStream_t st) {
-    const size_t bytes = FASTK ? Lay<GEOM>::bytes : LayS<GEOM, (SJ + 1) * (SK + 1), SJ * SK>::bytes;
+    const size_t bytes = FASTK ? (s.arith ? Lay<GEOM>::bytes_fm : Lay<GEOM>::bytes)
+                               : LayS<GEOM, (SJ + 1) * (SK + 1), SJ * SK>::bytes;
     if (FASTK && s.arith) {
         smem_limit((const void*)k_interior<GEOM, true, true>, (int)bytes);
         k_interior<GEOM, true, true><<<grid, dim3(FJ, FK), bytes, st>>>(A);

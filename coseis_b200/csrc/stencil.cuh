@@ -123,6 +123,8 @@ SORD_HD T stencil8(const T F[8], const T B[8], T h) {
 // of hourglass_cn the cells at minus the same offsets.  hg_corner(t) is the
 // corner id of term t; hg_neg(iq, t) is 1 where term t is subtracted.
 SORD_HD int hg_corner(int t) { return (int)((0x43251670u >> (4 * t)) & 0xFu); }
+// the inverse: the hourglass term whose corner is c
+SORD_HD int hg_term(int c) { return (int)((0x12476530u >> (4 * c)) & 0xFu); }
 SORD_HD int hg_neg(int iq, int t) { return (int)(((0xAA3CCCF0u >> (8 * iq)) >> t) & 1u); }
 
 template <class T>

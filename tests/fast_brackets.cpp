@@ -4,7 +4,8 @@
 // diff_cn_op.f90), evaluated in double:
 //   * terrain cells (x = x(j), y = y(k)): terrain_brackets_0 / _1 against
 //     brackets_nc_g of directions 0 and 1;
-//   * general cells: -nc[cn_of_nc(t)] against the divergence brackets.
+//   * general cells: -nc[cn_of_nc(t)] against the divergence brackets;
+//   * hg_term, the inverse of hg_corner.
 // Prints the largest error relative to the largest bracket of each cell for
 // both checks.  Built and run by tests/test_stencil.py.
 #include <cmath>
@@ -56,6 +57,12 @@ int main(int argc, char** argv) {
             for (int t = 0; t < 8; t++) ecn = fmax(ecn, fabs(cn[t] + nc[cn_of_nc(t)]) / m);
         }
     }
+    // hg_term inverts hg_corner (the fast kernel finds a cell's hourglass term by its corner)
+    for (int t = 0; t < 8; t++)
+        if (hg_term(hg_corner(t)) != t) {
+            printf("hg_term(hg_corner(%d)) = %d\n", t, hg_term(hg_corner(t)));
+            return 1;
+        }
     printf("%.3e %.3e\n", eterr, ecn);
     return 0;
 }
