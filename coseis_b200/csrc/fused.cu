@@ -83,8 +83,9 @@ struct Lay {
     // above it); groups: (e11 e22 e33 e23), (e31 e12) as float2, then per
     // reading node column q: its hourglass sums for the node above and
     // below, and its divergence brackets (NQ groups)
-    static constexpr int NQ = NDIR >= 2 ? 3 : 2;
-    static constexpr int NGCF = 2 + 4 * NQ;
+    // (terrain: 2 groups per q, the lower-cell brackets of all q in 2 float2 groups)
+    static constexpr int NQ = NDIR == 3 ? 3 : 2;
+    static constexpr int NGCF = 2 + 4 * NQ + (NDIR == 2 ? 2 : 0);
     static constexpr size_t bytes_fm = sizeof(float) * (size_t)RAWSZ + sizeof(float4) * (size_t)(3 * NPL * NGN + NCL * NGCF);
 };
 // scalar field numbers of the node and cell groups
@@ -1226,11 +1227,14 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
                 }
                 float4* cq = cw + (2 + NQ * q) * NCL;
                 cq[0] = make_float4(yu[0], yu[1], yu[2], yl[0]);
-                if constexpr (NDIR >= 2) {
+                if constexpr (NDIR == 3) {
                     const int tu = (q & 1) + 2 + 4 * (q >> 1), tl = (q & 1) + 4 * (q >> 1);
                     cq[NCL] = make_float4(yl[1], yl[2], cnb[0][tu], cnb[1][tu]);
-                    cq[2 * NCL] = make_float4(cnb[0][tl], cnb[1][tl], NDIR == 3 ? cnb[NDIR - 1][tu] : 0.f,
-                                              NDIR == 3 ? cnb[NDIR - 1][tl] : 0.f);
+                    cq[2 * NCL] = make_float4(cnb[0][tl], cnb[1][tl], cnb[NDIR - 1][tu], cnb[NDIR - 1][tl]);
+                } else if constexpr (NDIR == 2) {
+                    const int tu = (q & 1) + 2 + 4 * (q >> 1), tl = (q & 1) + 4 * (q >> 1);
+                    cq[NCL] = make_float4(yl[1], yl[2], cnb[0][tu], cnb[1][tu]);
+                    reinterpret_cast<float2*>(sC + (2 + 4 * NQ) * NCL)[q * NCL + tid] = make_float2(cnb[0][tl], cnb[1][tl]);
                 } else {
                     cq[NCL] = make_float4(yl[1], yl[2], 0.f, 0.f);
                 }
@@ -1530,16 +1534,20 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
             // diff_cn terms of this cell for node l (above it: cl = 1) and node l + 1 (cl = 0)
             const int tu = cj + 2 + 4 * ck, tl = cj + 4 * ck;
             float Bu[3], Bl[3];
-            if constexpr (NDIR >= 2) {
+            if constexpr (NDIR == 3) {
                 const float4 y2 = cq[2 * NCL];
                 Bu[0] = y1.z;
                 Bu[1] = y1.w;
                 Bl[0] = y2.x;
                 Bl[1] = y2.y;
-                if constexpr (NDIR == 3) {
-                    Bu[2] = y2.z;
-                    Bl[2] = y2.w;
-                }
+                Bu[2] = y2.z;
+                Bl[2] = y2.w;
+            } else if constexpr (NDIR == 2) {
+                const float2 bl = reinterpret_cast<const float2*>(sC + (2 + 4 * NQ) * NCL)[q * NCL + ci];
+                Bu[0] = y1.z;
+                Bu[1] = y1.w;
+                Bl[0] = bl.x;
+                Bl[1] = bl.y;
             }
 #pragma unroll
             for (int id = NDIR; id < 3; id++) {
