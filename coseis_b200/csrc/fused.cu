@@ -1248,6 +1248,7 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
     // The eight cells of node (jn, kn, l) are cell positions p = cj + 2 ck + 4 cl
     // at (J + cj, K + ck, l - 1 + cl); diff_cn term t sits at position
     // pt(t), hourglass_cn term t at position ph(t).
+    // (reference order only; fast arithmetic uses nodes_fm below)
     auto nodes = [&](int l, auto fast_tag) {
         constexpr bool F = decltype(fast_tag)::value;
         if (!outcol) return;
@@ -1277,26 +1278,11 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
             if (NDIR == 3) Bc[2][t] = reinterpret_cast<const float*>(cp + (9 + t / 4) * NCL)[t % 4];
             if (GEOM == GEOM_RECT)
 #pragma unroll
-                for (int id = 0; id < 3; id++) Bc[id][t] = FM ? A.brh.bcn[id][t] : A.br.bcn[id][t];
-            if (GEOM == GEOM_TERRAIN) Bc[2][t] = FM ? A.brh.bcn[2][t] : A.br.bcn[2][t];
+                for (int id = 0; id < 3; id++) Bc[id][t] = A.br.bcn[id][t];
+            if (GEOM == GEOM_TERRAIN) Bc[2][t] = A.br.bcn[2][t];
         }
         float f[3];
-        if constexpr (F && FM) {
-            // one fused multiply-add chain per component over its 24 terms
-#pragma unroll
-            for (int ic = 0; ic < 3; ic++) {
-                float acc = S[ic][0] * Bc[ic][0];
-#pragma unroll
-                for (int t = 1; t < 8; t++) acc = fmaf(S[ic][t], Bc[ic][t], acc);
-#pragma unroll
-                for (int iid = 1; iid < 3; iid++) {
-                    const int id = (ic + iid) % 3, comp = 3 + (3 - ic - id);
-#pragma unroll
-                    for (int t = 0; t < 8; t++) acc = fmaf(S[comp][t], Bc[id][t], acc);
-                }
-                f[ic] = acc;
-            }
-        } else if constexpr (F && !kPaired) {
+        if constexpr (F && !kPaired) {
 #pragma unroll
             for (int ic = 0; ic < 3; ic++)
 #pragma unroll
