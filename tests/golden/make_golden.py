@@ -22,6 +22,16 @@ files.
 * srf.json -- a small synthetic SRF rupture read and written by the
   reference (cst/srf.py:13-194) and the fault geometry of its points
   (cst/coord.py:190-202 slip_vectors, 336-351 potency_tensor).
+* loh1_fk.npz -- the Prose frequency-wavenumber solution of the PEER
+  LOH.1 problem (layer over a half-space, buried double couple) shipped
+  with the reference as data/LOH1-ProseFK-{Time,V-Radial,V-Transverse,
+  V-Vertical}.npy, the traces scripts/PEER-LOH1-plot.py compares SORD
+  with (receiver 9, 10 km from the epicentre), copied unchanged (float32).
+* tpv3_bi.npz -- the boundary-integral solution of SCEC TPV3 shipped with
+  the reference as data/TPV3-BI-*.npy (time, slip, slip rate and shear
+  traction at the mode II station P1 and the mode III station P2, rupture
+  time on a 300 x 150 grid of 0.1 km cells), the traces
+  scripts/TPV3-plot.py compares SORD with, copied unchanged (float32).
 * frontend.json -- for several parameter sets, the sord.in text and the
   metadata (indices, shapes, deltas) that the reference front end produces:
   cst/sord.py:prepare (cst/sord.py:296-468) followed by the sord.in
@@ -264,6 +274,23 @@ def make_dsp(ref):
             'brune2gauss': d.brune2gauss(x, 0.01, 0.05).tolist()}
 
 
+def write_loh1(ref):
+    import numpy as np
+    names = {'t': 'Time', 'radial': 'V-Radial', 'transverse': 'V-Transverse', 'vertical': 'V-Vertical'}
+    arrs = {k: np.load(os.path.join(ref, 'data', 'LOH1-ProseFK-%s.npy' % v)) for k, v in names.items()}
+    np.savez_compressed(os.path.join(HERE, 'loh1_fk.npz'), **arrs)
+
+
+def write_tpv3(ref):
+    import numpy as np
+    names = {'t': 'P-Time', 'trup': 'Rupture-Time'}
+    for sta in ('P1', 'P2'):
+        for k, v in (('slip', 'Slip'), ('sv', 'Slip-Velocity'), ('ts', 'Traction')):
+            names['%s_%s' % (sta.lower(), k)] = '%s-%s' % (sta, v)
+    arrs = {k: np.load(os.path.join(ref, 'data', 'TPV3-BI-%s.npy' % v)) for k, v in names.items()}
+    np.savez_compressed(os.path.join(HERE, 'tpv3_bi.npz'), **arrs)
+
+
 def main():
     ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('COSEIS_REFERENCE', '')
     if not ref or not os.path.isdir(os.path.join(ref, 'cst')):
@@ -279,6 +306,8 @@ def main():
         json.dump(make_dsp(ref), fh, indent=1, sort_keys=True)
     with open(os.path.join(HERE, 'srf.json'), 'w') as fh:
         json.dump(make_srf(ref), fh, indent=1, sort_keys=True, default=lambda o: o.item())
+    write_loh1(ref)
+    write_tpv3(ref)
 
 
 if __name__ == '__main__':
