@@ -16,7 +16,7 @@ SYMBOLS = [
     'sord_kernel_launches', 'sord_set_profiling', 'sord_kernel_times',
     'sord_last_error', 'sord_error_string', 'sord_destroy',
     'sord_vector_max_noalloc', 'sord_run_ensemble', 'sord_adjoint_forward', 'sord_adjoint_backward',
-    'sord_set_arithmetic', 'sord_get_arithmetic', 'sord_trim_memory',
+    'sord_set_arithmetic', 'sord_get_arithmetic', 'sord_trim_memory', 'sord_adjoint_source_gradients',
 ]
 
 # return codes (enum in include/sordgpu.h)
@@ -88,6 +88,9 @@ def load():
     lib.sord_adjoint_backward.argtypes = [P, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(FP), IP,
                                           FP, FP, FP, FP, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
     lib.sord_adjoint_backward.restype = ctypes.c_int
+    DP = ctypes.POINTER(ctypes.c_double)
+    lib.sord_adjoint_source_gradients.argtypes = [P, DP, DP, ctypes.c_int]
+    lib.sord_adjoint_source_gradients.restype = ctypes.c_int
     lib.sord_vector_max_noalloc.argtypes = [P, P, P, IP, IP, IP, P, P]
     lib.sord_vector_max_noalloc.restype = ctypes.c_int
     _lib = lib
@@ -156,7 +159,9 @@ class Solver(object):
     def adjoint_backward(self, dtraces, nmoment):
         """dtraces: {receiver file name: dL/d(samples)}.  Returns a dict of
         numpy arrays: lam, mu, yy (real cells, shape (nx-1, ny-1, nz-1),
-        index [j, k, l]), mr (nodes, (nx, ny, nz)) and moment (nmoment)."""
+        index [j, k, l]), mr (nodes, (nx, ny, nz)), moment (nmoment), and
+        for each moment op position (nmoment, 3; per metre) and delay
+        (nmoment; per second of delay of its time function)."""
         import numpy as np
         nn, it, nt = self.info()
         files = list(dtraces)
@@ -176,6 +181,13 @@ class Solver(object):
                                             nmoment), self._h)
         res = {k: v.T for k, v in out.items()}
         res['moment'] = gm[:nmoment]
+        gx = np.zeros(3 * max(nmoment, 1), np.float64)
+        gt = np.zeros(max(nmoment, 1), np.float64)
+        DP = ctypes.POINTER(ctypes.c_double)
+        _check(load().sord_adjoint_source_gradients(self._h, gx.ctypes.data_as(DP), gt.ctypes.data_as(DP), nmoment),
+               self._h)
+        res['position'] = gx[:3 * nmoment].reshape(nmoment, 3)  # dL/dx of each moment op (per metre)
+        res['delay'] = gt[:nmoment]                             # dL/dt0 of each moment op (per second)
         return res
 
     def run(self):

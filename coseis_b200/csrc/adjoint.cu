@@ -62,7 +62,8 @@ struct AdjointState {
     int nrecv = 0;
     float* trace = nullptr;
     MomEntry* mom = nullptr;
-    double* gmom = nullptr;
+    double* gmom = nullptr;     // per moment op: value, delay, position x y z (5 slots each)
+    std::vector<double> gsrc;   // delay and position gradients of the last backward pass
     std::vector<int> recv_ops;  // op indices of '.>' receivers, recorded before the forward run
     std::vector<int> mom_ops;   // op indices of '.' moment ops
 };
@@ -518,9 +519,13 @@ void adjoint_backward(Solver& s, int nrec, const char* const* files, const float
     }
     A->trace = dalloc(s, tr.size());
     if (!tr.empty()) SORD_CUDA(cudaMemcpyAsync(A->trace, tr.data(), sizeof(float) * tr.size(), cudaMemcpyHostToDevice, s.stream));
-    SORD_CUDA(dev_malloc(s, (void**)&A->gmom, sizeof(double) * std::max(nmom, 1)));
-    SORD_CUDA(cudaMemsetAsync(A->gmom, 0, sizeof(double) * std::max(nmom, 1), s.stream));
-    // moment-source entries of every step, uploaded once: me[moff[n] .. moff[n+1])
+    // gradient slots: nmom values, then per op its delay and its x y z position
+    const int nslot = 5 * std::max(nmom, 1);
+    SORD_CUDA(dev_malloc(s, (void**)&A->gmom, sizeof(double) * nslot));
+    SORD_CUDA(cudaMemsetAsync(A->gmom, 0, sizeof(double) * nslot, s.stream));
+    // moment-source entries of every step, uploaded once: me[moff[n] .. moff[n+1]).
+    // An injection is val tf(t - t0) r(x1); d/d val = tf r, d/d t0 = -val tf' r,
+    // d/d x1 = val tf dr/dx1 (per metre: divided by the spacing).
     std::vector<MomEntry> me;
     std::vector<int> moff(s.nt + 2, 0);
     for (int n = 1; n <= s.nt; n++) {
@@ -528,11 +533,24 @@ void adjoint_backward(Solver& s, int nrec, const char* const* files, const float
         s.it = n;
         s.tm = s.prm.tm0 + g.dt * (float)(n - 1);
         for (size_t m = 0; m < A->mom_ops.size(); m++) {
-            const IoOp& io = s.ops[A->mom_ops[m]];
+            IoOp& io = s.ops[A->mom_ops[m]];
             std::vector<Inject> e;
             moment_entries(s, A->mom_ops[m], e);
+            if (e.empty()) continue;
             for (const Inject& x : e)
                 if (io.val != 0.f) me.push_back(MomEntry{x.idx, x.comp, (int)m, x.inc / io.val});
+            std::vector<PointWeight> pw;
+            FieldView cells{s.d.sd[0], {g.nm[0], g.nm[1], g.nm[2]}};
+            point_weights(s, io, cells, pw);
+            const double tf = host_time_function(io.fname, s.tm, g.dt, io.tau);
+            const double rate = host_time_function_rate(io.fname, (double)s.tm, (double)io.tau);
+            for (const PointWeight& w : pw) {
+                const int comp = e[0].comp;
+                me.push_back(MomEntry{w.idx, comp, nmom + (int)m, (float)(-(double)io.val * rate * w.r)});
+                for (int d = 0; d < 3; d++)
+                    me.push_back(MomEntry{w.idx, comp, 2 * nmom + 3 * (int)m + d,
+                                          (float)((double)io.val * tf * w.dr[d] / (double)s.prm.delta[d])});
+            }
         }
     }
     moff[s.nt + 1] = (int)me.size();
@@ -683,11 +701,27 @@ void adjoint_backward(Solver& s, int nrec, const char* const* files, const float
     out(A->gmu, gmu, true);
     out(A->gyy, gyy, true);
     out(A->gmr, gmr, false);
-    if (gmom && nmom > 0) {
-        SORD_CUDA(cudaMemcpyAsync(gmom, A->gmom, sizeof(double) * nmom, cudaMemcpyDeviceToHost, s.stream));
-        SORD_CUDA(cudaStreamSynchronize(s.stream));
-    }
+    A->gsrc.assign(5 * (size_t)std::max(nmom, 1), 0.0);
+    SORD_CUDA(cudaMemcpyAsync(A->gsrc.data(), A->gmom, sizeof(double) * A->gsrc.size(), cudaMemcpyDeviceToHost,
+                              s.stream));
     SORD_CUDA(cudaStreamSynchronize(s.stream));
+    if (gmom && nmom > 0) std::copy(A->gsrc.begin(), A->gsrc.begin() + nmom, gmom);
+    A->gsrc.erase(A->gsrc.begin(), A->gsrc.begin() + std::max(nmom, 1));
+}
+
+// Delay (t0) and position gradients of each '.' moment op from the last
+// backward pass: gx[3 m + d] = dL/d(position d of op m) per metre, gt[m] =
+// dL/d(delay of op m's time function) per second.
+void adjoint_source_gradients(Solver& s, double* gx, double* gt, int nmom) {
+    AdjointState* A = s.adj;
+    if (!A || A->gsrc.empty()) throw SordError(SORD_E_STATE, "adjoint: no backward pass recorded");
+    if (nmom != (int)A->mom_ops.size())
+        throw SordError(SORD_E_PARAM, "adjoint: expected " + std::to_string(A->mom_ops.size()) + " moment ops");
+    for (int m = 0; m < nmom; m++) {
+        if (gt) gt[m] = A->gsrc[m];
+        for (int d = 0; d < 3; d++)
+            if (gx) gx[3 * m + d] = A->gsrc[nmom + 3 * m + d];
+    }
 }
 
 }  // namespace sordgpu

@@ -706,6 +706,16 @@ int sord_adjoint_backward(sord_handle* h, int nrec, const char* const* files, co
     return SORD_OK;
 }
 
+int sord_adjoint_source_gradients(sord_handle* h, double* grad_x0, double* grad_t0, int nmoment) {
+    if (!h || nmoment < 0) return SORD_E_PARAM;
+    try {
+        adjoint_source_gradients(h->s, grad_x0, grad_t0, nmoment);
+    } catch (const std::exception& e) {
+        return fail(h, e);
+    }
+    return SORD_OK;
+}
+
 int sord_run(sord_handle* h) {
     if (!h) return SORD_E_PARAM;
     return sord_step(h, h->s.nt - h->s.it);

@@ -201,6 +201,31 @@ float host_time_function(const std::string& pulse, float t, float dt, float tau)
     return f;
 }
 
+// d/dt of the time functions above, in double, for the adjoint's origin-time
+// gradient (derivatives of the formulas; zero for const, delta and step).
+double host_time_function_rate(const std::string& pulse, double t, double tau) {
+    const double pi = 3.14159265358979323846;
+    double f = 0, a, b;
+    if (pulse == "brune") {
+        if (0.0 < t) { a = 1.0 / tau; f = std::exp(-a * t) * a * a * (1.0 - a * t); }
+    } else if (pulse == "integral_brune") {
+        if (0.0 < t) { a = 1.0 / tau; f = std::exp(-a * t) * a * a * t; }
+    } else if (pulse == "hann") {
+        b = pi * tau;
+        if (-b < t && t < b) { a = 1.0 / tau; f = -0.5 / pi * a * a * std::sin(a * t); }
+    } else if (pulse == "integral_hann") {
+        b = pi * tau;
+        if (-b < t && t < b) { a = 1.0 / tau; f = 0.5 / pi * a * (1.0 + std::cos(a * t)); }
+    } else if (pulse == "gaussian" || pulse == "integral_ricker1") {
+        a = 0.5 / (tau * tau); b = std::sqrt(a / pi); f = -2.0 * a * t * std::exp(-a * t * t) * b;
+    } else if (pulse == "ricker1" || pulse == "integral_ricker2") {
+        a = 0.5 / (tau * tau); b = std::sqrt(a / pi) * 2.0 * a; f = -std::exp(-a * t * t) * b * (1.0 - 2.0 * a * t * t);
+    } else if (pulse == "ricker2") {
+        a = 0.5 / (tau * tau); b = std::sqrt(a / pi) * 4.0 * a; f = std::exp(-a * t * t) * b * 2.0 * a * t * (1.5 - a * t * t);
+    }
+    return f;
+}
+
 static inline float wgt(float x, int j, bool plane) { return plane ? 1.0f : 1.0f - std::fabs(x - (float)j); }
 
 static bool applies(Solver& s, const IoOp& io, const char* field, char pass) {
@@ -259,6 +284,36 @@ bool point_injection(Solver& s, IoOp& io, const FieldView& f, int comp, std::vec
                 e.idx = (long long)(j - 1) + (long long)f.n[0] * ((long long)(k - 1) + (long long)f.n[1] * (long long)(l - 1));
                 e.comp = comp;
                 e.inc = val * r;
+                out.push_back(e);
+            }
+    return true;
+}
+
+// The cells a '.' op touches with their trilinear weights r and dr/dx1
+// (x1 in node-index units), in the loop order of point_injection.
+bool point_weights(Solver& s, IoOp& io, const FieldView& f, std::vector<PointWeight>& out) {
+    PointGeom P;
+    point_geom(s, io, f, P);
+    for (int i = 0; i < 3; i++)
+        if (P.i2[i] < P.i1[i]) return false;
+    for (int i = 0; i < 3; i++)
+        if (P.plane[i]) P.i1[i] = P.i2[i] = 1;
+    for (int l = P.i1[2]; l <= P.i2[2]; l++)
+        for (int k = P.i1[1]; k <= P.i2[1]; k++)
+            for (int j = P.i1[0]; j <= P.i2[0]; j++) {
+                const int c[3] = {j, k, l};
+                double w[3], dw[3];
+                for (int i = 0; i < 3; i++) {
+                    const double d = (double)P.xi[i] - (double)c[i];
+                    w[i] = P.plane[i] ? 1.0 : 1.0 - std::fabs(d);
+                    dw[i] = P.plane[i] ? 0.0 : (d > 0.0 ? -1.0 : d < 0.0 ? 1.0 : 0.0);
+                }
+                PointWeight e;
+                e.idx = (long long)(j - 1) + (long long)f.n[0] * ((long long)(k - 1) + (long long)f.n[1] * (long long)(l - 1));
+                e.r = w[0] * w[1] * w[2];
+                e.dr[0] = dw[0] * w[1] * w[2];
+                e.dr[1] = w[0] * dw[1] * w[2];
+                e.dr[2] = w[0] * w[1] * dw[2];
                 out.push_back(e);
             }
     return true;

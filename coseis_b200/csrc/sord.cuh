@@ -237,6 +237,16 @@ struct FieldView {
 void field_io(Solver& s, const char* passes, const char* field, FieldView f);
 void field_io_flush_all(Solver& s);
 bool field_active(Solver& s, const char* field, char pass);
+// cells (or nodes) of a '.' op with their trilinear weights and the
+// weights' derivatives with respect to the op's position (adjoint)
+struct PointWeight {
+    long long idx;  // index into the field
+    double r;       // trilinear weight
+    double dr[3];   // d r / d x1, x1 in node-index units
+};
+bool point_weights(Solver& s, IoOp& io, const FieldView& f, std::vector<PointWeight>& out);
+float host_time_function(const std::string& pulse, float t, float dt, float tau);
+double host_time_function_rate(const std::string& pulse, double t, double tau);
 
 // misc device helpers (util.cu)
 void dev_fill(Solver& s, float* p, long long n, float v);
@@ -333,6 +343,7 @@ void adjoint_begin(Solver& s, int seg);
 void adjoint_checkpoint(Solver& s);
 void adjoint_backward(Solver& s, int nrec, const char* const* files, const float* const* dtrace, const int* ntrace,
                       float* glam, float* gmu, float* gyy, float* gmr, double* gmom, int nmom);
+void adjoint_source_gradients(Solver& s, double* gx, double* gt, int nmom);
 void mem_attach(int device);
 void mem_detach(int device);
 void mem_trim(int device);

@@ -107,6 +107,16 @@ int sord_adjoint_backward(sord_handle* h, int nrec, const char* const* files, co
  * at process exit). */
 int sord_trim_memory(int device);
 
+/* After sord_adjoint_backward: the gradients with respect to the position
+ * and the delay of each '.' moment op (sord.in order), which the backward
+ * pass computes with the moment values.  An op injects val tf(t - t0) r(x)
+ * with r its trilinear weights: grad_x0[3 m + d] = dL/dx_d of op m (per
+ * metre; the weights are piecewise linear, so this is the derivative inside
+ * the current cell), grad_t0[m] = dL/dt0 (per second, t0 a delay of the
+ * time function).  Either pointer may be NULL; nmoment as for
+ * sord_adjoint_backward. */
+int sord_adjoint_source_gradients(sord_handle* h, double* grad_x0, double* grad_t0, int nmoment);
+
 /* Copy a node or cell volume field to host memory (core region only, j
  * fastest; nn or nn-1 values per axis).  Names: vx vy vz ux uy uz ax ay az
  * (nodes; `a` holds the last acceleration) and lam mu yy vc (cells).

@@ -159,3 +159,50 @@ def test_adjoint_rejects_unsupported_runs(change, msg, tmp_path, gpu_lib):
         assert e.value.code == _lib.SORD_E_PARAM and msg in str(e.value)
     finally:
         s.close()
+
+
+@pytest.mark.gpu
+def test_source_position_and_delay_gradients(tmp_path, oracle_bins, gpu_lib):
+    """dL/d(source position) and dL/d(source delay) (sord_adjoint_source_gradients)
+    against central differences of the FP64 oracle: all six moment ops moved
+    together along each axis (h = 1e-3 cell, inside one cell, where the
+    trilinear weights are linear), and the source delayed through the clock
+    origin tm0 (dL/dt0 = -dL/dtm0, h = 1e-4 s)."""
+    from coseis_b200 import _lib
+    exe = oracle_bins['f64']
+    p = problem(7)
+    rho, vp, vs, m = model(11)
+    obs = oracle_traces(p, *model(12), str(tmp_path / 'obs'), exe)
+    d = str(tmp_path / 'adj')
+    files = p.stage(rho, vp, vs, m, d)
+    s = _lib.Solver(d, open(os.path.join(d, 'sord.in')).read())
+    try:
+        s.adjoint_forward(7)
+        tr = p.read_traces(d)
+        dtr = {f: (tr[i // 3, i % 3].astype(np.float64) - obs[i // 3, i % 3]).astype(np.float32)
+               for i, f in enumerate(files)}
+        g = s.adjoint_backward(dtr, 6)
+    finally:
+        s.close()
+    delta = p.prm['delta']
+
+    def L(tag, shift=(0.0, 0.0, 0.0), tm0=None):
+        q = adjoint.Problem(dict(p.prm), dict(p.source), p.receivers, segment=7)
+        q.source['x'] = [a + b for a, b in zip(p.source['x'], shift)]
+        if tm0 is not None:
+            q.prm['tm0'] = tm0
+        t = oracle_traces(q, rho, vp, vs, m, str(tmp_path / tag), exe)
+        return 0.5 * ((t - obs) ** 2).sum()
+
+    h = 1e-3
+    for ax in range(3):
+        e = [0.0, 0.0, 0.0]
+        e[ax] = h
+        fd = (L('xp%d' % ax, e) - L('xm%d' % ax, [-x for x in e])) / (2 * h)
+        an = g['position'][:, ax].sum() * delta[ax]
+        assert abs(an - fd) <= TOL * abs(fd), (ax, an, fd)
+    ht = 1e-4
+    tm0 = p.prm['tm0']
+    fd = (L('tp', tm0=tm0 + ht) - L('tm', tm0=tm0 - ht)) / (2 * ht)
+    an = -g['delay'].sum()
+    assert abs(an - fd) <= TOL * abs(fd), (an, fd)
