@@ -151,10 +151,20 @@ def _function():
     class ReceiverTraces(torch.autograd.Function):
         """traces[r, c, t] = v_c at receiver r, sample t, of the forward run
         with cell fields rho, vp, vs ([j, k, l]) and moment tensor
-        (xx yy zz yz zx xy)."""
+        (xx yy zz yz zx xy); optionally the source position (3, node-index
+        coordinates like the problem's source 'x') and a delay of the source
+        time function (seconds) as differentiable inputs too."""
 
         @staticmethod
-        def forward(ctx, rho, vp, vs, moment, problem):
+        def forward(ctx, rho, vp, vs, moment, problem, position=None, delay=None):
+            ctx.has_source = (position is not None, delay is not None)
+            if position is not None or delay is not None:
+                problem = Problem(problem.prm, problem.source, problem.receivers, problem.segment, problem.device)
+                if position is not None:
+                    problem.source['x'] = [float(a) for a in position.detach().cpu().numpy().ravel()]
+                if delay is not None:
+                    # a delay of the time function is an earlier clock origin
+                    problem.prm['tm0'] = float(problem.prm.get('tm0', 0.0)) - float(delay.detach().cpu())
             d = tempfile.mkdtemp(prefix='sord_adj_')
             try:
                 problem.stage(rho.detach().cpu().numpy(), vp.detach().cpu().numpy(), vs.detach().cpu().numpy(),
@@ -192,7 +202,13 @@ def _function():
             for m, c in enumerate(ctx.order):
                 gmom[c] += res['moment'][m]
             t = lambda a, like: torch.as_tensor(a, dtype=like.dtype, device=like.device)
-            return t(grho, rho), t(gvp, vp), t(gvs, vs), t(gmom, moment), None
+            # source position per node-index unit, summed over the six ops; delay per second
+            gpos = (res['position'].sum(0) * np.asarray(p.prm['delta'][:3], np.float64)
+                    if ctx.has_source[0] else None)
+            gdel = float(res['delay'].sum()) if ctx.has_source[1] else None
+            like = rho
+            return (t(grho, rho), t(gvp, vp), t(gvs, vs), t(gmom, moment), None,
+                    None if gpos is None else t(gpos, like), None if gdel is None else t(gdel, like))
 
     return ReceiverTraces
 

@@ -206,3 +206,35 @@ def test_source_position_and_delay_gradients(tmp_path, oracle_bins, gpu_lib):
     fd = (L('tp', tm0=tm0 + ht) - L('tm', tm0=tm0 - ht)) / (2 * ht)
     an = -g['delay'].sum()
     assert abs(an - fd) <= TOL * abs(fd), (an, fd)
+
+
+@pytest.mark.gpu
+def test_autograd_source_position_and_delay(tmp_path, oracle_bins, gpu_lib):
+    """ReceiverTraces with the source position and delay as inputs: their
+    gradients are the handle's (already held to finite differences) summed
+    over the six moment ops, in node-index units and seconds."""
+    import torch
+    from coseis_b200 import _lib
+    p = problem(7)
+    rho0, vp0, vs0, m0 = model(11)
+    obs = oracle_traces(p, *model(12), str(tmp_path / 'obs'), oracle_bins['f64'])
+    args = [torch.tensor(a, dtype=torch.float32, requires_grad=True) for a in (rho0, vp0, vs0, m0)]
+    pos = torch.tensor(p.source['x'], dtype=torch.float32, requires_grad=True)
+    delay = torch.tensor(0.0, dtype=torch.float32, requires_grad=True)
+    tr = adjoint.ReceiverTraces.apply(*args, p, pos, delay)
+    loss = 0.5 * ((tr.double() - torch.as_tensor(obs)) ** 2).sum()
+    loss.backward()
+    d = str(tmp_path / 'ref')
+    files = p.stage(rho0, vp0, vs0, m0, d)
+    s = _lib.Solver(d, open(os.path.join(d, 'sord.in')).read())
+    try:
+        s.adjoint_forward(7)
+        t = p.read_traces(d)
+        g = s.adjoint_backward({f: (t[i // 3, i % 3].astype(np.float64) - obs[i // 3, i % 3]).astype(np.float32)
+                                for i, f in enumerate(files)}, 6)
+    finally:
+        s.close()
+    ref = g['position'].sum(0) * np.asarray(p.prm['delta'][:3])
+    assert np.allclose(pos.grad.numpy(), ref, rtol=1e-5), (pos.grad, ref)
+    assert abs(float(delay.grad) - g['delay'].sum()) <= 1e-5 * abs(g['delay'].sum())
+    assert np.abs(args[0].grad.numpy()).max() > 0
