@@ -17,6 +17,7 @@ SYMBOLS = [
     'sord_last_error', 'sord_error_string', 'sord_destroy',
     'sord_vector_max_noalloc', 'sord_run_ensemble', 'sord_adjoint_forward', 'sord_adjoint_backward',
     'sord_set_arithmetic', 'sord_get_arithmetic', 'sord_trim_memory', 'sord_adjoint_source_gradients',
+    'sord_set_field',
 ]
 
 # return codes (enum in include/sordgpu.h)
@@ -55,6 +56,8 @@ def load():
     lib.sord_run_directory.restype = ctypes.c_int
     lib.sord_get_field.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(ctypes.c_float), ctypes.c_size_t]
     lib.sord_get_field.restype = ctypes.c_int
+    lib.sord_set_field.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(ctypes.c_float), ctypes.c_size_t]
+    lib.sord_set_field.restype = ctypes.c_int
     lib.sord_info.argtypes = [P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
     lib.sord_info.restype = ctypes.c_int
     lib.sord_stats.argtypes = [P, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
@@ -209,6 +212,14 @@ class Solver(object):
         ptr = out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
         _check(load().sord_get_field(self._h, name.encode(), ptr, out.size), self._h)
         return out.T
+
+    def set_field(self, name, a):
+        """Overwrite field `name` (vx vy vz ux uy uz lam mu yy) with the array
+        `a` of shape (nx, ny, nz) (cells: one less per axis), index [j, k, l]."""
+        import numpy as np
+        a = np.ascontiguousarray(np.asarray(a, dtype=np.float32).T)
+        ptr = a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        _check(load().sord_set_field(self._h, name.encode(), ptr, a.size), self._h)
 
     def stats(self):
         out = (ctypes.c_double * 16)()

@@ -809,6 +809,43 @@ int sord_get_field(sord_handle* h, const char* name, float* host, size_t n) {
     return SORD_OK;
 }
 
+int sord_set_field(sord_handle* h, const char* name, const float* host, size_t n) {
+    if (!h || !name || !host) return SORD_E_PARAM;
+    Solver& s = h->s;
+    try {
+        SORD_CUDA(cudaSetDevice(s.device));
+        std::string f = name;
+        float* dst = nullptr;
+        bool cell = false;
+        const char* vn[6] = {"vx", "vy", "vz", "ux", "uy", "uz"};
+        for (int i = 0; i < 6; i++)
+            if (f == vn[i]) dst = i < 3 ? s.d.v[i] : s.d.u[i - 3];
+        if (f == "lam") { dst = s.d.lam; cell = true; }
+        if (f == "mu") { dst = s.d.mu; cell = true; }
+        if (f == "yy") { dst = s.d.yy; cell = true; }
+        if (!dst) throw SordError(SORD_E_PARAM, "field cannot be set: " + f);
+        int c[3];
+        for (int i = 0; i < 3; i++) c[i] = cell ? s.g.nn[i] - 1 : s.g.nn[i];
+        size_t need = (size_t)c[0] * c[1] * c[2];
+        if (n != need) throw SordError(SORD_E_PARAM, "host array has " + std::to_string(n) + " values, the field " +
+                                                     std::to_string(need));
+        // read-modify-write of the whole array keeps the halo as it is
+        std::vector<float> all((size_t)s.g.nv);
+        SORD_CUDA(cudaMemcpyAsync(all.data(), dst, sizeof(float) * (size_t)s.g.nv, cudaMemcpyDeviceToHost, s.stream));
+        SORD_CUDA(cudaStreamSynchronize(s.stream));
+        size_t q = 0;
+        for (int l = 0; l < c[2]; l++)
+            for (int k = 0; k < c[1]; k++)
+                for (int j = 0; j < c[0]; j++)
+                    all[(size_t)s.g.idx(s.g.i1core[0] + j, s.g.i1core[1] + k, s.g.i1core[2] + l)] = host[q++];
+        SORD_CUDA(cudaMemcpyAsync(dst, all.data(), sizeof(float) * (size_t)s.g.nv, cudaMemcpyHostToDevice, s.stream));
+        SORD_CUDA(cudaStreamSynchronize(s.stream));
+    } catch (const std::exception& e) {
+        return fail(h, e);
+    }
+    return SORD_OK;
+}
+
 int sord_info(const sord_handle* h, int* nn3, int* it, int* nt) {
     if (!h) return SORD_E_PARAM;
     if (nn3) for (int i = 0; i < 3; i++) nn3[i] = h->s.g.nn[i];

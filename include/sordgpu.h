@@ -123,6 +123,14 @@ int sord_adjoint_source_gradients(sord_handle* h, double* grad_x0, double* grad_
  * `n` is the capacity of `host` in floats. */
 int sord_get_field(sord_handle* h, const char* name, float* host, size_t n);
 
+/* Overwrite a field between steps from host memory (the layout of
+ * sord_get_field; `n` must equal the field's core size): the state vx vy vz
+ * ux uy uz (initial conditions, perturbations) or the cell moduli lam mu yy
+ * (no consistency with the other material arrays or the Courant condition
+ * is checked).  Halo values are kept.  Replaces: fields read by '=<' ops
+ * (sord/input_output.f90:392-419), from memory and between any two steps. */
+int sord_set_field(sord_handle* h, const char* name, const float* host, size_t n);
+
 /* Query dimensions and progress: nn[3] global nodes, it (steps done), nt. */
 int sord_info(const sord_handle* h, int* nn3, int* it, int* nt);
 
