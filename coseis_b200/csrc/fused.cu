@@ -887,6 +887,9 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
     } while (0)
 
     // ---------------------------------------------------------------- cell phase
+    constexpr bool CARRY = FM && GEOM != GEOM_GENERAL;
+    float4 ca[4], cb[4];  // plane l+1 corners of the last cell computed, for plane l+1's cell
+    int carry_l = -1000;  // the plane of that cell
     auto cells = [&](int l, auto fast_tag) {
         constexpr bool F = decltype(fast_tag)::value;
         const int cs = FM ? 0 : l & 1;
@@ -898,15 +901,28 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
             return;
         }
         const long long q = g.idx(J, K, l);
-        // corner values by corner id n = dj + 2 dk + 4 dl (node planes l, l+1)
+        // corner values by corner id n = dj + 2 dk + 4 dl (node planes l, l+1);
+        // fast arithmetic keeps the plane l+1 corners for the next plane's cell
         float Wc[3][8], Hc[3][8], X0[8], X1[8], X2[8];
         {
             const float4* p0 = sN + (l % 3) * (NGN * NPL) + (tx + FNJ * ty);
             const float4* p1 = sN + ((l + 1) % 3) * (NGN * NPL) + (tx + FNJ * ty);
+            const bool reuse = CARRY && carry_l == l - 1;
 #pragma unroll
             for (int n = 0; n < 8; n++) {
                 const float4* p = ((n >> 2) ? p1 : p0) + (n & 1) + FNJ * ((n >> 1) & 1);
-                const float4 a = p[0], b = p[NPL];
+                float4 a, b;
+                if (CARRY && n < 4 && reuse) {
+                    a = ca[n];
+                    b = cb[n];
+                } else {
+                    a = p[0];
+                    b = p[NPL];
+                }
+                if (CARRY && n >= 4) {
+                    ca[n - 4] = a;
+                    cb[n - 4] = b;
+                }
                 Wc[0][n] = a.x; Wc[1][n] = a.y; Wc[2][n] = a.z;
                 Hc[0][n] = b.x; Hc[1][n] = b.y; Hc[2][n] = b.z;
                 if (GEOM == GEOM_TERRAIN) {
@@ -919,6 +935,7 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
                     X2[n] = p[2 * NPL].x;
                 }
             }
+            if (CARRY) carry_l = l;
         }
         // support-operator brackets; directions 0 and 1 in the two lanes
         float B[3][8];
