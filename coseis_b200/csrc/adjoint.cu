@@ -31,6 +31,7 @@
 #include <vector>
 
 #include "sord.cuh"
+#include "timefn.h"
 #include "stencil.cuh"
 
 namespace sordgpu {

@@ -246,7 +246,6 @@ struct PointWeight {
 };
 bool point_weights(Solver& s, IoOp& io, const FieldView& f, std::vector<PointWeight>& out);
 float host_time_function(const std::string& pulse, float t, float dt, float tau);
-double host_time_function_rate(const std::string& pulse, double t, double tau);
 
 // misc device helpers (util.cu)
 void dev_fill(Solver& s, float* p, long long n, float v);

@@ -30,3 +30,13 @@ def test_fast_brackets_match_reference_forms(tmp_path):
     assert eterr < 1e-6, eterr
     # the identity holds in exact arithmetic; double rounding only
     assert ecn < 1e-12, ecn
+
+
+def test_time_function_rates(tmp_path):
+    """The time derivatives behind the adjoint's delay gradient match central
+    differences of every smooth source time function."""
+    exe = str(tmp_path / 'rate')
+    subprocess.check_call(['g++', '-std=c++17', '-O2', '-ffp-contract=off', '-o', exe,
+                           os.path.join(HERE, 'timefn_rate.cpp')])
+    out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()
+    assert out[-2] == 'worst' and float(out[-1]) < 1e-6, out
