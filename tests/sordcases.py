@@ -256,6 +256,47 @@ def case_free(nt=24):
     return prm
 
 
+def case_io_ops(nt=6):
+    """Every field-I/O op kind on a node field (ax) and a cell field (wxx),
+    after cst/tests/sord_io.py: '#', '= + *', the random '=~ +~ *~', the
+    cube '=@ +@ *@', '=' with every time function, a '.' point op and the
+    file reads '.< =< +< *<'; outputs of several fields by '.>' and '=>'."""
+    from coseis_b200 import sord
+    prm = {'shape': [9, 10, 11, nt], 'delta': [100.0, 100.0, 100.0, 0.008], 'itstats': 1, 'itio': 3,
+           'bc1': ['free'] * 3, 'bc2': ['free'] * 3, 'npml': 0, 'gam': [0.1], 'hourglass': [1.0, 0.5],
+           'mxx': [([4.0, 4.5, 5.0, []], '.', 1e14, 'brune', 0.05)]}
+    x1, x2 = [110.0, 110.0, 110.0], [590.0, 690.0, 790.0]
+    ii = [4.4, 5.5, 6.6, 1]
+    for k in ('ax', 'wxx'):
+        ops = [([], '#')]
+        for op in ('=', '+', '*', '=~', '+~', '*~'):
+            ops.append(([], op, 2.2))
+        for op in ('=@', '+@', '*@'):
+            ops.append(([], op, x1, x2, 2.2))
+        for func in sorted(sord.time_functions):
+            ops.append(([], '=', 2.2, func, 0.033))
+        ops.append((ii, '.', 2.2))
+        for i, op in enumerate(('.<', '=<', '+<', '*<')):
+            ops.append((ii if op == '.<' else [4, 5, 6, 1], op, '%s_i%d.bin' % (k, i)))
+        prm[k] = ops
+    # ops whose results last (the sequences above end in plain sets)
+    prm['gam'] = [([], '=~', 0.2)]
+    prm['rho'] = [2670.0, ([], '+@', x1, x2, 100.0)]
+    prm['vx'] = [([], '+~', 1e-4)]
+    prm['vy'] = [([], '*@', x1, x2, 0.5)]
+    prm['vz'] = [([], '*~', 1.0)]
+    for k in ('vx', 'vy', 'uz', 'ax', 'wxx', 'wyz', 'am2', 'wm2'):
+        prm[k] = list(prm.get(k, [])) + [([4.4, 5.5, 6.6, []], '.>', 'o1-%s.bin' % k),
+                                          ([[], [], 5, []], '=>', 'o0-%s.bin' % k)]
+    return prm
+
+
+def io_ops_inputs(path):
+    for k in ('ax', 'wxx'):
+        for i in range(4):
+            np.array([1.5 + i], '<f4').tofile(os.path.join(path, '%s_i%d.bin' % (k, i)))
+
+
 CASES = {
     'mpi': case_mpi,
     'pml': case_pml,
@@ -273,8 +314,9 @@ CASES = {
     'fault_x': case_fault_x,
     'fault_noise': case_fault_noise,
     'free': case_free,
+    'io_ops': case_io_ops,
 }
-INPUTS = {'wave': wave_inputs, 'interior_wave': interior_wave_inputs}
+INPUTS = {'wave': wave_inputs, 'interior_wave': interior_wave_inputs, 'io_ops': io_ops_inputs}
 
 
 def stage(prm, path, realsize=4, inputs=None):
