@@ -824,6 +824,11 @@ int sord_set_field(sord_handle* h, const char* name, const float* host, size_t n
         if (f == "mu") { dst = s.d.mu; cell = true; }
         if (f == "yy") { dst = s.d.yy; cell = true; }
         if (!dst) throw SordError(SORD_E_PARAM, "field cannot be set: " + f);
+        // a fault's moduli (lamf, muf) and the zeroed hourglass constant of
+        // its cell layer are derived from lam, mu and yy at setup
+        if (cell && s.g.ifn != 0)
+            throw SordError(SORD_E_PARAM, "field cannot be set on a run with a fault (its fault-plane moduli are "
+                                          "derived from lam and mu at setup): " + f);
         int c[3];
         for (int i = 0; i < 3; i++) c[i] = cell ? s.g.nn[i] - 1 : s.g.nn[i];
         size_t need = (size_t)c[0] * c[1] * c[2];

@@ -126,9 +126,15 @@ extern "C" int sord_vector_max_noalloc(const float* w0, const float* w1, const f
     long long want = (cnt + kNoAllocThreads - 1) / kNoAllocThreads;
     int nb = (int)(want < kNoAllocBlocks ? want : kNoAllocBlocks);
     cudaStream_t st = (cudaStream_t)stream;
-    k_vmax_partials<<<nb, kNoAllocThreads, 0, st>>>(w0, w1, w2, nm[0], nm[1], i1[0], i1[1], i1[2], c[0], c[1], c[2], partials);
-    k_vmax_final<<<1, kNoAllocThreads, 0, st>>>(partials, nb, out);
-    cudaError_t e = cudaGetLastError();
+    // each launch reports its own status: an error the caller left pending
+    // from an earlier launch stays the caller's (no cudaGetLastError here)
+    int n0 = nm[0], n1 = nm[1], a0 = i1[0], a1 = i1[1], a2 = i1[2], c0 = c[0], c1 = c[1], c2 = c[2];
+    void* pargs[] = {(void*)&w0, (void*)&w1, (void*)&w2, &n0, &n1, &a0, &a1, &a2, &c0, &c1, &c2, (void*)&partials};
+    cudaError_t e = cudaLaunchKernel((const void*)k_vmax_partials, dim3(nb), dim3(kNoAllocThreads), pargs, 0, st);
+    if (e != cudaSuccess) return set_error(SORD_E_CUDA, cudaGetErrorString(e));
+    const unsigned* cpart = partials;
+    void* fargs[] = {(void*)&cpart, &nb, (void*)&out};
+    e = cudaLaunchKernel((const void*)k_vmax_final, dim3(1), dim3(kNoAllocThreads), fargs, 0, st);
     if (e != cudaSuccess) return set_error(SORD_E_CUDA, cudaGetErrorString(e));
     return SORD_OK;
 }

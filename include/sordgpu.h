@@ -125,9 +125,14 @@ int sord_get_field(sord_handle* h, const char* name, float* host, size_t n);
 
 /* Overwrite a field between steps from host memory (the layout of
  * sord_get_field; `n` must equal the field's core size): the state vx vy vz
- * ux uy uz (initial conditions, perturbations) or the cell moduli lam mu yy
- * (no consistency with the other material arrays or the Courant condition
- * is checked).  Halo values are kept.  Replaces: fields read by '=<' ops
+ * ux uy uz (initial conditions, perturbations) or the cell moduli lam mu yy,
+ * where yy is the hourglass coefficient as sord_get_field returns it (the
+ * material setup's mu (lam + mu) / (lam + 2 mu) times the cell-size factor,
+ * sord/material_model.f90:120-131, zero outside the cell region,
+ * sord/material_resample.f90:40).  No consistency with the other material
+ * arrays or the Courant condition is checked, and on a run with a fault the
+ * moduli cannot be set (SORD_E_PARAM): the fault-plane moduli are derived
+ * from them at setup.  Halo values are kept.  Replaces: fields read by '=<' ops
  * (sord/input_output.f90:392-419), from memory and between any two steps. */
 int sord_set_field(sord_handle* h, const char* name, const float* host, size_t n);
 

@@ -25,7 +25,9 @@
 //
 // Build: oracle/build.py (FP32 -> _build/sord_oracle_f32, FP64 -> _f64).
 // Run:   cd <dir containing sord.in> && sord_oracle_f32 [--threads N]
-//        [--nt-limit K]  -> writes the same output files as sord.x.
+//        [--nt-limit K] [--w1-geometry]  -> writes the same output files as
+//        sord.x.  --w1-geometry reproduces the reference's fault normals and
+//        hypocentral radius from w1 (see the list of decisions below).
 //
 // Decisions where the reference is undefined or broken are the same ones the
 // CUDA solver makes: the PML bounds from sord.in are converted so that exactly npml node
@@ -183,6 +185,11 @@ struct Sord {
     std::chrono::steady_clock::time_point clock0;
     int nt_limit = -1;
     int timed_from = -1;              // report the time of steps timed_from+1 .. nt
+    // --w1-geometry: fault normals and the hypocentral radius from w1 as the
+    // reference computes them (dynamic_rupture.f90:120,186,197-199): w1 then
+    // holds cell centres with a zeroed halo (grid_generation.f90:127-132).
+    // Off by default: node coordinates xx.
+    bool w1_geometry = false;
     double timed_seconds = 0;
 
     long long clock_ticks() {
@@ -1338,7 +1345,7 @@ struct Sord {
             int a1[3], a2[3];
             for (int i = 0; i < 3; i++) { a1[i] = i1core[i]; a2[i] = i2core[i]; }
             a1[ifn - 1] = irup; a2[ifn - 1] = irup;
-            node_normals(nhat, xx, a1, a2, ifn);
+            node_normals(nhat, w1_geometry ? w1 : xx, a1, a2, ifn);
         }
         size_t np = area.size();
         for (size_t q = 0; q < np; q++) {
@@ -1383,6 +1390,7 @@ struct Sord {
             for (size_t q = 0; q < np; q++)
                 t0.d[q + c * np] = t0.d[q + c * np] + t3.d[q] * t1.d[q + c * np] + t3.d[q + np] * t2.d[q + c * np] + t3.d[q + 2 * np] * nhat.d[q + c * np];
         if (rcrit > R(0) && vrup > R(0)) {
+            A4& geo = w1_geometry ? w1 : xx;
             real xhypo[3] = {0, 0, 0}, xi[3];
             int i1[3];
             for (int i = 0; i < 3; i++) { xi[i] = hypocenter[i] - R(nnoff[i]) + R(1); i1[i] = ffloor(xi[i]); }
@@ -1391,7 +1399,7 @@ struct Sord {
                     for (int k = i1[1]; k <= i1[1] + 1; k++)
                         for (int j2 = i1[0]; j2 <= i1[0] + 1; j2++) {
                             real w = (R(1) - std::fabs(xi[0] - R(j2))) * (R(1) - std::fabs(xi[1] - R(k))) * (R(1) - std::fabs(xi[2] - R(l)));
-                            for (int i = 1; i <= 3; i++) xhypo[i - 1] = xhypo[i - 1] + w * xx(j2, k, l, i);
+                            for (int i = 1; i <= 3; i++) xhypo[i - 1] = xhypo[i - 1] + w * geo(j2, k, l, i);
                         }
             }
             for (int ll = 1; ll <= fn3[2]; ll++)
@@ -1400,7 +1408,7 @@ struct Sord {
                         size_t q = (size_t)(jj - 1) + (size_t)fn3[0] * ((size_t)(kk - 1) + (size_t)fn3[1] * (size_t)(ll - 1));
                         size_t vq = vol_index(jj, kk, ll, irup);
                         size_t nv = (size_t)nm[0] * nm[1] * nm[2];
-                        for (int i = 0; i < 3; i++) t2.d[q + i * np] = xx.d[vq + i * nv] - xhypo[i];
+                        for (int i = 0; i < 3; i++) t2.d[q + i * np] = geo.d[vq + i * nv] - xhypo[i];
                         rhypo.d[q] = std::sqrt(t2.d[q] * t2.d[q] + t2.d[q + np] * t2.d[q + np] + t2.d[q + 2 * np] * t2.d[q + 2 * np]);
                     }
         }
@@ -1986,11 +1994,13 @@ struct Sord {
 int main(int argc, char** argv) {
     std::string path = "sord.in";
     int threads = 1, ntl = -1, tfrom = -1;
+    bool w1g = false;
     for (int i = 1; i < argc; i++) {
         std::string a = argv[i];
         if (a == "--threads" && i + 1 < argc) threads = atoi(argv[++i]);
         else if (a == "--nt-limit" && i + 1 < argc) ntl = atoi(argv[++i]);
         else if (a == "--timed-from" && i + 1 < argc) tfrom = atoi(argv[++i]);
+        else if (a == "--w1-geometry") w1g = true;
         else path = a;
     }
 #ifdef _OPENMP
@@ -2001,6 +2011,7 @@ int main(int argc, char** argv) {
     Sord* s = new Sord();
     s->nt_limit = ntl;
     s->timed_from = tfrom;
+    s->w1_geometry = w1g;
     try {
         auto t0 = std::chrono::steady_clock::now();
         s->run(path);

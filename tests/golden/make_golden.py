@@ -17,8 +17,6 @@ files.
   pulse), sampled on the solver's output times, unfiltered and after the
   lowpass of scripts/Explosion-plot.py:54-58 (cst/dsp.py:107-142), plus a
   probe vector through the same filter to pin its restatement.
-* dsp.json -- reference time functions, Brune-to-Gauss replacement and
-  filters (cst/dsp.py:26-142) on fixed probe signals.
 * srf.json -- a small synthetic SRF rupture read and written by the
   reference (cst/srf.py:13-194) and the fault geometry of its points
   (cst/coord.py:190-202 slip_vectors, 336-351 potency_tensor).
@@ -254,26 +252,6 @@ def make_srf(ref):
             'potency': [[np.asarray(a, dtype=float).tolist() for a in part] for p_ in pot for part in p_]}
 
 
-def make_dsp(ref):
-    """Reference time functions, Brune-to-Gauss replacement and filters
-    (cst/dsp.py:26-142) on fixed probes."""
-    sys.path.insert(0, ref)
-    import cst.dsp as d
-    t = np.linspace(-0.3, 0.5, 81)
-    pulses = ['const', 'delta', 'step', 'integral_delta', 'brune', 'integral_brune', 'hann', 'integral_hann',
-              'gaussian', 'integral_ricker1', 'ricker1', 'integral_ricker2', 'ricker2']
-    tf = {p: d.time_function(p, t, 0.05).tolist() for p in pulses}
-    x = np.sin(np.linspace(0, 12, 200)) + np.linspace(-1, 1, 200) ** 3
-    filt = {
-        'low2': d.filter(x, 0.01, 5.0, 'lowpass', 2, 0).tolist(),
-        'high4': d.filter(x, 0.01, 3.0, 'highpass', 4, 1).tolist(),
-        'band': d.filter(x, 0.01, (2.0, 8.0), 'bandpass', 2, -1).tolist(),
-        'hann': d.filter(x, 0.01, 4.0, 'hann', 2, 1).tolist(),
-    }
-    return {'t': t.tolist(), 'tau': 0.05, 'time_function': tf, 'x': x.tolist(), 'filter': filt,
-            'brune2gauss': d.brune2gauss(x, 0.01, 0.05).tolist()}
-
-
 def write_loh1(ref):
     import numpy as np
     names = {'t': 'Time', 'radial': 'V-Radial', 'transverse': 'V-Transverse', 'vertical': 'V-Vertical'}
@@ -302,8 +280,6 @@ def main():
         json.dump(make_kostrov(ref), fh, indent=1, sort_keys=True)
     with open(os.path.join(HERE, 'explosion.json'), 'w') as fh:
         json.dump(make_explosion(ref), fh, indent=1, sort_keys=True)
-    with open(os.path.join(HERE, 'dsp.json'), 'w') as fh:
-        json.dump(make_dsp(ref), fh, indent=1, sort_keys=True)
     with open(os.path.join(HERE, 'srf.json'), 'w') as fh:
         json.dump(make_srf(ref), fh, indent=1, sort_keys=True, default=lambda o: o.item())
     write_loh1(ref)

@@ -77,13 +77,28 @@ def fk_traces():
     return t, np.apply_along_axis(np.convolve, -1, v, b, 'same')
 
 
+def brune_to_gauss(x, dt, tau, sigma):
+    """Replace the Brune moment-rate pulse b(t) = t exp(-t / tau) / tau^2 of
+    a trace by a unit Gaussian of width sigma, the processing of
+    scripts/PEER-LOH1-plot.py.  The Brune pulse has the transfer function
+    1 / (1 + i w tau)^2, so the replacement is the convolution with
+    (1 + tau d/dt)^2 g for the Gaussian g = sqrt(s / 2 pi) exp(-s t^2 / 2),
+    s = 1 / sigma^2; g' = -s t g and g'' = (s^2 t^2 - s) g give the kernel
+    g (1 - 2 s tau t + tau^2 (s^2 t^2 - s)), truncated at 6 sigma."""
+    s = 1.0 / (sigma * sigma)
+    n = int(6.0 * sigma / dt)
+    t = np.arange(-n, n + 1) * dt
+    g = np.sqrt(0.5 * s / math.pi) * np.exp(-0.5 * s * t * t)
+    k = dt * g * (1.0 - 2.0 * s * tau * t + tau * tau * (s * s * t * t - s))
+    return np.apply_along_axis(np.convolve, -1, x, k, 'same')
+
+
 def sord_traces(path):
-    from coseis_b200 import dsp
     v = np.array([np.fromfile(os.path.join(path, 'p9-%s.bin' % f), '<f4') for f in ('vx', 'vy', 'vz')],
                  dtype=np.float64)
     m = 0.2 * np.array([(3, 4, 0), (-4, 3, 0), (0, 0, 5)], dtype=np.float64)
     v = m @ v
-    return np.arange(v.shape[1]) * DT, dsp.brune2gauss(v, DT, TAU, SIGMA)
+    return np.arange(v.shape[1]) * DT, brune_to_gauss(v, DT, TAU, SIGMA)
 
 
 def misfit(ts, vs, tf, vf):

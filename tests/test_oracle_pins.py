@@ -5,7 +5,10 @@ The reference ships no solver output, so the oracle is pinned through the
 physics checks the reference itself uses, with the analytic values computed
 by the reference's own code into tests/golden/ (make_golden.py):
 
-* the Kostrov crack test, cst/tests/sord_kostrov.py:12-76;
+* the Kostrov crack test, cst/tests/sord_kostrov.py:12-76, at the
+  reference's resolution and refined twofold (where it meets the
+  reference's 1.5 % per receiver), and with the reference's own fault
+  geometry (which fails it);
 * the explosion point source of scripts/Explosion-sim.py against the analytic
   solution of scripts/Explosion-plot.py:41-58;
 * the decomposition-identity tests cst/tests/sord_mpi.py:49-71 and
@@ -16,6 +19,7 @@ by the reference's own code into tests/golden/ (make_golden.py):
 import json
 import math
 import os
+import subprocess
 
 import numpy as np
 import pytest
@@ -29,39 +33,100 @@ def _golden(name):
     return json.load(open(os.path.join(GOLDEN, name)))
 
 
-def kostrov_prm():
-    """cst/tests/sord_kostrov.py:12-49 (serial)."""
+def kostrov_prm(refine=1):
+    """cst/tests/sord_kostrov.py:12-49 (serial).  refine > 1 divides dx and
+    dt by it and keeps the physical problem: the same domain, PML thickness,
+    fault plane half a cell below the last node, and receivers 2 km from the
+    hypocentre."""
     g = _golden('kostrov.json')
     nx, ny, nz, nt = g['shape']
+    f = refine
     prm = {
-        'delta': [g['dx'], g['dx'], g['dx'], g['dt']], 'shape': [nx, ny, nz, nt],
+        'delta': [g['dx'] / f, g['dx'] / f, g['dx'] / f, g['dt'] / f],
+        'shape': [(nx - 1) * f + 1, (ny - 1) * f + 1, (nz - 2) * f + 2, nt * f],
         'rho': [g['rho']], 'vp': [g['vp']], 'vs': [g['vs']], 'gam': 1.0, 'hourglass': [1.0, 1.0],
-        'bc1': ['pml', 'pml', 'pml'], 'bc2': ['-node', '+node', '-cell'],
+        'bc1': ['pml', 'pml', 'pml'], 'bc2': ['-node', '+node', '-cell'], 'npml': 10 * f,
         'faultnormal': '+z', 'hypocenter': [-1.0, -1.0, -1.5], 'vrup': g['vrup'],
         'rcrit': 1e9, 'trelax': 0.0, 'mud': 1.0, 'mus': 1e9, 'dc': 1e9,
         'tn': -90e6, 'ts': -90e6 - g['dtau'],
-        'svm': [([-1, -21, []], '=>', 'p20a.bin'), ([-13, -17, []], '=>', 'p20b.bin'),
-                ([-17, -13, []], '=>', 'p20c.bin'), ([-21, -1, []], '=>', 'p20d.bin')],
+        'svm': [([-1, -1 - 20 * f, []], '=>', 'p20a.bin'), ([-1 - 12 * f, -1 - 16 * f, []], '=>', 'p20b.bin'),
+                ([-1 - 16 * f, -1 - 12 * f, []], '=>', 'p20c.bin'), ([-1 - 20 * f, -1, []], '=>', 'p20d.bin')],
     }
     return prm, g
 
 
-def test_kostrov_slip_rate(tmp_path, oracle_bins):
-    """Final slip rate 2 km from the hypocentre vs Kostrov's solution.  The
-    reference test asserts 1.5 %; this restatement gives 1.2-2.1 % on the four
-    receivers (a larger mesh does not reduce it: discretisation error), so
-    the bound here is 2.5 %."""
-    prm, g = kostrov_prm()
-    d = str(tmp_path / 'k')
-    sc.stage(prm, d)
-    sc.run_oracle(d, oracle_bins['f32'], threads=os.cpu_count() or 1)
+def kostrov_errors(d, g, nt, dtype='<f4'):
+    """Relative error of the final slip rate at the four receivers
+    (cst/tests/sord_kostrov.py:70-76)."""
     errs = []
     for p in 'abcd':
-        v = np.fromfile(os.path.join(d, 'p20%s.bin' % p), '<f4')
-        assert v.shape == (g['shape'][3],)
+        v = np.fromfile(os.path.join(d, 'p20%s.bin' % p), dtype)
+        assert v.shape == (nt,)
         errs.append((g['slip_rate'] - float(v[-1])) / g['slip_rate'])
+    return errs
+
+
+def run_kostrov(tmp_path, exe, refine=1, extra=()):
+    prm, g = kostrov_prm(refine)
+    d = str(tmp_path / ('k%d' % refine))
+    sc.stage(prm, d)
+    r = subprocess.run([exe, '--threads', str(os.cpu_count() or 1)] + list(extra), cwd=d,
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return kostrov_errors(d, g, prm['shape'][3])
+
+
+def test_kostrov_reference_geometry_fails(tmp_path, oracle_bins):
+    """The reference as shipped computes fault normals and the hypocentral
+    radius from w1 (dynamic_rupture.f90:120,186,197-199), which holds cell
+    centres with a zeroed halo at that point (grid_generation.f90:127-132).
+    The Kostrov hypocentre sits on the last node row, so its interpolated
+    position is the origin (the far PML corner): the forced rupture starts
+    there and never reaches the receivers within the run.  The oracle's
+    --w1-geometry switch reproduces that; the slip rate stays near zero and
+    the reference's own 1.5 % assertion fails at every receiver (measured
+    error 0.9999-1.0000).  The oracle therefore uses the node coordinates."""
+    errs = run_kostrov(tmp_path, oracle_bins['f32'], extra=['--w1-geometry'])
+    assert min(abs(e) for e in errs) > 0.99, errs
+
+
+def test_kostrov_slip_rate(tmp_path, oracle_bins):
+    """Final slip rate 2 km from the hypocentre vs Kostrov's solution at the
+    reference test's resolution (dx 100 m): 1.2, 2.1, 1.5 and 1.7 % on the
+    four receivers, against the reference test's 1.5 %.  The error is
+    discretisation error: at dx 50 m (test_kostrov_slip_rate_refined) every
+    receiver is within 1.5 %.  Bound here 2.5 %."""
+    errs = run_kostrov(tmp_path, oracle_bins['f32'])
     assert max(abs(e) for e in errs) < 0.025, errs
-    assert min(abs(e) for e in errs) < g['reference_tolerance'], errs
+    assert min(abs(e) for e in errs) < 0.015, errs
+
+
+def test_kostrov_slip_rate_refined(tmp_path, oracle_bins):
+    """The same crack at dx = 50 m (twice the resolution, 101 x 101 x 46
+    nodes, 400 steps): every receiver within the reference test's own bound
+    of 1.5 % (cst/tests/sord_kostrov.py:76); measured 1.1, 1.25, 1.3 and
+    0.85 %, each below its dx = 100 m error."""
+    errs = run_kostrov(tmp_path, oracle_bins['f32'], refine=2)
+    assert max(abs(e) for e in errs) < 0.015, errs
+
+
+@pytest.mark.gpu
+def test_kostrov_slip_rate_gpu_refined(tmp_path, gpu_lib):
+    """The CUDA solver (reference order, bit-identical to the oracle) on the
+    crack at dx = 50 m and 25 m (201 x 201 x 90 nodes, 800 steps, too long
+    for the CPU suite): every receiver within 1.5 % at both resolutions, and
+    the largest error smaller at 25 m than at 50 m."""
+    worst = []
+    for refine in (2, 4):
+        prm, g = kostrov_prm(refine)
+        d = str(tmp_path / ('g%d' % refine))
+        sc.stage(prm, d)
+        sc.run_gpu(d)
+        errs = kostrov_errors(d, g, prm['shape'][3])
+        print('Kostrov dx = %g m: %s' % (g['dx'] / refine, ', '.join('%.4f' % e for e in errs)))
+        assert max(abs(e) for e in errs) < 0.015, (refine, errs)
+        worst.append(max(abs(e) for e in errs))
+    assert worst[1] < worst[0], worst
 
 
 def lowpass2(x, dt, cutoff):

@@ -53,6 +53,43 @@ def test_vector_max_noalloc_matches_solver_stats(tmp_path, gpu_lib):
     assert math.sqrt(got[1]) == stats[2]
 
 
+def _max_sq(f, i1, i2):
+    """FP32 max of (x^2 + y^2) + z^2 over the 1-based region, in the
+    kernel's order of operations."""
+    sl = tuple(slice(a - 1, b) for a, b in zip(i1, i2))
+    x, y, z = (np.asarray(c[sl], dtype=np.float32) for c in f)
+    return np.float32((x * x + y * y) + z * z).max() if x.size else None
+
+
+def test_vector_max_noalloc_sub_regions(gpu_lib):
+    """Offset sub-regions, a region of two elements and NaN handling,
+    exactly against numpy on the same FP32 values."""
+    import torch
+    from coseis_b200 import _lib
+
+    nn = [13, 11, 9]
+    rng = np.random.default_rng(7)
+    f = [rng.standard_normal(nn).astype(np.float32) for _ in range(3)]
+
+    def run(fields, i1, i2):
+        dev = [torch.from_numpy(np.ascontiguousarray(a.T)).cuda() for a in fields]
+        out = torch.full((1,), -1.0, dtype=torch.float32, device='cuda')
+        _lib.vector_max_noalloc(dev[0].data_ptr(), dev[1].data_ptr(), dev[2].data_ptr(), nn, i1, i2,
+                                out.data_ptr())
+        torch.cuda.synchronize()
+        return np.float32(out.cpu().numpy()[0])
+
+    for i1, i2 in (([2, 3, 4], [nn[0] - 1, nn[1] - 2, nn[2] - 1]), ([5, 7, 3], [5, 7, 4]),
+                   ([1, 1, 1], [1, 1, 1]), ([13, 2, 1], [13, 11, 9])):
+        got = run(f, i1, i2)
+        assert got == _max_sq(f, i1, i2), (i1, i2)
+    # a NaN inside the region wins; one outside it is not read
+    g = [a.copy() for a in f]
+    g[1][6, 8, 4] = np.nan
+    assert np.isnan(run(g, [2, 3, 4], [12, 9, 8]))
+    assert run(g, [2, 3, 6], [12, 9, 8]) == _max_sq(g, [2, 3, 6], [12, 9, 8])
+
+
 def test_vector_max_noalloc_rejects_bad_regions(gpu_lib):
     import torch
     from coseis_b200 import _lib
