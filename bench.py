@@ -251,6 +251,153 @@ def stage_scenarios(indices, root, seed=SEED, nt=ENS_NT, shape=None):
     return dirs
 
 
+# ------------------------------------------------------- explosion and rupture configs
+def explosion_prm(nt=200, seed=SEED):
+    """Plain point-source explosion: 61^3 rectilinear nodes, dx 100 m,
+    dt 0.008 s, 200 steps; rho 2670, vp 6000, vs 3464; isotropic moment
+    source (M0 1e16 N m, Brune, tau 0.1 s) at the centre node, spread over
+    its 8 cells; 10-node PML on all six faces; default hourglass constants;
+    vx, vy, vz on the k mid-plane every 10 steps and at 8 seeded interior
+    nodes."""
+    n, c = 61, 30
+    prm = {'shape': [n, n, n, nt], 'delta': [100.0, 100.0, 100.0, 0.008],
+           'rho': [2670.0], 'vp': [6000.0], 'vs': [3464.0], 'gam': [0.0], 'hourglass': [1.0, 1.0],
+           'bc1': ['pml'] * 3, 'bc2': ['pml'] * 3, 'npml': 10, 'itstats': 10, 'itio': 50}
+    for f in ('mxx', 'myy', 'mzz'):
+        prm[f] = [([c, c, c, []], '.', 1e16, 'brune', 0.1)]
+    rng = np.random.default_rng([seed, 1])
+    rec = rng.integers(12, n - 12, size=(8, 3))
+    for f in ('vx', 'vy', 'vz'):
+        prm[f] = [([[], c, [], [0, None, 10]], '=>', 'snap-%s.bin' % f)]
+        prm[f] += [([int(j), int(k), int(l), []], '=>', 'rec%d-%s.bin' % (r, f)) for r, (j, k, l) in enumerate(rec)]
+    return prm
+
+
+RUP_SHAPE = (600, 300, 300)
+
+
+def rupture3_prm(nt=1500, shape=RUP_SHAPE, seed=SEED, dx=50.0, dt=0.004):
+    """Spontaneous rupture on a planar fault: 600 x 300 x 300 nodes, dx 50 m,
+    dt 0.004 s, 1500 steps, homogeneous rho 2670, vp 6000, vs 3464;
+    double-node fault ('+y') at the k mid-plane; 20 km x 10 km frictional
+    region (mu_s = 1e4 outside); linear slip weakening mu_s 0.65, mu_d 0.50,
+    Dc 0.30 m; normal stress -100 MPa; initial shear stress 58 MPa plus a
+    seeded Gaussian random field (std 3 MPa, correlation 1 km); 3 km square
+    nucleation patch at 1.02 mu_s |tn|; 10-node PML; final slip, slip rate,
+    shear traction and rupture time on the fault.  Smaller shapes keep the
+    physical sizes where they fit (region and patch clipped to the plane).
+    Returns (parameter dict, {file name: float32 array})."""
+    nx, ny, nz = shape
+    rng = np.random.default_rng([seed, 7])
+    ts = 58e6 + gaussian_field_2d((nx, nz), dx, 1000.0, 3e6, rng)
+    jc, lc = nx // 2, nz // 2
+    rj, rl = min(int(10000.0 / dx), nx // 2 - 2), min(int(5000.0 / dx), nz // 2 - 2)
+    half = max(1, min(int(1500.0 / dx), rj // 3, rl // 3))
+    ts[jc - half:jc + half, lc - half:lc + half] = 1.02 * 0.65 * 100e6
+    prm = {
+        'shape': [nx, ny, nz, nt], 'delta': [dx, dx, dx, dt],
+        'rho': [2670.0], 'vp': [6000.0], 'vs': [3464.0], 'gam': [0.0], 'hourglass': [1.0, 1.0],
+        'bc1': ['pml'] * 3, 'bc2': ['pml'] * 3, 'npml': 10,
+        'faultnormal': '+y', 'hypocenter': [float(jc), ny * 0.5 - 0.5, float(lc)], 'vrup': -1.0,
+        'mus': [1e4, ([[jc - rj, jc + rj], [lc - rl, lc + rl]], '=', 0.65)], 'mud': [0.5], 'dc': [0.3],
+        'tn': [-100e6], 'ts': [([], '=<', 'ts.bin')],
+        'itstats': 10, 'itio': 100,
+    }
+    for f in ('sum', 'svm', 'tsm', 'trup'):
+        prm[f] = [([[], [], -1], '=>', f + '.bin')]
+    return prm, {'ts.bin': np.ascontiguousarray(ts.T, dtype='<f4')}
+
+
+def stage_files(prm, files, d, realsize=4):
+    from coseis_b200 import sord
+    os.makedirs(d, exist_ok=True)
+    for f, a in files.items():
+        a.astype('<f8' if realsize == 8 else '<f4').tofile(os.path.join(d, f))
+    cwd = os.getcwd()
+    os.chdir(d)
+    try:
+        sord.stage(prm, realsize=realsize)
+    finally:
+        os.chdir(cwd)
+    return open(os.path.join(d, 'sord.in')).read()
+
+
+def run_config_bench(name, prm, files, steps, warmup, device, full_steps):
+    """Device node-updates/s of one configuration (its own handle, inputs
+    resident, CUDA events around one sord_step call of `steps` steps after
+    `warmup`), and end to end: sord_run_directory of the whole run
+    (`full_steps` steps, setup and output files included, host clock)."""
+    from coseis_b200 import _lib
+    nodes = float(np.prod(prm['shape'][:3]))
+    work = tempfile.mkdtemp(prefix='sord_%s_' % name)
+    try:
+        p = dict(prm)
+        p['shape'] = list(prm['shape'][:3]) + [warmup + steps]
+        text = stage_files(p, files, os.path.join(work, 'dev'))
+        s = _lib.Solver(os.path.join(work, 'dev'), text, device=device)
+        try:
+            s.step(warmup)
+            s.step(steps)
+            ms = s.last_step_ms()
+        finally:
+            s.close()
+        out = {'value': nodes * steps / (ms / 1e3), 'unit': 'node-updates/s', 'ms_per_step': ms / steps,
+               'nodes': int(nodes), 'timed_steps': steps}
+        if full_steps:
+            p = dict(prm)
+            p['shape'] = list(prm['shape'][:3]) + [full_steps]
+            stage_files(p, files, os.path.join(work, 'e2e'))
+            t0 = time.time()
+            _lib.run_directory(os.path.join(work, 'e2e'), device)
+            wall = time.time() - t0
+            out['e2e'] = {'value': nodes * full_steps / wall, 'unit': 'node-updates/s', 'steps': full_steps,
+                          'wall_s': round(wall, 3), 'includes': 'setup, all steps, output files, teardown'}
+        return out
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
+def oracle_config_rate(prm, files, steps, warmup, threads):
+    """CPU oracle node-updates/s on a configuration (steps after warm-up)."""
+    exe = oracle_exe()
+    work = tempfile.mkdtemp(prefix='sord_cpucfg_')
+    try:
+        p = dict(prm)
+        p['shape'] = list(prm['shape'][:3]) + [warmup + steps]
+        stage_files(p, files, work)
+        r = subprocess.run([exe, '--threads', str(threads), '--timed-from', str(warmup)], cwd=work,
+                           capture_output=True, text=True, timeout=1800)
+        if r.returncode:
+            raise RuntimeError(r.stderr[-2000:])
+        info = json.loads(r.stdout.strip().splitlines()[-1])
+        return float(np.prod(prm['shape'][:3])) * steps / info['timed_seconds']
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
+def run_other_configs(device, cpu=True):
+    """node-updates/s of the explosion (61^3, all 200 steps timed) and of the
+    600 x 300 x 300 rupture (30 steps after 5, of its 1500), each beside the
+    CPU oracle on all host threads on the same configuration (explosion: the
+    whole run; rupture: 2 steps after 1)."""
+    thr = os.cpu_count() or 1
+    res = {}
+    prm = explosion_prm()
+    r = run_config_bench('explosion', prm, {}, 200, 3, device, 200)
+    r['workload'] = 'explosion: 61^3 rectilinear nodes, 200 steps, moment source, 10-node PML, snapshots + 8 receivers'
+    if cpu:
+        r['cpu_oracle'] = {'value': oracle_config_rate(prm, {}, 199, 1, thr), 'cores': thr, 'steps': 199}
+    res['explosion'] = r
+    prm, files = rupture3_prm()
+    r = run_config_bench('rupture', prm, files, 30, 5, device, 0)
+    r['workload'] = ('rupture: 600x300x300 nodes, slip-weakening +y fault (20 x 10 km region, 3 km patch, '
+                     'seeded 3 MPa stress field), 10-node PML; 30 of 1500 steps timed')
+    if cpu:
+        r['cpu_oracle'] = {'value': oracle_config_rate(prm, files, 2, 1, thr), 'cores': thr, 'steps': 2}
+    res['rupture'] = r
+    return res
+
+
 # ------------------------------------------------------- adjoint
 def adjoint_problem(shape=(128, 128, 128), nt=1200, nrec=32, seed=SEED, segment=35):
     """The adjoint workload: 128^3 nodes, dx 100 m, dt 0.008 s, 1200 steps;
@@ -547,6 +694,9 @@ def run_ours(args):
         adj = None
         if ws == 1 and args.adjoint_steps > 0:
             adj = run_adjoint_bench(local, args.adjoint_steps)
+        cfgs = None
+        if ws == 1 and not args.no_configs:
+            cfgs = run_other_configs(local, cpu=not args.no_cpu)
     finally:
         shutil.rmtree(work, ignore_errors=True)
     if rank != 0:
@@ -568,8 +718,7 @@ def run_ours(args):
         'n_gpus': ws, 'steps': args.steps, 'warmup': args.warmup,
         'ms_per_step': ms_max / args.steps, 'higher_is_better': True, 'scaling': 'weak',
         'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic (seeded)',
-        'config': {'workload': 'wave226: %dx%dx%d nodes curvilinear terrain, layered von Karman medium, '
-                               '12-node PML on 5 faces, moment-tensor source, 64 receivers' % shape,
+        'config': {'workload': wave_workload(shape),
                    'nodes': int(nodes), 'dx_m': DX, 'dt_s': DT, 'parallelism': 'replicas' if ws > 1 else 'single',
                    'arithmetic': args.arithmetic,
                    'l2': 'inputs larger than L2 (%.1f GB resident)' % (nodes * 100 / 1e9),
@@ -586,6 +735,7 @@ def run_ours(args):
         'e2e': e2e,
         'ensemble': ens,
         'adjoint': adj,
+        'configs': cfgs,
     }
     if ws == 1 and not args.no_cpu:
         try:
@@ -658,13 +808,17 @@ def run_ensemble_bench(n, nthreads, device, nt=ENS_NT, seed=SEED):
         t0 = time.time()
         _lib.run_ensemble(ens, device, nthreads)
         t_ens = time.time() - t0
-        same = all(open(os.path.join(a, f), 'rb').read() == open(os.path.join(b, f), 'rb').read()
-                   for a, b in zip(ser, ens) for f in ('sum.bin', 'trup.bin'))
+        outs = [sorted(f for f in os.listdir(a) if f.endswith('.bin') and f != 'ts.bin') for a in ser]
+        same = all(o == sorted(f for f in os.listdir(b) if f.endswith('.bin') and f != 'ts.bin') and
+                   all(open(os.path.join(a, f), 'rb').read() == open(os.path.join(b, f), 'rb').read() for f in o)
+                   for a, b, o in zip(ser, ens, outs))
+        nfiles = sum(len(o) for o in outs)
         nodes = [int(np.prod(rupture_scenario(i, seed, nt)[0]['shape'][:3])) for i in range(n)]
         return {'metric': 'scenarios/s', 'value': n / t_ens, 'unit': 'scenarios/s',
                 'one_at_a_time': n / t_ser, 'speedup': t_ser / t_ens, 'scenarios': n,
                 'concurrent': nthreads, 'steps': nt, 'wall_s': round(t_ens, 3), 'serial_wall_s': round(t_ser, 3),
                 'node_updates_per_s': float(sum(nodes)) * nt / t_ens, 'outputs_identical': bool(same),
+                'files_compared': nfiles,
                 'arithmetic': os.environ.get('SORD_ARITHMETIC', 'reference'),
                 'workload': 'rupture ensemble: seeded grids 64x64x64..192x96x96, dx 100 m, dt 0.008 s, '
                             'slip-weakening +z fault, seeded friction / stresses (scenarios 0..%d)' % (n - 1)}
@@ -672,22 +826,72 @@ def run_ensemble_bench(n, nthreads, device, nt=ENS_NT, seed=SEED):
         shutil.rmtree(work, ignore_errors=True)
 
 
+def wave_workload(shape):
+    return ('wave226: %dx%dx%d nodes curvilinear terrain, layered von Karman medium, '
+            '12-node PML on 5 faces, moment-tensor source, 64 receivers' % tuple(shape))
+
+
+def host_memory_available():
+    try:
+        for line in open('/proc/meminfo'):
+            if line.startswith('MemAvailable:'):
+                return int(line.split()[1]) * 1024
+    except Exception:
+        pass
+    return 0
+
+
 def run_reference(args):
+    """The reference arm: the CPU oracle (the C++ OpenMP restatement of
+    sord/*.f90; the Fortran cannot be built here) on all host threads, on the
+    same workload as the GPU arm: the full mesh when the host holds it (23
+    FP32 arrays of the mesh with halos), timing --steps whole time steps
+    after --warmup (each about 20 s on 16 threads at 768 x 768 x 384);
+    otherwise the --cpu-shape sample for --steps steps."""
     ws = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))
     if rank != 0:
         return
     thr = os.cpu_count() or 1
-    shape_s = tuple(args.cpu_shape)
-    v, info = cpu_sample(shape_s, args.steps, args.warmup, thr)
-    sample = ('CPU oracle (C++ restatement of sord/*.f90, OpenMP) on the same workload at %dx%dx%d '
-              'nodes, %d timed steps after %d warm-up steps' % (shape_s + (args.steps, args.warmup)))
+    shape = tuple(args.shape)
+    need = 23 * 4 * float(np.prod([n + 2 for n in shape])) * 1.15 + 6e9
+    full = host_memory_available() >= need
+    if full:
+        steps = args.steps if args.ref_steps <= 0 else max(1, min(args.steps, args.ref_steps))
+        warm = args.warmup
+        exe = oracle_exe()
+        inputs = os.path.join(args.cache, 'wave_%dx%dx%d_%d_%g' % (shape + (SEED, args.hill)))
+        make_inputs(shape, inputs, hill=args.hill)
+        d = tempfile.mkdtemp(prefix='sord_ref_')
+        try:
+            stage_in(wave_prm(shape, warm + steps), d, inputs)
+            r = subprocess.run([exe, '--threads', str(thr), '--timed-from', str(warm)], cwd=d,
+                               capture_output=True, text=True, timeout=3600)
+            if r.returncode:
+                raise RuntimeError(r.stderr[-2000:])
+            info = json.loads(r.stdout.strip().splitlines()[-1])
+        finally:
+            shutil.rmtree(d, ignore_errors=True)
+        nodes = float(np.prod(shape))
+        v = nodes * steps / info['timed_seconds']
+        sample = ('CPU oracle (C++ restatement of sord/*.f90, OpenMP, %d threads) on the whole %dx%dx%d mesh: '
+                  '%d timed time steps after %d warm-up steps (setup %.0f s untimed)'
+                  % ((thr,) + shape + (steps, warm, info['seconds'] - info['timed_seconds'])))
+        cfg_shape = shape
+    else:
+        shape_s = tuple(args.cpu_shape)
+        steps = args.steps
+        v, info = cpu_sample(shape_s, args.steps, args.warmup, thr)
+        sample = ('CPU oracle on the same workload at %dx%dx%d nodes, %d timed steps after %d warm-up steps '
+                  '(the host has %.0f GB available, the whole mesh needs %.0f GB)'
+                  % (shape_s + (args.steps, args.warmup, host_memory_available() / 1e9, need / 1e9)))
+        cfg_shape = shape_s
     out = {
         'impl': 'reference', 'metric': 'node-updates/s', 'value': v, 'unit': 'node-updates/s',
-        'n_gpus': ws, 'steps': args.steps, 'warmup': args.warmup,
-        'ms_per_step': info['timed_seconds'] * 1e3 / args.steps, 'higher_is_better': True,
+        'n_gpus': ws, 'steps': steps, 'warmup': args.warmup,
+        'ms_per_step': float(np.prod(cfg_shape)) / v * 1e3, 'higher_is_better': True,
         'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic (seeded)',
-        'config': {'workload': 'wave226 sample %dx%dx%d' % shape_s, 'nodes': int(np.prod(shape_s))},
+        'config': {'workload': wave_workload(cfg_shape), 'nodes': int(np.prod(cfg_shape)), 'dx_m': DX, 'dt_s': DT},
         'cpu_baseline': {'value': v, 'unit': 'node-updates/s', 'cores': thr, 'kind': 'port', 'sample': sample},
         'e2e': {'value': v, 'unit': 'node-updates/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
     }
@@ -706,7 +910,10 @@ def main():
     ap.add_argument('--cache', default=os.environ.get('SORD_BENCH_CACHE', os.path.join(tempfile.gettempdir(), 'sord_bench')))
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu', action='store_true')
-    ap.add_argument('--ensemble', type=int, default=32, help='rupture-ensemble scenarios (0: skip)')
+    ap.add_argument('--ensemble', type=int, default=256, help='rupture-ensemble scenarios (0: skip)')
+    ap.add_argument('--no-configs', action='store_true', help='skip the explosion and rupture throughput lines')
+    ap.add_argument('--ref-steps', type=int, default=0,
+                    help='reference arm: cap on the timed steps of the full mesh (0: all --steps)')
     ap.add_argument('--ensemble-threads', type=int, default=8)
     ap.add_argument('--adjoint-steps', type=int, default=1200, help='adjoint workload steps (0: skip)')
     ap.add_argument('--hill', type=float, default=500.0, help='topography peak (m); 0 gives a rectilinear mesh')

@@ -1,0 +1,76 @@
+"""The benchmark configurations against the oracle.
+
+* The point-source explosion at its stated size (61^3 nodes, 200 steps,
+  10-node PML, snapshots of v on the k mid-plane every 10 steps and 8
+  interior receivers; bench.explosion_prm): in reference order the CUDA
+  solver is bit-identical to the FP32 oracle; in fast arithmetic every
+  output is within relative L2 1e-4 of the FP64 oracle.
+* The planar-fault rupture (bench.rupture3_prm: slip weakening, seeded
+  3 MPa stress field, nucleation patch, 10-node PML) on a 120 x 64 x 64
+  grid at dx 100 m for 400 steps (the rupture spreads over half the
+  fault in 2 s): bit-identical to the FP32 oracle in reference order;
+  in fast arithmetic slip and slip rate within relative L2 1e-4 of the FP64
+  oracle and rupture times within one time step.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import sordcases as sc
+from test_fast_arithmetic import floor_of, load, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _stage_all(tmp_path, prm, files):
+    import bench
+    dirs = {t: str(tmp_path / t) for t in ('o32', 'o64', 'ref', 'fast')}
+    for t, d in dirs.items():
+        bench.stage_files(prm, files, d, realsize=8 if t == 'o64' else 4)
+    return dirs
+
+
+def _check(dirs, prm, oracle_bins):
+    sc.run_oracle(dirs['o32'], oracle_bins['f32'], threads=os.cpu_count() or 1)
+    sc.run_oracle(dirs['o64'], oracle_bins['f64'], threads=os.cpu_count() or 1)
+    sc.run_gpu(dirs['ref'], arithmetic='reference')
+    sc.run_gpu(dirs['fast'], arithmetic='fast')
+    same = sc.compare(dirs['o32'], dirs['ref'])
+    skip = ('stats-e', 'stats-moment', 'stats-mw')
+    bad = {f: r for f, (r, exact) in same.items() if not exact and not f.startswith(skip)}
+    assert same and not bad, bad
+    errs = {}
+    dt = prm['delta'][3]
+    for f in sc.outputs(dirs['fast']):
+        if f.startswith('stats-'):
+            continue
+        b = load(dirs['o64'], f, '<f8')
+        a = load(dirs['fast'], f, '<f4')
+        if f in ('trup.bin', 'tarr.bin'):
+            m = (b < 1e8) | (a < 1e8)
+            assert np.all(np.abs(a[m] - b[m]) <= dt * (1 + 1e-6)), f
+            errs[f] = float(np.abs(a[m] - b[m]).max() / dt) if m.any() else 0.0
+            continue
+        fl = floor_of(dirs['o64'], f, '<f8')
+        errs[f] = (rel_l2(a, b, fl), rel_l2(load(dirs['o32'], f, '<f4'), b, fl))
+        assert errs[f][0] <= 1e-4, (f, errs[f])
+    return errs
+
+
+def test_explosion_config(tmp_path, oracle_bins, gpu_lib):
+    import bench
+    prm = bench.explosion_prm()
+    dirs = _stage_all(tmp_path, prm, {})
+    errs = _check(dirs, prm, oracle_bins)
+    print('explosion 61^3 x 200:', {f: ('%.1e' % e[0], '%.1e' % e[1]) for f, e in sorted(errs.items())})
+
+
+def test_rupture_config_reduced(tmp_path, oracle_bins, gpu_lib):
+    import bench
+    prm, files = bench.rupture3_prm(nt=400, shape=(120, 64, 64), dx=100.0, dt=0.008)
+    dirs = _stage_all(tmp_path, prm, files)
+    errs = _check(dirs, prm, oracle_bins)
+    trup = load(dirs['o64'], 'trup.bin', '<f8')
+    assert (trup < 1e8).mean() > 0.05, 'the rupture did not spread'
+    print('rupture 120x64x64 x 400:', errs)
