@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, 'csrc')
 LIB = os.path.join(HERE, 'libsordgpu.so')
 SOURCES = ['api.cu', 'kernels.cu', 'fused.cu', 'setup.cu', 'fault.cu', 'fieldio.cu', 'util.cu', 'noalloc.cu', 'adjoint.cu']
-HEADERS = ['sord.cuh', 'stencil.cuh', 'inject.cuh', 'timefn.h']
+HEADERS = ['sord.cuh', 'stencil.cuh', 'inject.cuh', 'timefn.h', 'slab.cuh']
 NVCC = os.environ.get('NVCC', '/usr/local/cuda/bin/nvcc')
 FLAGS = [
     '-std=c++17', '-O3', '-lineinfo',

@@ -33,6 +33,7 @@
 // once and shared by the cell's gradient and its eight corner nodes'
 // divergence (stencil.cuh: cell_cn_brackets).
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <type_traits>
 #include <utility>
@@ -1631,6 +1632,14 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
 #undef HVALS
 }
 
+#include "slab.cuh"
+
+// A region of shell items made by one push_box call: boxes of 15 x 15
+// nodes from (j1, k1) and ipl planes from l1, l outermost, j innermost.
+struct BoxRegion {
+    int j1, k1, l1, j2, k2, l2, ipl, nbj, nbk, nbl, first;
+};
+
 // Work decomposition of a fused step, fixed by the mesh.  The interior
 // rectangle holds the node columns (j, k) whose adjacent cells all lie
 // strictly inside the non-PML region, jf..jend x kf..kend; it is tiled by
@@ -1648,6 +1657,8 @@ struct FusedPlan {
     int segl = 0, nseg = 1;                     // interior planes per block, blocks per column
     int ipl = 96;                               // deepest shell item
     std::vector<int> base;                      // shell items without point sources (6 ints each)
+    std::vector<int> bmask;                     // per base item: k_slab class (0..3: MASK 1, 2, 4, 7)
+    std::vector<BoxRegion> regions;             // how the base items were laid out
     std::vector<int> cur;                       // items of the last upload
     int* d_items = nullptr;
     int* h_items = nullptr;                     // pinned staging
@@ -1681,8 +1692,12 @@ static constexpr int kMinPlanes = 8;
 static constexpr int kWaveBlocks = 4;
 
 // shell items covering node box [j1, j2] x [k1, k2] x [l1, l2]
-static void push_box(std::vector<int>& v, int ipl, int j1, int j2, int k1, int k2, int l1, int l2) {
+static void push_box(std::vector<int>& v, int ipl, int j1, int j2, int k1, int k2, int l1, int l2,
+                     std::vector<BoxRegion>* reg = nullptr) {
     if (j1 > j2 || k1 > k2 || l1 > l2) return;
+    if (reg)
+        reg->push_back({j1, k1, l1, j2, k2, l2, ipl, (j2 - j1) / (SJ - 1) + 1, (k2 - k1) / (SK - 1) + 1,
+                        (l2 - l1) / ipl + 1, (int)v.size() / 6});
     for (int a = l1; a <= l2; a += ipl)
         for (int k = k1; k <= k2; k += SK - 1)
             for (int j = j1; j <= j2; j += SJ - 1) {
@@ -1721,17 +1736,28 @@ static FusedPlan& fused_plan(Solver& s) {
     int sms = 148;
     SORD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s.device));
     const int want = kWaveBlocks * sms;
+    // boxes of the shell, cut where the PML of another axis begins so that
+    // each box is damped along as few axes as possible (the k_slab class)
     auto shell = [&](int ipl) {
         std::vector<int> v;
+        std::vector<BoxRegion>* r = &P->regions;
+        r->clear();
         if (!inner) {
-            push_box(v, ipl, g.i1node[0], g.i2node[0], g.i1node[1], g.i2node[1], L1, L2);
+            push_box(v, ipl, g.i1node[0], g.i2node[0], g.i1node[1], g.i2node[1], L1, L2, r);
         } else {
-            push_box(v, ipl, g.i1node[0], P->jf - 1, g.i1node[1], g.i2node[1], L1, L2);
-            push_box(v, ipl, P->jend + 1, g.i2node[0], g.i1node[1], g.i2node[1], L1, L2);
-            push_box(v, ipl, P->jf, P->jend, g.i1node[1], P->kf - 1, L1, L2);
-            push_box(v, ipl, P->jf, P->jend, P->kend + 1, g.i2node[1], L1, L2);
-            push_box(v, ipl, P->jf, P->jend, P->kf, P->kend, L1, P->lf0 - 1);
-            push_box(v, ipl, P->jf, P->jend, P->kf, P->kend, P->lf1 + 1, L2);
+            const int kr[3][2] = {{g.i1node[1], P->kf - 1}, {P->kf, P->kend}, {P->kend + 1, g.i2node[1]}};
+            const int lr[3][2] = {{L1, P->lf0 - 1}, {P->lf0, P->lf1}, {P->lf1 + 1, L2}};
+            for (int a = 0; a < 3; a++)
+                for (int b = 0; b < 3; b++) {
+                    push_box(v, ipl, g.i1node[0], P->jf - 1, kr[a][0], kr[a][1], lr[b][0], lr[b][1], r);
+                    push_box(v, ipl, P->jend + 1, g.i2node[0], kr[a][0], kr[a][1], lr[b][0], lr[b][1], r);
+                }
+            for (int b = 0; b < 3; b++) {
+                push_box(v, ipl, P->jf, P->jend, g.i1node[1], P->kf - 1, lr[b][0], lr[b][1], r);
+                push_box(v, ipl, P->jf, P->jend, P->kend + 1, g.i2node[1], lr[b][0], lr[b][1], r);
+            }
+            push_box(v, ipl, P->jf, P->jend, P->kf, P->kend, L1, P->lf0 - 1, r);
+            push_box(v, ipl, P->jf, P->jend, P->kf, P->kend, P->lf1 + 1, L2, r);
         }
         return v;
     };
@@ -1740,6 +1766,21 @@ static FusedPlan& fused_plan(Solver& s) {
     while (P->ipl > kMinPlanes && (int)P->base.size() / 6 < want) {
         P->ipl = std::max(kMinPlanes, P->ipl * 2 / 3);
         P->base = shell(P->ipl);
+    }
+    // k_slab class of each box: axis d needs the PML terms when a real cell
+    // the box computes (node range a..b -> cells a-1..b) or one of its real
+    // nodes lies in a PML slab of d; one axis -> its own class, more -> all
+    for (size_t i = 0; i < P->base.size(); i += 6) {
+        const int* b = &P->base[i];
+        const int lo[3] = {b[0], b[1], b[4]}, hi[3] = {b[2], b[3], b[5]};
+        int m = 0;
+        for (int d = 0; d < 3; d++) {
+            for (int c = std::max(lo[d] - 1, g.i1cell[d]); c <= std::min(hi[d], g.i2cell[d]); c++)
+                if (c <= g.i1pml[d] || c >= g.i2pml[d] - 1) m |= 1 << d;
+            for (int c = std::max(lo[d], g.i1node[d]); c <= std::min(hi[d], g.i2node[d]); c++)
+                if (c <= g.i1pml[d] || c >= g.i2pml[d]) m |= 1 << d;
+        }
+        P->bmask.push_back(m == 2 ? 1 : m == 4 ? 2 : (m == 0 || m == 1) ? 0 : 3);
     }
     if (!inner) {
         P->jend = P->jf - 1;
@@ -1799,6 +1840,29 @@ static void launch_mode(Solver& s, const StepArgs& A, dim3 grid, cudaStream_t st
     }
     s.launches++;
     SORD_CUDA(cudaGetLastError());
+}
+
+template <int GEOM, int MASK>
+static void launch_slab_m(Solver& s, const StepArgs& A, unsigned n, cudaStream_t st) {
+    const size_t bytes = LaySl<GEOM>::bytes;
+    smem_limit((const void*)k_slab<GEOM, MASK>, (int)bytes);
+    k_slab<GEOM, MASK><<<dim3(n, 1, 1), dim3(SJ, SK), bytes, st>>>(A);
+    s.launches++;
+    SORD_CUDA(cudaGetLastError());
+}
+
+template <int GEOM>
+static void launch_slab_g(Solver& s, const StepArgs& A, int cls, unsigned n, cudaStream_t st) {
+    if (cls == 0) launch_slab_m<GEOM, 1>(s, A, n, st);
+    else if (cls == 1) launch_slab_m<GEOM, 2>(s, A, n, st);
+    else if (cls == 2) launch_slab_m<GEOM, 4>(s, A, n, st);
+    else launch_slab_m<GEOM, 7>(s, A, n, st);
+}
+
+static void launch_slab(Solver& s, const StepArgs& A, int cls, unsigned n, cudaStream_t st) {
+    if (s.geom == GEOM_RECT) launch_slab_g<GEOM_RECT>(s, A, cls, n, st);
+    else if (s.geom == GEOM_TERRAIN) launch_slab_g<GEOM_TERRAIN>(s, A, cls, n, st);
+    else launch_slab_g<GEOM_GENERAL>(s, A, cls, n, st);
 }
 
 template <bool FASTK>
@@ -1866,11 +1930,59 @@ void launch_fused(Solver& s, const InjectList& pot, const InjectList& mom, const
         std::sort(src.begin(), src.end());
         src.erase(std::unique(src.begin(), src.end()), src.end());
     }
-    std::vector<int> items(P.base);
+    // In fast arithmetic the boxes without a point source go to k_slab, by
+    // class; k_shell takes the rest (the boxes k_shell tests: cells
+    // j0-1..j0+14 for potency / moment entries, nodes j0..j0+14 for forces).
+    // Upload order: k_shell items, then the k_slab classes.
+    const int nbase = (int)P.base.size() / 6;
+    std::vector<char> hit(nbase, s.arith ? 0 : 1);
+    if (s.arith) {
+        // an entry at (j, k, l) reaches box (j0, k0, L0..L1) when
+        // j0 - o <= j <= j0 + 14 (o = 1 for cells), likewise k, and
+        // L0 - o <= l <= L1: at most two boxes per axis in each region
+        auto mark = [&](const std::vector<Inject>& e, bool cell) {
+            const int o = cell ? 1 : 0;
+            auto span = [](int x, int x1, int step, int n, int lo, int hi, int& a, int& b) {
+                // boxes i (origin x1 + step i) with origin + lo <= x <= origin + hi
+                a = std::max(0, (int)std::ceil((double)(x - hi - x1) / step));
+                b = std::min(n - 1, (int)std::floor((double)(x - lo - x1) / step));
+            };
+            for (const Inject& x : e) {
+                const int j = (int)(x.idx % s.g.sy) + 1, k = (int)((x.idx / s.g.sy) % s.g.nm[1]) + 1;
+                const int l = (int)(x.idx / s.g.sz) + 1;
+                for (const BoxRegion& r : P.regions) {
+                    int ja, jb, ka, kb, la, lb;
+                    span(j, r.j1, SJ - 1, r.nbj, -o, SJ - 2, ja, jb);
+                    span(k, r.k1, SK - 1, r.nbk, -o, SK - 2, ka, kb);
+                    span(l, r.l1, r.ipl, r.nbl, -o, r.ipl - 1, la, lb);
+                    for (int bl = la; bl <= lb; bl++)
+                        for (int bk = ka; bk <= kb; bk++)
+                            for (int bj = ja; bj <= jb; bj++) {
+                                const int i = r.first + (bl * r.nbk + bk) * r.nbj + bj;
+                                if (l <= P.base[6 * i + 5]) hit[i] = 1;
+                            }
+                }
+            }
+        };
+        mark(hpot, true);
+        mark(hmom, true);
+        mark(hforce, false);
+    }
+    std::vector<int> items;
+    for (int i = 0; i < nbase; i++)
+        if (hit[i]) items.insert(items.end(), P.base.begin() + 6 * i, P.base.begin() + 6 * i + 6);
     for (auto& c : src) {
         const int j0 = P.jf + c.first * FOJ, k0 = P.kf + c.second * FOK;
         push_box(items, P.ipl, j0, std::min(P.jend, j0 + FOJ - 1), k0, std::min(P.kend, k0 + FOK - 1), P.lf0, P.lf1);
     }
+    const int nshell = (int)items.size() / 6;
+    int nslab[4] = {0, 0, 0, 0};
+    for (int m = 0; m < 4; m++)
+        for (int i = 0; i < nbase; i++)
+            if (!hit[i] && P.bmask[i] == m) {
+                items.insert(items.end(), P.base.begin() + 6 * i, P.base.begin() + 6 * i + 6);
+                nslab[m]++;
+            }
     const int nitems = (int)items.size() / 6;
     if (items != P.cur) {
         if (nitems > P.cap) throw SordError(SORD_E_PARAM, "too many point-source tiles in one step");
@@ -1885,17 +1997,29 @@ void launch_fused(Solver& s, const InjectList& pot, const InjectList& mom, const
     s.prof_begin(KC_FUSED, &e0);
     const bool inner = P.nbx > 0 && P.nby > 0;
     const dim3 igrid(P.nbx, P.nby, P.nseg);
+    // the shell launches: k_shell, then each k_slab class
+    auto shell_launches = [&](cudaStream_t st) {
+        if (nshell > 0) launch_geom<false>(s, A, dim3((unsigned)nshell, 1, 1), st);
+        int off = nshell;
+        for (int m = 0; m < 4; m++) {
+            if (nslab[m] == 0) continue;
+            StepArgs B = A;
+            B.items = P.d_items + 6 * (size_t)off;
+            launch_slab(s, B, m, (unsigned)nslab[m], st);
+            off += nslab[m];
+        }
+    };
     if (inner && nitems > 0) {
         SORD_CUDA(cudaEventRecord(P.fork, s.stream));
         SORD_CUDA(cudaStreamWaitEvent(P.side, P.fork, 0));
-        launch_geom<false>(s, A, dim3((unsigned)nitems, 1, 1), P.side);
+        shell_launches(P.side);
         launch_geom<true>(s, A, igrid, s.stream);
         SORD_CUDA(cudaEventRecord(P.join, P.side));
         SORD_CUDA(cudaStreamWaitEvent(s.stream, P.join, 0));
     } else if (inner) {
         launch_geom<true>(s, A, igrid, s.stream);
     } else if (nitems > 0) {
-        launch_geom<false>(s, A, dim3((unsigned)nitems, 1, 1), s.stream);
+        shell_launches(s.stream);
     }
     s.prof_end(KC_FUSED, e0);
     if (fold) {
