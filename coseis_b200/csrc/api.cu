@@ -188,7 +188,7 @@ static bool tensor_point_ops(Solver& s, const char* const* names, std::vector<In
     return true;
 }
 
-static InjectList upload(Solver& s, int slot, const std::vector<Inject>& e) {
+InjectList upload_inject(Solver& s, int slot, const std::vector<Inject>& e) {
     if ((int)e.size() > kMaxInject) throw SordError(SORD_E_PARAM, "too many point injections in one step");
     if (e.empty()) return InjectList{s.d.inj + inj_off(slot, 0), 0};
     // a ring of staging buffers per slot: the copy that last used buffer r
@@ -217,7 +217,7 @@ void bare_step(Solver& s, int n, bool update, bool fold) {
     std::vector<Inject> pot, mom, frc;
     tensor_point_ops(s, kPot, pot);
     tensor_point_ops(s, kMom, mom);
-    InjectList lp = upload(s, 0, pot), lm = upload(s, 1, mom), lf = upload(s, 2, frc);
+    InjectList lp = upload_inject(s, 0, pot), lm = upload_inject(s, 1, mom), lf = upload_inject(s, 2, frc);
     launch_fused(s, lp, lm, lf, pot, mom, frc, fold, true, false);
     s.folded = fold;
 }
@@ -326,7 +326,7 @@ void Solver::step(bool last_in_call) {
     // the state after its last step
     const bool fold = !last_in_call && it < nt && fusable(it + 1);
     const bool write_a = any_pass(*this, kAcc, 3, '>') || field_active(*this, "am2", '>') || it == nt;
-    InjectList lp = upload(*this, 0, pot), lm = upload(*this, 1, mom), lf = upload(*this, 2, frc);
+    InjectList lp = upload_inject(*this, 0, pot), lm = upload_inject(*this, 1, mom), lf = upload_inject(*this, 2, frc);
     launch_fused(*this, lp, lm, lf, pot, mom, frc, fold, write_a, st);
     if (g.ifn) fault_rupture_fused(*this);
     folded = fold;
@@ -372,7 +372,7 @@ void Solver::step_general(bool st) {
     bool fuse = tensor_point_ops(*this, kPot, pot) && tensor_point_ops(*this, kMom, mom) && !any_pass(*this, kStr, 6, '<');
     float* sdso[6] = {d.sd[0], d.sd[1], d.sd[2], d.so[0], d.so[1], d.so[2]};
     if (fuse) {
-        InjectList lp = upload(*this, 0, pot), lm = upload(*this, 1, mom);
+        InjectList lp = upload_inject(*this, 0, pot), lm = upload_inject(*this, 1, mom);
         launch_stress(*this, lp, lm, true);
         for (int i = 0; i < 6; i++) io("<>", kStr[i], vol(*this, sdso[i]));
         if (st) wmax = read_max(*this, 3);
@@ -381,10 +381,10 @@ void Solver::step_general(bool st) {
         launch_stress(*this, none, none, false);
         pot.clear();
         mom.clear();
-        if (prm.source == "potency") { finite_source_entries(*this, pot); launch_inject(*this, sdso, upload(*this, 0, pot)); }
+        if (prm.source == "potency") { finite_source_entries(*this, pot); launch_inject(*this, sdso, upload_inject(*this, 0, pot)); }
         for (int i = 0; i < 6; i++) io("<>", kPot[i], vol(*this, sdso[i]));
         launch_hooke(*this);
-        if (prm.source == "moment") { finite_source_entries(*this, mom); launch_inject(*this, sdso, upload(*this, 1, mom)); }
+        if (prm.source == "moment") { finite_source_entries(*this, mom); launch_inject(*this, sdso, upload_inject(*this, 1, mom)); }
         for (int i = 0; i < 6; i++) io("<>", kMom[i], vol(*this, sdso[i]));
         launch_volume_scale(*this);
         for (int i = 0; i < 6; i++) io("<>", kStr[i], vol(*this, sdso[i]));
@@ -401,12 +401,12 @@ void Solver::step_general(bool st) {
     const bool ain = any_pass(*this, kAcc, 3, '<');
     const bool fuse_a = G.ifn == 0 && bc_noop(prm) && !any_pass(*this, kForce, 3, '<') && !any_pass(*this, kForce, 3, '>');
     if (fuse_a) {
-        launch_accel(*this, true, st && !ain, upload(*this, 2, frc));
+        launch_accel(*this, true, st && !ain, upload_inject(*this, 2, frc));
     } else {
         InjectList none{d.inj, 0};
         launch_accel(*this, false, false, none);
         float* w6[6] = {d.w1n[0], d.w1n[1], d.w1n[2], d.w1n[0], d.w1n[1], d.w1n[2]};
-        if (!frc.empty()) launch_inject(*this, w6, upload(*this, 2, frc));
+        if (!frc.empty()) launch_inject(*this, w6, upload_inject(*this, 2, frc));
         for (int i = 0; i < 3; i++) io("<", kForce[i], vol(*this, d.w1n[i]));
         launch_vector_bc(*this, d.w1n, prm.bc1, prm.bc2, G.i1bc, G.i2bc);
         if (G.ifn) fault_rupture(*this);
@@ -556,6 +556,7 @@ void Solver::prof_collect() {
 void Solver::destroy() {
     if (device >= 0) cudaSetDevice(device);
     if (stream) cudaStreamSynchronize(stream);
+    writer_free(*this);
     auto fr = [this](void* p) { dev_free(*this, p); };
     for (int i = 0; i < 3; i++) { fr(d.x[i]); fr(d.v[i]); fr(d.u[i]); fr(d.w1n[i]); fr(d.sd[i]); fr(d.so[i]); }
     fr(d.vc); fr(d.mr); fr(d.lam); fr(d.mu); fr(d.gam); fr(d.yy); fr(d.s1); fr(d.s2); fr(d.pmlc); fr(d.red); fr(d.inj); fr(d.fp);
@@ -662,6 +663,7 @@ int sord_step(sord_handle* h, int nsteps) {
         float ms = 0;
         SORD_CUDA(cudaEventElapsedTime(&ms, s.ev0, s.ev1));
         s.last_step_ms = ms;
+        writer_drain(s);
     } catch (const std::exception& e) {
         return fail(h, e);
     }
@@ -686,6 +688,7 @@ int sord_adjoint_forward(sord_handle* h, int segment) {
         float ms = 0;
         SORD_CUDA(cudaEventElapsedTime(&ms, s.ev0, s.ev1));
         s.last_step_ms = ms;
+        writer_drain(s);
     } catch (const std::exception& e) {
         return fail(h, e);
     }

@@ -12,16 +12,22 @@
 //                 buffers straight into a device record, checked for
 //                 NaN / Inf, staged into the volume scratch s1 and applied
 //                 on the device; other inputs (sub-cell '.<', strided or
-//                 half-dimension records, time-varying inputs) take the
-//                 host path: the field is copied down, the op applied with
-//                 the reference's buffer / interpolation / half-dimension
-//                 fill rules, and copied back
+//                 half-dimension records, time-varying inputs) read their
+//                 records on the host nb at a time (checked there), and
+//                 each record is copied to the device when its step comes
+//                 and applied there with the reference's staging,
+//                 interpolation and half-dimension fill rules: only the
+//                 file's records cross to the device
+//   output flush  records are copied into pinned buffers on the stream and
+//                 written to disk by a writer thread (write_async)
 #include <fcntl.h>
 #include <unistd.h>
 
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <condition_variable>
+#include <deque>
 #include <cstdio>
 #include <cstring>
 #include <limits>
@@ -163,6 +169,83 @@ __global__ void k_apply_in(float* f, const float* s1, Region R, int op) {
         else if (op == 1) f[q] = f[q] + a;
         else f[q] = f[q] * a;
     }
+}
+
+// One disk-input record (input_output.f90:392-398): the record, j fastest,
+// into the strided region of S.
+__global__ void k_rec_scatter(float* S, const float* rec, Region R) {
+    const long long c0 = (R.i2[0] - R.i1[0]) / R.di[0] + 1, c1 = (R.i2[1] - R.i1[1]) / R.di[1] + 1;
+    const long long c2 = (R.i2[2] - R.i1[2]) / R.di[2] + 1, n = c0 * c1 * c2;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int j = R.i1[0] + R.di[0] * (int)(t % c0), k = R.i1[1] + R.di[1] * (int)((t / c0) % c1);
+        const int l = R.i1[2] + R.di[2] * (int)(t / (c0 * c1));
+        S[(j - 1) + (long long)R.n[0] * ((k - 1) + (long long)R.n[1] * (l - 1))] = rec[t];
+    }
+}
+
+// Linear interpolation between strided samples along one axis
+// (utilities.f90:168-220), every i = 1..d-1 at once: positions j + i are
+// never samples, so no thread reads what another writes.  The loops, with
+// their bounds and steps, are the reference's: axis 0 steps l by di2 and k
+// by di1; axis 1 steps l by di0 (sic); axis 2 takes every k and j.
+__global__ void k_rec_interp(float* S, int n0, int n1, int axis, int d, int a10, int a11, int a12, int a20, int a21,
+                             int a22, int lstep, int kstep) {
+    const int jstep = axis == 0 ? d : 1;
+    const int kst = axis == 1 ? d : axis == 0 ? kstep : 1, lst = axis == 2 ? d : lstep;
+    const int jhi = axis == 0 ? a20 - d : a20, khi = axis == 1 ? a21 - d : a21, lhi = axis == 2 ? a22 - d : a22;
+    if (jhi < a10 || khi < a11 || lhi < a12) return;
+    const long long cj = (jhi - a10) / jstep + 1, ck = (khi - a11) / kst + 1, cl = (lhi - a12) / lst + 1;
+    const long long n = cj * ck * cl * (long long)(d - 1);
+    const float rd = 1.0f / (float)d;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int i = 1 + (int)(t % (d - 1));
+        const long long u = t / (d - 1);
+        const int j = a10 + jstep * (int)(u % cj), k = a11 + kst * (int)((u / cj) % ck), l = a12 + lst * (int)(u / (cj * ck));
+        const float h1 = rd * (float)i, h2 = rd * (float)(d - i);
+        auto at = [&](int jj, int kk, int ll) -> float& {
+            return S[(jj - 1) + (long long)n0 * ((kk - 1) + (long long)n1 * (ll - 1))];
+        };
+        if (axis == 0) at(j + i, k, l) = h1 * at(j, k, l) + h2 * at(j + d, k, l);
+        else if (axis == 1) at(j, k + i, l) = h1 * at(j, k, l) + h2 * at(j, k + d, l);
+        else at(j, k, l + i) = h1 * at(j, k, l) + h2 * at(j, k, l + d);
+    }
+}
+
+// Half-dimension fill (input_output.f90:399-405): plane 1 of `axis` copied
+// along the whole extent of that axis.
+__global__ void k_rec_fill(float* S, int n0, int n1, int n2, int axis) {
+    const int na = axis == 0 ? n0 : axis == 1 ? n1 : n2;
+    const long long plane = (long long)n0 * n1 * n2 / na, n = plane * (na - 1);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int a = 2 + (int)(t / plane);
+        const long long r = t % plane;
+        long long q, q1;
+        if (axis == 0) {
+            q1 = r * n0;
+            q = q1 + (a - 1);
+        } else if (axis == 1) {
+            const long long j = r % n0, l = r / n0;
+            q1 = j + (long long)n0 * n1 * l;
+            q = q1 + (long long)n0 * (a - 1);
+        } else {
+            q1 = r;
+            q = r + (long long)n0 * n1 * (a - 1);
+        }
+        S[q] = S[q1];
+    }
+}
+
+// '.<': the record value times each trilinear weight added to the field
+// (input_output.f90:378-390); weights from the host, in its order of
+// operations
+struct PointIn {
+    long long idx[8];
+    float r[8];
+    int n;
+};
+__global__ void k_point_in(float* f, PointIn P, const float* v) {
+    const int t = threadIdx.x;
+    if (t < P.n) f[P.idx[t]] = f[P.idx[t]] + P.r[t] * v[0];
 }
 
 // ------------------------------------------------------------ host
@@ -382,6 +465,112 @@ void probes_free(Solver& s) {
     }
 }
 
+// Output records go to disk on a writer thread per handle: a flush copies
+// the device record buffer into a pinned buffer on the solver's stream and
+// queues the write behind an event, so the stream never waits for the
+// disk; the writer takes the jobs in order (so each file's records are
+// written in order), waits for each copy, writes and returns the buffer.
+// Errors are kept and reported by writer_drain.
+struct OutJob {
+    size_t opi;
+    float* pin;
+    cudaEvent_t ev;
+    int recl, nrec, m, o;
+    std::string filename;
+};
+struct OutWriter {
+    std::thread th;
+    std::mutex mu;
+    std::condition_variable cv, idle;
+    std::deque<OutJob> q;
+    bool stop = false, busy = false;
+    int code = 0;
+    std::string msg;
+};
+
+static void writer_loop(Solver* s, OutWriter* w) {
+    cudaSetDevice(s->device);
+    for (;;) {
+        OutJob job;
+        {
+            std::unique_lock<std::mutex> lock(w->mu);
+            w->cv.wait(lock, [&] { return w->stop || !w->q.empty(); });
+            if (w->q.empty()) return;
+            job = std::move(w->q.front());
+            w->q.pop_front();
+            w->busy = true;
+        }
+        int code = 0;
+        std::string msg;
+        try {
+            SORD_CUDA(cudaEventSynchronize(job.ev));
+            file_write(*s, s->ops[job.opi], job.pin, job.recl, job.nrec, job.filename, job.m, job.o);
+        } catch (const SordError& e) {
+            code = e.code;
+            msg = e.what();
+        } catch (const std::exception& e) {
+            code = SORD_E_IO;
+            msg = e.what();
+        }
+        cudaEventDestroy(job.ev);
+        pinned_put(job.pin);
+        std::lock_guard<std::mutex> lock(w->mu);
+        if (code && !w->code) { w->code = code; w->msg = msg; }
+        w->busy = false;
+        if (w->q.empty()) w->idle.notify_all();
+    }
+}
+
+// Wait until every queued record is on disk; throw the first write error.
+void writer_drain(Solver& s) {
+    OutWriter* w = s.writer;
+    if (!w) return;
+    std::unique_lock<std::mutex> lock(w->mu);
+    w->idle.wait(lock, [&] { return w->q.empty() && !w->busy; });
+    if (w->code) {
+        const int c = w->code;
+        w->code = 0;
+        throw SordError(c, w->msg);
+    }
+}
+
+void writer_free(Solver& s) {
+    OutWriter* w = s.writer;
+    if (!w) return;
+    {
+        std::lock_guard<std::mutex> lock(w->mu);
+        w->stop = true;
+    }
+    w->cv.notify_all();
+    if (w->th.joinable()) w->th.join();
+    delete w;
+    s.writer = nullptr;
+}
+
+static void write_async(Solver& s, IoOp& io, int nrec, const std::string& filename, int m, int o) {
+    if (!s.writer) {
+        s.writer = new OutWriter();
+        s.writer->th = std::thread(writer_loop, &s, s.writer);
+    }
+    OutJob job;
+    job.opi = (size_t)(&io - s.ops.data());
+    job.recl = io.bufn;
+    job.nrec = nrec;
+    job.m = m;
+    job.o = o;
+    job.filename = filename;
+    const size_t bytes = sizeof(float) * (size_t)io.bufn * nrec;
+    job.pin = (float*)pinned_get(bytes);
+    SORD_CUDA(cudaMemcpyAsync(job.pin, io.dbuf, bytes, cudaMemcpyDeviceToHost, s.stream));
+    SORD_CUDA(cudaEventCreateWithFlags(&job.ev, cudaEventDisableTiming));
+    SORD_CUDA(cudaEventRecord(job.ev, s.stream));
+    {
+        std::lock_guard<std::mutex> lock(s.writer->mu);
+        s.writer->q.push_back(std::move(job));
+    }
+    s.writer->cv.notify_one();
+}
+
 static void flush_output(Solver& s, IoOp& io, int n3[3], int m3[3]) {
     int it1 = io.ii[3][0], it2 = io.ii[3][1], dit = io.ii[3][2];
     int n4 = io.ib;
@@ -389,12 +578,7 @@ static void flush_output(Solver& s, IoOp& io, int n3[3], int m3[3]) {
     int o4 = (s.it - it1) / dit + 1 - n4;
     std::string filename = io.fname;
     if ((n3[0] != m3[0] || n3[1] != m3[1] || n3[2] != m3[2]) && s.prm.mpout == 0) filename += "-000000";
-    if (!(n3[0] < 1 || n3[1] < 1 || n3[2] < 1 || n4 < 1)) {
-        io.hbuf.resize((size_t)io.bufn * n4);
-        SORD_CUDA(cudaMemcpyAsync(io.hbuf.data(), io.dbuf, sizeof(float) * (size_t)io.bufn * n4, cudaMemcpyDeviceToHost, s.stream));
-        SORD_CUDA(cudaStreamSynchronize(s.stream));
-        file_write(s, io, io.hbuf.data(), io.bufn, n4, filename, m4, o4);
-    }
+    if (!(n3[0] < 1 || n3[1] < 1 || n3[2] < 1 || n4 < 1)) write_async(s, io, n4, filename, m4, o4);
     io.ib = 0;
     if (s.it == it2 || n3[0] < 1 || n3[1] < 1 || n3[2] < 1 || n4 < 1) {
         dev_free(s, io.dbuf);
@@ -461,6 +645,26 @@ static void read_to_device(Solver& s, const std::string& fn, size_t off, size_t 
     if (err == 2) SORD_CUDA(cudaGetLastError());
 }
 
+// Copy `count` floats of host memory to device memory `dst` on the solver's
+// stream through the pinned chunk buffers, so that the copy is queued
+// behind the stream's work instead of waiting for it (a pageable source
+// would); a chunk buffer is refilled once its previous copy has run.
+static void upload_record(Solver& s, const float* src, size_t count, float* dst) {
+    for (size_t c = 0; c * kChunk < count; c++) {
+        const int t = s.rec_slot;
+        s.rec_slot = (s.rec_slot + 1) % kReaders;
+        if (!s.pin_io[t]) {
+            s.pin_io[t] = (float*)pinned_get(sizeof(float) * kChunk);
+            SORD_CUDA(cudaEventCreateWithFlags(&s.pin_ev[t], cudaEventDisableTiming));
+        }
+        SORD_CUDA(cudaEventSynchronize(s.pin_ev[t]));
+        const size_t want = std::min(kChunk, count - c * kChunk);
+        std::memcpy(s.pin_io[t], src + c * kChunk, sizeof(float) * want);
+        SORD_CUDA(cudaMemcpyAsync(dst + c * kChunk, s.pin_io[t], sizeof(float) * want, cudaMemcpyHostToDevice, s.stream));
+        SORD_CUDA(cudaEventRecord(s.pin_ev[t], s.stream));
+    }
+}
+
 // Device path of disk input for one whole-volume record with unit stride
 // and no half-dimension fill, read once (static inputs).  Same semantics as
 // the host path below: s1 keeps the staged record, f gets the op.
@@ -504,7 +708,8 @@ static bool device_volume_input(Solver& s, IoOp& io, FieldView f, const int* i1,
     return true;
 }
 
-// host-side disk input (input_output.f90:296-437)
+// disk input (input_output.f90:296-437): records read on the host in
+// batches of nb, each applied on the device when its step comes
 static void disk_input(Solver& s, IoOp& io, FieldView f, int* i1, int* i2, int* di, int* m, int* n, int* o, const PointGeom* P) {
     const Geom& g = s.g;
     int it1 = io.ii[3][0], it2 = io.ii[3][1], dit = io.ii[3][2];
@@ -543,32 +748,46 @@ static void disk_input(Solver& s, IoOp& io, FieldView f, int* i1, int* i2, int* 
     }
     io.ib = io.ib + 1;
     const float* buf = io.hbuf.data() + (size_t)io.bufn * (io.ib - 1);
-    // bring the field to the host
-    size_t fsz = (size_t)f.n[0] * f.n[1] * f.n[2];
-    std::vector<float> F(fsz);
-    SORD_CUDA(cudaMemcpyAsync(F.data(), f.p, sizeof(float) * fsz, cudaMemcpyDeviceToHost, s.stream));
-    SORD_CUDA(cudaStreamSynchronize(s.stream));
-    auto at = [&](std::vector<float>& A, int j, int k, int l) -> float& {
-        return A[(size_t)(j - 1) + (size_t)f.n[0] * ((size_t)(k - 1) + (size_t)f.n[1] * (size_t)(l - 1))];
-    };
+    // on the device: only the record crosses to it
+    const size_t fsz = (size_t)f.n[0] * f.n[1] * f.n[2];
+    const bool volume = f.n[0] == g.nm[0] && f.n[1] == g.nm[1] && f.n[2] == g.nm[2];
+    // S: the volume scratch s1 for volume fields (the reference stages the
+    // record there, and s1 keeps it), else a zeroed temporary after the
+    // record; a field that is s1 itself also takes the temporary, and ends
+    // as its old values op S like the reference's (F op S, then f = F)
+    const bool in_s1 = volume && f.p != s.d.s1;
+    const size_t need = (size_t)nsp + (in_s1 ? 0 : fsz) + 1;
+    if (s.stage_cap < need) {
+        dev_free(s, s.d_stage);
+        s.d_stage = nullptr;
+        s.stage_cap = 0;
+        if (dev_malloc(s, (void**)&s.d_stage, sizeof(float) * need) != cudaSuccess) {
+            cudaGetLastError();
+            throw SordError(SORD_E_NOMEM, "cannot allocate the input staging record");
+        }
+        s.stage_cap = need;
+    }
+    upload_record(s, buf, (size_t)nsp, s.d_stage);
     if (io.op == ".<") {
+        PointIn pin{};
         for (int l = i1[2]; l <= i2[2]; l++)
             for (int k = i1[1]; k <= i2[1]; k++)
                 for (int j = i1[0]; j <= i2[0]; j++) {
-                    float r = wgt(P->xi[0], j, P->plane[0]) * wgt(P->xi[1], k, P->plane[1]) * wgt(P->xi[2], l, P->plane[2]);
-                    at(F, j, k, l) = at(F, j, k, l) + r * buf[0];
+                    pin.idx[pin.n] = (long long)(j - 1) + (long long)f.n[0] * ((long long)(k - 1) + (long long)f.n[1] * (long long)(l - 1));
+                    pin.r[pin.n] = wgt(P->xi[0], j, P->plane[0]) * wgt(P->xi[1], k, P->plane[1]) * wgt(P->xi[2], l, P->plane[2]);
+                    pin.n++;
                 }
+        k_point_in<<<1, 32, 0, s.stream>>>(f.p, pin, s.d_stage);
+        FCHK(s);
     } else {
-        std::vector<float> S(fsz, 0.f);
-        if (f.n[0] == g.nm[0] && f.n[1] == g.nm[1] && f.n[2] == g.nm[2]) {
-            // the reference stages through the volume scratch s1: keep its contents
-            SORD_CUDA(cudaMemcpyAsync(S.data(), s.d.s1, sizeof(float) * fsz, cudaMemcpyDeviceToHost, s.stream));
-            SORD_CUDA(cudaStreamSynchronize(s.stream));
-        }
-        size_t q = 0;
-        for (int l = i1[2]; l <= i2[2]; l += di[2])
-            for (int k = i1[1]; k <= i2[1]; k += di[1])
-                for (int j = i1[0]; j <= i2[0]; j += di[0]) at(S, j, k, l) = buf[q++];
+        float* S = in_s1 ? s.d.s1 : s.d_stage + nsp;
+        if (!in_s1) SORD_CUDA(cudaMemsetAsync(S, 0, sizeof(float) * fsz, s.stream));
+        Region R;
+        for (int i = 0; i < 3; i++) { R.n[i] = f.n[i]; R.i1[i] = i1[i]; R.i2[i] = i2[i]; R.di[i] = di[i]; }
+        R.vsy = g.sy;
+        R.vsz = g.sz;
+        k_rec_scatter<<<gf((long long)nsp), 256, 0, s.stream>>>(S, s.d_stage, R);
+        FCHK(s);
         if (di[0] > 1 || di[1] > 1 || di[2] > 1) {
             // utilities.f90:168-220
             int a1[3], a2[3];
@@ -577,45 +796,34 @@ static void disk_input(Solver& s, IoOp& io, FieldView f, int* i1, int* i2, int* 
                 if (a1[i] < 1) a1[i] = a1[i] + (-a1[i] / di[i] + 1) * di[i];
                 if (a2[i] > f.n[i]) a2[i] = a1[i] + (f.n[i] - a1[i]) / di[i] * di[i];
             }
-            int d = di[0];
-            for (int i = 1; i <= d - 1; i++) {
-                float h1 = 1.0f / (float)d * (float)i, h2 = 1.0f / (float)d * (float)(d - i);
-                for (int l = a1[2]; l <= a2[2]; l += di[2])
-                    for (int k = a1[1]; k <= a2[1]; k += di[1])
-                        for (int j = a1[0]; j <= a2[0] - d; j += d) at(S, j + i, k, l) = h1 * at(S, j, k, l) + h2 * at(S, j + d, k, l);
-            }
-            d = di[1];
-            for (int i = 1; i <= d - 1; i++) {
-                float h1 = 1.0f / (float)d * (float)i, h2 = 1.0f / (float)d * (float)(d - i);
-                for (int l = a1[2]; l <= a2[2]; l += di[0])
-                    for (int k = a1[1]; k <= a2[1] - d; k += d)
-                        for (int j = a1[0]; j <= a2[0]; j++) at(S, j, k + i, l) = h1 * at(S, j, k, l) + h2 * at(S, j, k + d, l);
-            }
-            d = di[2];
-            for (int i = 1; i <= d - 1; i++) {
-                float h1 = 1.0f / (float)d * (float)i, h2 = 1.0f / (float)d * (float)(d - i);
-                for (int l = a1[2]; l <= a2[2] - d; l += d)
-                    for (int k = a1[1]; k <= a2[1]; k++)
-                        for (int j = a1[0]; j <= a2[0]; j++) at(S, j, k, l + i) = h1 * at(S, j, k, l) + h2 * at(S, j, k, l + d);
+            for (int axis = 0; axis < 3; axis++) {
+                const int d = di[axis];
+                if (d <= 1) continue;
+                k_rec_interp<<<gf((long long)fsz), 256, 0, s.stream>>>(S, f.n[0], f.n[1], axis, d, a1[0], a1[1], a1[2],
+                                                                       a2[0], a2[1], a2[2], axis == 0 ? di[2] : di[0], di[1]);
+                FCHK(s);
             }
         }
-        if (m[0] == 1) { i2[0] = f.n[0]; for (int l = 1; l <= f.n[2]; l++) for (int k = 1; k <= f.n[1]; k++) for (int j = 2; j <= i2[0]; j++) at(S, j, k, l) = at(S, 1, k, l); }
-        if (m[1] == 1) { i2[1] = f.n[1]; for (int l = 1; l <= f.n[2]; l++) for (int k = 2; k <= i2[1]; k++) for (int j = 1; j <= f.n[0]; j++) at(S, j, k, l) = at(S, j, 1, l); }
-        if (m[2] == 1) { i2[2] = f.n[2]; for (int l = 2; l <= i2[2]; l++) for (int k = 1; k <= f.n[1]; k++) for (int j = 1; j <= f.n[0]; j++) at(S, j, k, l) = at(S, j, k, 1); }
-        for (int l = i1[2]; l <= i2[2]; l++)
-            for (int k = i1[1]; k <= i2[1]; k++)
-                for (int j = i1[0]; j <= i2[0]; j++) {
-                    if (io.op == "=<") at(F, j, k, l) = at(S, j, k, l);
-                    else if (io.op == "+<") at(F, j, k, l) = at(F, j, k, l) + at(S, j, k, l);
-                    else if (io.op == "*<") at(F, j, k, l) = at(F, j, k, l) * at(S, j, k, l);
-                    else throw SordError(SORD_E_PARAM, "bad i/o op");
+        for (int axis = 0; axis < 3; axis++)
+            if (m[axis] == 1) {
+                i2[axis] = f.n[axis];
+                if (f.n[axis] > 1) {
+                    k_rec_fill<<<gf((long long)fsz), 256, 0, s.stream>>>(S, f.n[0], f.n[1], f.n[2], axis);
+                    FCHK(s);
                 }
-        if (f.n[0] == g.nm[0] && f.n[1] == g.nm[1] && f.n[2] == g.nm[2]) {
-            SORD_CUDA(cudaMemcpyAsync(s.d.s1, S.data(), sizeof(float) * fsz, cudaMemcpyHostToDevice, s.stream));
+            }
+        const int code = io.op == "=<" ? 0 : io.op == "+<" ? 1 : io.op == "*<" ? 2 : -1;
+        if (code < 0) throw SordError(SORD_E_PARAM, "bad i/o op");
+        Region A;
+        for (int i = 0; i < 3; i++) { A.n[i] = f.n[i]; A.i1[i] = i1[i]; A.i2[i] = i2[i]; A.di[i] = 1; }
+        A.vsy = g.sy;
+        A.vsz = g.sz;
+        const long long na = (long long)(i2[0] - i1[0] + 1) * (i2[1] - i1[1] + 1) * (i2[2] - i1[2] + 1);
+        if (na > 0) {
+            k_apply_in<<<gf(na), 256, 0, s.stream>>>(f.p, S, A, code);
+            FCHK(s);
         }
     }
-    SORD_CUDA(cudaMemcpyAsync(f.p, F.data(), sizeof(float) * fsz, cudaMemcpyHostToDevice, s.stream));
-    SORD_CUDA(cudaStreamSynchronize(s.stream));
     region_scalar_bc(s, io, f);
     if (s.it == it2) { io.hbuf.clear(); io.op = "#"; }
 }
@@ -649,15 +857,8 @@ static void field_io_op(Solver& s, size_t opi, FieldView f, ProbeBatch& batch) {
             std::vector<Inject> e;
             point_injection(s, io, f, 0, e);
             if (!e.empty()) {
-                if ((int)e.size() > kMaxInject) throw SordError(SORD_E_PARAM, "too many point injections");
-                Inject* h = s.hinj + inj_off(3, 0);
-                std::memcpy(h, e.data(), sizeof(Inject) * e.size());
-                Inject* dptr = s.d.inj + inj_off(3, 0);
-                SORD_CUDA(cudaMemcpyAsync(dptr, h, sizeof(Inject) * e.size(), cudaMemcpyHostToDevice, s.stream));
                 float* F6[6] = {f.p, f.p, f.p, f.p, f.p, f.p};
-                InjectList l{dptr, (int)e.size()};
-                launch_inject(s, F6, l);
-                SORD_CUDA(cudaStreamSynchronize(s.stream));
+                launch_inject(s, F6, upload_inject(s, 3, e));
             }
         } else {
             float val = io.val * host_time_function(io.fname, s.tm, g.dt, io.tau);

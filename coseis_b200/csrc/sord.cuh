@@ -236,6 +236,9 @@ struct FieldView {
 };
 void field_io(Solver& s, const char* passes, const char* field, FieldView f);
 void field_io_flush_all(Solver& s);
+InjectList upload_inject(Solver& s, int slot, const std::vector<Inject>& e);  // through the slot's ring (api.cu)
+void writer_drain(Solver& s);  // every queued output record on disk; throws the first write error
+void writer_free(Solver& s);
 bool field_active(Solver& s, const char* field, char pass);
 // cells (or nodes) of a '.' op with their trilinear weights and the
 // weights' derivatives with respect to the op's position (adjoint)
@@ -312,9 +315,11 @@ struct Solver {
     size_t stage_cap = 0;
     float* pin_io[8] = {};     // pinned chunks of the whole-volume input readers
     cudaEvent_t pin_ev[8] = {};
+    int rec_slot = 0;          // next chunk buffer for a time-varying input record
     // work decomposition of the fused step kernels (fused.cu)
     FusedPlan* fplan = nullptr;
     struct AdjointState* adj = nullptr;  // checkpoints and adjoint fields (adjoint.cu)
+    struct OutWriter* writer = nullptr;  // output-record writer thread (fieldio.cu)
     bool mem_attached = false;  // holds a reference on the device's memory pool
     cudaEvent_t inj_done[kInjectSlots][kInjectRing] = {};
     int inj_ring[kInjectSlots] = {};
