@@ -734,6 +734,26 @@ __global__ void __launch_bounds__(SJ * SK, GEOM == GEOM_GENERAL ? 1 : 2) k_shell
 #undef CELL
 }
 
+// Zero one cell of the fast-arithmetic cell plane (layout of Lay: NGCF
+// groups of ncl float4) in the pattern the cell phase writes it: group 1
+// and, with two bracket directions, the lower-bracket groups hold float2
+// values at index tid, which a float4 store at tid would miss (and would
+// clear two other cells' values instead).
+template <int NDIR, int NQ>
+__device__ __forceinline__ void zero_cell_fm(float4* sC, int tid, int ncl) {
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    sC[tid] = z;
+    reinterpret_cast<float2*>(sC + ncl)[tid] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        float4* cq = sC + (2 + NQ * q) * ncl + tid;
+        cq[0] = z;
+        cq[ncl] = z;
+        if (NDIR == 3) cq[2 * ncl] = z;
+        if (NDIR == 2) reinterpret_cast<float2*>(sC + (2 + 4 * NQ) * ncl)[q * ncl + tid] = make_float2(0.f, 0.f);
+    }
+}
+
 // Interior kernel: tiles of 31 x 7 nodes from (A.jf, A.kf), planes A.lf0..A.lf1,
 // strictly inside the non-PML region, with no PML or boundary terms.
 // FM (fast arithmetic): fused multiply-adds, brackets scaled by h once per
@@ -896,9 +916,13 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
         const int cs = FM ? 0 : l & 1;
         const bool valid = (F || cellcol) && l >= g.i1cell[2] && l <= g.i2cell[2];
         if (!valid) {
-            float4* cw = sC + cs * (NGC * NCL) + tid;
+            if constexpr (FM) {
+                zero_cell_fm<NDIR, NQ>(sC, tid, NCL);
+            } else {
+                float4* cw = sC + cs * (NGC * NCL) + tid;
 #pragma unroll
-            for (int i = 0; i < (FM ? NGCF : NGC); i++) cw[i * NCL] = make_float4(0.f, 0.f, 0.f, 0.f);
+                for (int i = 0; i < NGC; i++) cw[i * NCL] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
             return;
         }
         const long long q = g.idx(J, K, l);

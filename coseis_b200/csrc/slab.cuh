@@ -163,9 +163,7 @@ __global__ void __launch_bounds__(SJ * SK, GEOM == GEOM_GENERAL ? 1 : 2) k_slab(
     auto cells = [&](int l) {
         const bool valid = cellcol && l >= g.i1cell[2] && l <= g.i2cell[2];
         if (!valid) {
-            float4* cw = sC + tid;
-#pragma unroll
-            for (int i = 0; i < NGCF; i++) cw[i * NCL_] = make_float4(0.f, 0.f, 0.f, 0.f);
+            zero_cell_fm<NDIR, NQ>(sC, tid, NCL_);
             return;
         }
         float Uc[3][8], Vc[3][8], Gc[8], X0[8], X1[8], X2[8];
