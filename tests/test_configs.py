@@ -10,7 +10,10 @@
   grid at dx 100 m for 400 steps (the rupture spreads over half the
   fault in 2 s): bit-identical to the FP32 oracle in reference order;
   in fast arithmetic slip and slip rate within relative L2 1e-4 of the FP64
-  oracle and rupture times within one time step.
+  oracle, or within 3 times the FP32 oracle's own error where that is
+  larger (the final slip rate near a rupture front is sensitive to
+  rounding: the FP32 oracle differs from FP64 by 1.9e-4 there), and
+  rupture times within one time step.
 """
 import os
 
@@ -54,7 +57,7 @@ def _check(dirs, prm, oracle_bins):
             continue
         fl = floor_of(dirs['o64'], f, '<f8')
         errs[f] = (rel_l2(a, b, fl), rel_l2(load(dirs['o32'], f, '<f4'), b, fl))
-        assert errs[f][0] <= 1e-4, (f, errs[f])
+        assert errs[f][0] <= max(1e-4, 3.0 * errs[f][1]), (f, errs[f])
     return errs
 
 
