@@ -808,8 +808,10 @@ def run_ensemble_bench(n, nthreads, device, nt=ENS_NT, seed=SEED):
         t0 = time.time()
         _lib.run_ensemble(ens, device, nthreads)
         t_ens = time.time() - t0
-        outs = [sorted(f for f in os.listdir(a) if f.endswith('.bin') and f != 'ts.bin') for a in ser]
-        same = all(o == sorted(f for f in os.listdir(b) if f.endswith('.bin') and f != 'ts.bin') and
+        # every output file but the wall-clock timers (prof-*.bin)
+        keep = lambda f: f.endswith('.bin') and f != 'ts.bin' and not f.startswith('prof-')
+        outs = [sorted(f for f in os.listdir(a) if keep(f)) for a in ser]
+        same = all(o == sorted(f for f in os.listdir(b) if keep(f)) and
                    all(open(os.path.join(a, f), 'rb').read() == open(os.path.join(b, f), 'rb').read() for f in o)
                    for a, b, o in zip(ser, ens, outs))
         nfiles = sum(len(o) for o in outs)
