@@ -1679,7 +1679,7 @@ struct FusedPlan {
     int nbx = 0, nby = 0;                       // interior tiles
     int lf0 = 0, lf1 = -1;                      // interior node planes (inclusive)
     int segl = 0, nseg = 1;                     // interior planes per block, blocks per column
-    int ipl = 96;                               // deepest shell item
+    int ipl = 16;                               // planes per item of a point-source tile
     std::vector<int> base;                      // shell items without point sources (6 ints each)
     std::vector<int> bmask;                     // per base item: k_slab class (0..3: MASK 1, 2, 4, 7)
     std::vector<BoxRegion> regions;             // how the base items were laid out
@@ -1692,6 +1692,10 @@ struct FusedPlan {
     // interior kernel (they write disjoint nodes and read the same inputs)
     cudaStream_t side = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
+    // each k_slab class on its own stream, forked from and joined back into
+    // the stream of the shell launches, so that the classes' tails overlap
+    cudaStream_t cst[4] = {};
+    cudaEvent_t cfork = nullptr, cdone[4] = {};
 };
 
 void fused_free(Solver& s) {
@@ -1701,6 +1705,11 @@ void fused_free(Solver& s) {
     if (P->fork) cudaEventDestroy(P->fork);
     if (P->join) cudaEventDestroy(P->join);
     if (P->side) cudaStreamDestroy(P->side);
+    if (P->cfork) cudaEventDestroy(P->cfork);
+    for (int c = 0; c < 4; c++) {
+        if (P->cdone[c]) cudaEventDestroy(P->cdone[c]);
+        if (P->cst[c]) cudaStreamDestroy(P->cst[c]);
+    }
     dev_free(s, P->d_items);
     pinned_put(P->h_items);
     delete P;
@@ -1714,6 +1723,9 @@ void fused_free(Solver& s) {
 static constexpr int kItemPlanes = 96;
 static constexpr int kMinPlanes = 8;
 static constexpr int kWaveBlocks = 4;
+// planes per item of an interior tile holding a point source (k_shell): a
+// few tile columns only, so short items spread them over the SMs
+static constexpr int kSourcePlanes = 16;
 
 // shell items covering node box [j1, j2] x [k1, k2] x [l1, l2]
 static void push_box(std::vector<int>& v, int ipl, int j1, int j2, int k1, int k2, int l1, int l2,
@@ -1760,43 +1772,36 @@ static FusedPlan& fused_plan(Solver& s) {
     int sms = 148;
     SORD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s.device));
     const int want = kWaveBlocks * sms;
-    // boxes of the shell, cut where the PML of another axis begins so that
-    // each box is damped along as few axes as possible (the k_slab class)
-    auto shell = [&](int ipl) {
-        std::vector<int> v;
-        std::vector<BoxRegion>* r = &P->regions;
-        r->clear();
-        if (!inner) {
-            push_box(v, ipl, g.i1node[0], g.i2node[0], g.i1node[1], g.i2node[1], L1, L2, r);
-        } else {
-            const int kr[3][2] = {{g.i1node[1], P->kf - 1}, {P->kf, P->kend}, {P->kend + 1, g.i2node[1]}};
-            const int lr[3][2] = {{L1, P->lf0 - 1}, {P->lf0, P->lf1}, {P->lf1 + 1, L2}};
-            for (int a = 0; a < 3; a++)
-                for (int b = 0; b < 3; b++) {
-                    push_box(v, ipl, g.i1node[0], P->jf - 1, kr[a][0], kr[a][1], lr[b][0], lr[b][1], r);
-                    push_box(v, ipl, P->jend + 1, g.i2node[0], kr[a][0], kr[a][1], lr[b][0], lr[b][1], r);
-                }
-            for (int b = 0; b < 3; b++) {
-                push_box(v, ipl, P->jf, P->jend, g.i1node[1], P->kf - 1, lr[b][0], lr[b][1], r);
-                push_box(v, ipl, P->jf, P->jend, P->kend + 1, g.i2node[1], lr[b][0], lr[b][1], r);
-            }
-            push_box(v, ipl, P->jf, P->jend, P->kf, P->kend, L1, P->lf0 - 1, r);
-            push_box(v, ipl, P->jf, P->jend, P->kf, P->kend, P->lf1 + 1, L2, r);
-        }
-        return v;
+    // regions of the shell, cut where the PML of another axis begins so that
+    // each is damped along as few axes as possible (its k_slab class)
+    struct RegionBox {
+        int lo[3], hi[3];
     };
-    P->ipl = kItemPlanes;
-    P->base = shell(P->ipl);
-    while (P->ipl > kMinPlanes && (int)P->base.size() / 6 < want) {
-        P->ipl = std::max(kMinPlanes, P->ipl * 2 / 3);
-        P->base = shell(P->ipl);
+    std::vector<RegionBox> rb;
+    auto add = [&](int j1, int j2, int k1, int k2, int l1, int l2) {
+        if (j1 <= j2 && k1 <= k2 && l1 <= l2) rb.push_back({{j1, k1, l1}, {j2, k2, l2}});
+    };
+    if (!inner) {
+        add(g.i1node[0], g.i2node[0], g.i1node[1], g.i2node[1], L1, L2);
+    } else {
+        const int kr[3][2] = {{g.i1node[1], P->kf - 1}, {P->kf, P->kend}, {P->kend + 1, g.i2node[1]}};
+        const int lr[3][2] = {{L1, P->lf0 - 1}, {P->lf0, P->lf1}, {P->lf1 + 1, L2}};
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) {
+                add(g.i1node[0], P->jf - 1, kr[a][0], kr[a][1], lr[b][0], lr[b][1]);
+                add(P->jend + 1, g.i2node[0], kr[a][0], kr[a][1], lr[b][0], lr[b][1]);
+            }
+        for (int b = 0; b < 3; b++) {
+            add(P->jf, P->jend, g.i1node[1], P->kf - 1, lr[b][0], lr[b][1]);
+            add(P->jf, P->jend, P->kend + 1, g.i2node[1], lr[b][0], lr[b][1]);
+        }
+        add(P->jf, P->jend, P->kf, P->kend, L1, P->lf0 - 1);
+        add(P->jf, P->jend, P->kf, P->kend, P->lf1 + 1, L2);
     }
-    // k_slab class of each box: axis d needs the PML terms when a real cell
+    // k_slab class of a node box: axis d needs the PML terms when a real cell
     // the box computes (node range a..b -> cells a-1..b) or one of its real
     // nodes lies in a PML slab of d; one axis -> its own class, more -> all
-    for (size_t i = 0; i < P->base.size(); i += 6) {
-        const int* b = &P->base[i];
-        const int lo[3] = {b[0], b[1], b[4]}, hi[3] = {b[2], b[3], b[5]};
+    auto klass = [&](const int* lo, const int* hi) {
         int m = 0;
         for (int d = 0; d < 3; d++) {
             for (int c = std::max(lo[d] - 1, g.i1cell[d]); c <= std::min(hi[d], g.i2cell[d]); c++)
@@ -1804,7 +1809,37 @@ static FusedPlan& fused_plan(Solver& s) {
             for (int c = std::max(lo[d], g.i1node[d]); c <= std::min(hi[d], g.i2node[d]); c++)
                 if (c <= g.i1pml[d] || c >= g.i2pml[d]) m |= 1 << d;
         }
-        P->bmask.push_back(m == 2 ? 1 : m == 4 ? 2 : (m == 0 || m == 1) ? 0 : 3);
+        return m == 2 ? 1 : m == 4 ? 2 : (m == 0 || m == 1) ? 0 : 3;
+    };
+    // Planes per item, per class: each class is one launch (on its own
+    // stream), so its items are cut as long as the launch still has about
+    // kWaveBlocks blocks per SM, and no shorter than kMinPlanes (an item
+    // starts with a prologue of about two planes).
+    std::vector<int> rcls;
+    for (const RegionBox& r : rb) rcls.push_back(klass(r.lo, r.hi));
+    int iplc[4];
+    for (int c = 0; c < 4; c++) {
+        auto count = [&](int ipl) {
+            long long n = 0;
+            for (size_t i = 0; i < rb.size(); i++)
+                if (rcls[i] == c)
+                    n += (long long)((rb[i].hi[0] - rb[i].lo[0]) / (SJ - 1) + 1) * ((rb[i].hi[1] - rb[i].lo[1]) / (SK - 1) + 1) *
+                         ((rb[i].hi[2] - rb[i].lo[2]) / ipl + 1);
+            return n;
+        };
+        int ipl = kItemPlanes;
+        while (ipl > kMinPlanes && count(ipl) < want) ipl = std::max(kMinPlanes, ipl * 2 / 3);
+        iplc[c] = ipl;
+    }
+    P->regions.clear();
+    for (size_t i = 0; i < rb.size(); i++)
+        push_box(P->base, iplc[rcls[i]], rb[i].lo[0], rb[i].hi[0], rb[i].lo[1], rb[i].hi[1], rb[i].lo[2], rb[i].hi[2],
+                 &P->regions);
+    P->ipl = kSourcePlanes;
+    for (size_t i = 0; i < P->base.size(); i += 6) {
+        const int* b = &P->base[i];
+        const int lo[3] = {b[0], b[1], b[4]}, hi[3] = {b[2], b[3], b[5]};
+        P->bmask.push_back(klass(lo, hi));
     }
     if (!inner) {
         P->jend = P->jf - 1;
@@ -1816,13 +1851,18 @@ static FusedPlan& fused_plan(Solver& s) {
         P->segl = (planes + nseg - 1) / nseg;
         P->nseg = (planes + P->segl - 1) / P->segl;
     }
-    P->cap = (int)P->base.size() / 6 + 4096;
+    P->cap = (int)P->base.size() / 6 + 16384;
     SORD_CUDA(dev_malloc(s, (void**)&P->d_items, sizeof(int) * 6 * P->cap));
     P->h_items = (int*)pinned_get(sizeof(int) * 6 * P->cap);
     SORD_CUDA(cudaEventCreateWithFlags(&P->done, cudaEventDisableTiming));
     SORD_CUDA(cudaEventCreateWithFlags(&P->fork, cudaEventDisableTiming));
     SORD_CUDA(cudaEventCreateWithFlags(&P->join, cudaEventDisableTiming));
     SORD_CUDA(cudaStreamCreateWithFlags(&P->side, cudaStreamNonBlocking));
+    SORD_CUDA(cudaEventCreateWithFlags(&P->cfork, cudaEventDisableTiming));
+    for (int c = 0; c < 4; c++) {
+        SORD_CUDA(cudaEventCreateWithFlags(&P->cdone[c], cudaEventDisableTiming));
+        SORD_CUDA(cudaStreamCreateWithFlags(&P->cst[c], cudaStreamNonBlocking));
+    }
     return *P;
 }
 
@@ -2024,12 +2064,16 @@ void launch_fused(Solver& s, const InjectList& pot, const InjectList& mom, const
     // the shell launches: k_shell, then each k_slab class
     auto shell_launches = [&](cudaStream_t st) {
         if (nshell > 0) launch_geom<false>(s, A, dim3((unsigned)nshell, 1, 1), st);
+        SORD_CUDA(cudaEventRecord(P.cfork, st));
         int off = nshell;
         for (int m = 0; m < 4; m++) {
             if (nslab[m] == 0) continue;
             StepArgs B = A;
             B.items = P.d_items + 6 * (size_t)off;
-            launch_slab(s, B, m, (unsigned)nslab[m], st);
+            SORD_CUDA(cudaStreamWaitEvent(P.cst[m], P.cfork, 0));
+            launch_slab(s, B, m, (unsigned)nslab[m], P.cst[m]);
+            SORD_CUDA(cudaEventRecord(P.cdone[m], P.cst[m]));
+            SORD_CUDA(cudaStreamWaitEvent(st, P.cdone[m], 0));
             off += nslab[m];
         }
     };
