@@ -597,7 +597,11 @@ def cpu_sample(shape_s, steps, warm, threads):
 
 
 # ------------------------------------------------------------------ arms
-def dist_init():
+def dist_init(backend='nccl'):
+    """World size, rank, this rank's device and the process group (None for
+    one rank).  backend 'gloo' moves the halo planes through host memory and
+    lets several ranks share a device (their kernels never wait on one
+    another: the ranks meet on the host between steps)."""
     ws = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))
     local = int(os.environ.get('LOCAL_RANK', '0'))
@@ -607,10 +611,20 @@ def dist_init():
         import torch
         import torch.distributed as dist
         os.environ.setdefault('MASTER_ADDR', '127.0.0.1')
+        local = local % max(torch.cuda.device_count(), 1)
         torch.cuda.set_device(local)
-        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
         pg = dist
     return ws, rank, local, pg
+
+
+def reduce_sum(pg, v):
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([float(v)], dtype=torch.float64, device='cuda' if pg.get_backend() == 'nccl' else 'cpu')
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
 
 
 def reduce_max(pg, v):
@@ -624,10 +638,36 @@ def reduce_max(pg, v):
     return float(t.item())
 
 
-def job_rate(ws, nodes, steps, ms_max):
-    """Whole-job node-updates/s: every rank advances its own replica of
-    `nodes` nodes by `steps` steps; the job takes the slowest rank's time."""
-    return ws * nodes * steps / (ms_max / 1e3)
+def job_rate(nodes, steps, ms_max):
+    """Whole-job node-updates/s: the ranks advance one mesh of `nodes` nodes
+    by `steps` steps, each its slab of l planes; the job takes the slowest
+    rank's time."""
+    return nodes * steps / (ms_max / 1e3)
+
+
+def shared_workdir(pg, rank, prefix):
+    """A scratch directory that every rank of the job sees (one node)."""
+    d = [tempfile.mkdtemp(prefix=prefix) if rank == 0 else None]
+    if pg is not None:
+        pg.broadcast_object_list(d, src=0)
+    return d[0]
+
+
+def split_prm(prm, ws):
+    """The parameters of a run split into ws slabs of l planes."""
+    if ws > 1:
+        prm = dict(prm)
+        prm['nproc3'] = [1, 1, ws]
+    return prm
+
+
+def open_solver(work, text, local, rank, ws, pg=None):
+    from coseis_b200 import _lib
+    if ws == 1:
+        return _lib.Solver(work, text, device=local)
+    from coseis_b200 import parallel
+    transport = 'device' if pg.get_backend() == 'nccl' else 'host'
+    return _lib.Solver(work, text, device=local, part=rank, exchange=parallel.DistExchange(transport))
 
 
 def barrier(pg):
@@ -641,7 +681,7 @@ def run_ours(args):
     from coseis_b200 import _lib
     # read by every handle this process creates (timed run, e2e, ensemble, adjoint)
     os.environ['SORD_ARITHMETIC'] = args.arithmetic
-    ws, rank, local, pg = dist_init()
+    ws, rank, local, pg = dist_init(args.backend)
     shape = tuple(args.shape)
     nodes = float(np.prod(shape))
     inputs = os.path.join(args.cache, 'wave_%dx%dx%d_%d_%g' % (shape + (SEED, args.hill)))
@@ -653,11 +693,16 @@ def run_ours(args):
     # kernel too (2 warm-up steps + the same number of timed steps)
     other = args.arithmetic == 'fast' and not args.no_reference_order
     nt = args.warmup + args.steps + prof_steps + ((2 + args.steps) if other else 0)
-    work = tempfile.mkdtemp(prefix='sord_bench_%d_' % rank)
+    # N > 1: the mesh split into N slabs of l planes, one per rank, halo
+    # planes exchanged over NCCL every step (strong scaling)
+    work = shared_workdir(pg, rank, 'sord_bench_')
     try:
-        text = stage_in(wave_prm(shape, nt), work, inputs)
+        if rank == 0:
+            stage_in(split_prm(wave_prm(shape, nt), ws), work, inputs)
+        barrier(pg)
+        text = open(os.path.join(work, 'sord.in')).read()
         t0 = time.time()
-        s = _lib.Solver(work, text, device=local)
+        s = open_solver(work, text, local, rank, ws, pg)
         setup_s = time.time() - t0
         s.step(args.warmup)
         barrier(pg)
@@ -671,6 +716,7 @@ def run_ours(args):
         launches = s.kernel_launches() - l0
         clocks = clk.stop()
         ms_max = reduce_max(pg, ms)
+        launches = reduce_sum(pg, launches)
         s.set_profiling(True)
         s.step(prof_steps)
         kt = s.kernel_times()
@@ -682,11 +728,12 @@ def run_ours(args):
             barrier(pg)
             s.step(args.steps)
             r_ms = reduce_max(pg, s.last_step_ms())
-            ref_order = {'ms_per_step': r_ms / args.steps, 'value': job_rate(ws, nodes, args.steps, r_ms)}
+            ref_order = {'ms_per_step': r_ms / args.steps, 'value': job_rate(nodes, args.steps, r_ms)}
         s.close()
+        barrier(pg)
         e2e = None
         if not args.no_e2e:
-            e2e = run_e2e(args, shape, inputs, local)
+            e2e = run_e2e(args, shape, inputs, local, pg, ws, rank)
             barrier(pg)
         ens = None
         if ws == 1 and args.ensemble > 0:
@@ -698,10 +745,11 @@ def run_ours(args):
         if ws == 1 and not args.no_configs:
             cfgs = run_other_configs(local, cpu=not args.no_cpu)
     finally:
-        shutil.rmtree(work, ignore_errors=True)
+        if rank == 0:
+            shutil.rmtree(work, ignore_errors=True)
     if rank != 0:
         return
-    value = job_rate(ws, nodes, args.steps, ms_max)
+    value = job_rate(nodes, args.steps, ms_max)
     hbm, src = peaks()
     alg = algorithmic_bytes_per_node(shape)
     # dominant kernel: the fused whole-step kernel, average launch duration
@@ -711,23 +759,31 @@ def run_ours(args):
     else:
         kernel = 'k_time + k_stress + k_accel (separate-kernel step)'
         launch_ms = sum(kt[k][0] for k in ('time', 'stress', 'accel', 'mass')) / prof_steps
-    achieved = alg * nodes / (launch_ms / 1e3) / 1e9
+    # rank 0's kernels advance its slab only
+    knodes = nodes
+    if ws > 1:
+        from coseis_b200 import parallel
+        a, b = parallel.part_planes(shape[2], ws)[0]
+        knodes = float(shape[0] * shape[1] * (b - a + 1))
+    achieved = alg * knodes / (launch_ms / 1e3) / 1e9
     tr = traffic_per_node()
     out = {
         'metric': 'node-updates/s', 'value': value, 'unit': 'node-updates/s',
         'n_gpus': ws, 'steps': args.steps, 'warmup': args.warmup,
-        'ms_per_step': ms_max / args.steps, 'higher_is_better': True, 'scaling': 'weak',
+        'ms_per_step': ms_max / args.steps, 'higher_is_better': True, 'scaling': 'strong',
         'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic (seeded)',
         'config': {'workload': wave_workload(shape),
-                   'nodes': int(nodes), 'dx_m': DX, 'dt_s': DT, 'parallelism': 'replicas' if ws > 1 else 'single',
+                   'nodes': int(nodes), 'dx_m': DX, 'dt_s': DT,
+                   'parallelism': ('l-slabs x %d (nproc3 = [1, 1, %d], NCCL halo exchange)' % (ws, ws)) if ws > 1
+                   else 'single',
                    'arithmetic': args.arithmetic,
                    'l2': 'inputs larger than L2 (%.1f GB resident)' % (nodes * 100 / 1e9),
                    'setup_s': round(setup_s, 2), 'host_wall_s': round(wall, 4)},
         'roofline': {'bound': 'hbm', 'kernel': kernel, 'launch_ms': launch_ms,
                      'achieved': achieved, 'peak': hbm, 'unit': 'GB/s', 'frac': achieved / hbm,
                      'peak_source': src, 'algorithmic_bytes_per_node': alg,
-                     'algorithmic_bytes_per_launch': alg * nodes,
-                     'traffic': (tr * nodes if tr else None)},
+                     'algorithmic_bytes_per_launch': alg * knodes,
+                     'traffic': (tr * knodes if tr else None)},
         'kernels_ms_per_step': {k: v[0] / prof_steps for k, v in kt.items() if v[1]},
         'reference_order': ref_order,
         'gpu_launches': int(launches),
@@ -749,22 +805,36 @@ def run_ours(args):
     print(json.dumps(out))
 
 
-def run_e2e(args, shape, inputs, device):
-    """User call end to end: staged files on the host -> sord_run_directory."""
+def run_e2e(args, shape, inputs, device, pg=None, ws=1, rank=0):
+    """User call end to end: staged files on the host -> sord_run_directory
+    (N > 1: every rank runs its slab, coseis_b200.parallel.run_dist, into
+    one shared directory; the job takes the slowest rank's host time)."""
     from coseis_b200 import _lib
     nodes = float(np.prod(shape))
-    work = tempfile.mkdtemp(prefix='sord_e2e_')
+    work = shared_workdir(pg, rank, 'sord_e2e_')
     try:
-        stage_in(wave_prm(shape, args.steps), work, inputs)
+        if rank == 0:
+            stage_in(split_prm(wave_prm(shape, args.steps), ws), work, inputs)
         h2d = sum(os.path.getsize(os.path.join(inputs, f)) for f in ('rho.bin', 'vp.bin', 'vs.bin', 'z.bin'))
-        h2d += os.path.getsize(os.path.join(work, 'sord.in'))
+        h2d += os.path.getsize(os.path.join(work, 'sord.in')) if rank == 0 else 0
         # start from an idle device: the memory of the handles before is back with the driver
         _lib.trim_memory(device)
+        barrier(pg)
         t0 = time.time()
-        _lib.run_directory(work, device)
-        wall = time.time() - t0
+        if ws > 1:
+            from coseis_b200 import parallel
+            parallel.run_dist(work, device, transport='device' if pg.get_backend() == 'nccl' else 'host')
+        else:
+            _lib.run_directory(work, device)
+        wall = reduce_max(pg, time.time() - t0)
+        barrier(pg)
         d2h = sum(os.path.getsize(os.path.join(work, f)) for f in os.listdir(work)
                   if f.endswith('.bin') and not os.path.islink(os.path.join(work, f)))
+        if ws > 1:
+            return {'value': nodes * args.steps / wall, 'unit': 'node-updates/s',
+                    'h2d_bytes_per_step': h2d / args.steps, 'd2h_bytes_per_step': d2h / args.steps,
+                    'wall_s': round(wall, 3), 'includes': 'setup of every slab from the staged host files, '
+                                                          '%d steps, output files, teardown' % args.steps}
         # where the time goes: the same run again through the handle calls
         part = os.path.join(work, 'parts')
         text = stage_in(wave_prm(shape, args.steps), part, inputs)
@@ -785,7 +855,8 @@ def run_e2e(args, shape, inputs, device):
                             'teardown': round(t3 - t2, 3),
                             'memory_return_after_teardown': round(t4 - t3, 3)}}
     finally:
-        shutil.rmtree(work, ignore_errors=True)
+        if rank == 0:
+            shutil.rmtree(work, ignore_errors=True)
 
 
 def run_ensemble_bench(n, nthreads, device, nt=ENS_NT, seed=SEED):
@@ -892,7 +963,7 @@ def run_reference(args):
         'impl': 'reference', 'metric': 'node-updates/s', 'value': v, 'unit': 'node-updates/s',
         'n_gpus': ws, 'steps': steps, 'warmup': args.warmup,
         'ms_per_step': float(np.prod(cfg_shape)) / v * 1e3, 'higher_is_better': True,
-        'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic (seeded)',
+        'scaling': 'strong', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic (seeded)',
         'config': {'workload': wave_workload(cfg_shape), 'nodes': int(np.prod(cfg_shape)), 'dx_m': DX, 'dt_s': DT},
         'cpu_baseline': {'value': v, 'unit': 'node-updates/s', 'cores': thr, 'kind': 'port', 'sample': sample},
         'e2e': {'value': v, 'unit': 'node-updates/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
@@ -921,6 +992,8 @@ def main():
     ap.add_argument('--hill', type=float, default=500.0, help='topography peak (m); 0 gives a rectilinear mesh')
     ap.add_argument('--arithmetic', choices=['reference', 'fast'], default='fast',
                     help='interior step kernel arithmetic (sord_set_arithmetic)')
+    ap.add_argument('--backend', choices=['nccl', 'gloo'], default='nccl',
+                    help='N > 1: halo planes over NCCL from device memory, or over gloo through host memory')
     ap.add_argument('--no-reference-order', action='store_true',
                     help='with --arithmetic fast, skip timing the reference-order kernel on the same handle')
     args = ap.parse_args()

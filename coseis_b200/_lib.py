@@ -17,8 +17,14 @@ SYMBOLS = [
     'sord_last_error', 'sord_error_string', 'sord_destroy',
     'sord_vector_max_noalloc', 'sord_run_ensemble', 'sord_adjoint_forward', 'sord_adjoint_backward',
     'sord_set_arithmetic', 'sord_get_arithmetic', 'sord_trim_memory', 'sord_adjoint_source_gradients',
-    'sord_set_field',
+    'sord_set_field', 'sord_create_part',
 ]
+
+# callbacks of a partitioned run (include/sordgpu.h: sord_halo_fn, sord_reduce_fn)
+HALO_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_longlong)
+REDUCE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_int,
+                             ctypes.c_int)
 
 # return codes (enum in include/sordgpu.h)
 SORD_OK, SORD_E_PARAM, SORD_E_CFL, SORD_E_NEGVOL, SORD_E_NANINF = 0, -1, -2, -3, -4
@@ -48,6 +54,9 @@ def load():
     P = ctypes.c_void_p
     lib.sord_create.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(P)]
     lib.sord_create.restype = ctypes.c_int
+    lib.sord_create_part.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, HALO_FN, REDUCE_FN,
+                                     P, ctypes.POINTER(P)]
+    lib.sord_create_part.restype = ctypes.c_int
     lib.sord_step.argtypes = [P, ctypes.c_int]
     lib.sord_step.restype = ctypes.c_int
     lib.sord_run.argtypes = [P]
@@ -146,10 +155,35 @@ class Solver(object):
     """One simulation handle: ``Solver(workdir, text)`` runs the setup;
     ``step(n)`` advances n time steps; ``close()`` frees the device memory."""
 
-    def __init__(self, workdir, sord_in_text, device=0):
+    def __init__(self, workdir, sord_in_text, device=0, part=None, exchange=None):
+        """part, exchange: part `part` of a run split along l by the sord.in
+        parameter nproc3 (sord_create_part); `exchange` provides
+        halo(part, send_lo, recv_lo, send_hi, recv_hi, n) and
+        reduce(part, vals, op) (coseis_b200.parallel)."""
         lib = load()
         h = ctypes.c_void_p()
-        _check(lib.sord_create(os.fsencode(workdir), sord_in_text.encode(), device, ctypes.byref(h)))
+        if part is None:
+            _check(lib.sord_create(os.fsencode(workdir), sord_in_text.encode(), device, ctypes.byref(h)))
+        else:
+            def halo(ctx, prt, slo, rlo, shi, rhi, n):
+                try:
+                    return exchange.halo(prt, slo, rlo, shi, rhi, n)
+                except Exception:  # noqa: BLE001 -- reported to the solver as a failed exchange
+                    import traceback
+                    traceback.print_exc()
+                    return 1
+
+            def reduce(ctx, prt, vals, n, op):
+                try:
+                    return exchange.reduce(prt, vals, n, op)
+                except Exception:  # noqa: BLE001
+                    import traceback
+                    traceback.print_exc()
+                    return 1
+            # the C callbacks must live as long as the handle
+            self._cb = (HALO_FN(halo), REDUCE_FN(reduce))
+            _check(lib.sord_create_part(os.fsencode(workdir), sord_in_text.encode(), device, part, self._cb[0],
+                                        self._cb[1], None, ctypes.byref(h)))
         self._h = h
 
     def step(self, n=1):

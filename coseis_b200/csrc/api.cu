@@ -79,6 +79,7 @@ Params parse_sord_in(const std::string& str, std::vector<IoOp>& ops) {
         }
         if (io.nb < 1) io.nb = 1;
         io.ib = -1;
+        io.op0 = io.op;
     }
     return P;
 }
@@ -266,10 +267,12 @@ static bool fault_field(const std::string& f) {
 bool Solver::fusable(int n) const {
     if (!use_fused || !bc_noop(prm)) return false;
     for (auto& io : ops) {
+        // the parts of a partitioned run decide alike: by the ops as read
+        const std::string& op = nparts > 1 ? io.op0 : io.op;
         int it1 = io.ii[3][0], it2 = io.ii[3][1], dit = io.ii[3][2];
-        if (n > it2 || io.op[0] == '#' || n < it1 || ((n - it1) % dit) != 0) continue;
+        if (n > it2 || op[0] == '#' || n < it1 || ((n - it1) % dit) != 0) continue;
         const std::string& f = io.field;
-        char op2 = io.op.size() > 1 ? io.op[1] : ' ';
+        char op2 = op.size() > 1 ? op[1] : ' ';
         bool out = op2 == '>';
         if (out) {
             bool ok = f == "vx" || f == "vy" || f == "vz" || f == "ux" || f == "uy" || f == "uz" || f == "ax" ||
@@ -277,7 +280,7 @@ bool Solver::fusable(int n) const {
             if (!ok) return false;
         } else {
             bool tensor = f[0] == 'p' || f[0] == 'm';
-            if (!(tensor && io.op == "." && bc_cells_noop(prm))) return false;
+            if (!(tensor && op == "." && bc_cells_noop(prm))) return false;
         }
     }
     return true;
@@ -330,6 +333,14 @@ void Solver::step(bool last_in_call) {
     launch_fused(*this, lp, lm, lf, pot, mom, frc, fold, write_a, st);
     if (g.ifn) fault_rupture_fused(*this);
     folded = fold;
+    if (nparts > 1) {
+        // the halo planes of the state the step leaves: v, u of the next
+        // step (folded) and a (the start of an unfolded next step advances
+        // every plane with it) -- the reference's swap of w1 at
+        // acceleration.f90:232, taken after the update
+        float* F[9] = {d.v[0], d.v[1], d.v[2], d.u[0], d.u[1], d.u[2], d.w1n[0], d.w1n[1], d.w1n[2]};
+        halo_exchange(*this, F, 9);
+    }
     for (int i = 0; i < 3; i++) io("<>", kAcc[i], vol(*this, d.w1n[i]));
     io(">", "am2", vol(*this, d.s1));
     if (st) {
@@ -402,6 +413,9 @@ void Solver::step_general(bool st) {
     const bool fuse_a = G.ifn == 0 && bc_noop(prm) && !any_pass(*this, kForce, 3, '<') && !any_pass(*this, kForce, 3, '>');
     if (fuse_a) {
         launch_accel(*this, true, st && !ain, upload_inject(*this, 2, frc));
+        // the halo of a = f m (pointwise from the force halo the reference
+        // swaps, acceleration.f90:229-233; the mass halo came at setup)
+        halo_exchange(*this, d.w1n, 3);
     } else {
         InjectList none{d.inj, 0};
         launch_accel(*this, false, false, none);
@@ -410,6 +424,7 @@ void Solver::step_general(bool st) {
         for (int i = 0; i < 3; i++) io("<", kForce[i], vol(*this, d.w1n[i]));
         launch_vector_bc(*this, d.w1n, prm.bc1, prm.bc2, G.i1bc, G.i2bc);
         if (G.ifn) fault_rupture(*this);
+        halo_exchange(*this, d.w1n, 3);  // acceleration.f90:229-233
         for (int i = 0; i < 3; i++) io(">", kForce[i], vol(*this, d.w1n[i]));
         launch_mass(*this, st && !ain);
     }
@@ -435,6 +450,7 @@ void Solver::stats() {
         int j = stats_j;
         double* M = maxl.data() + (size_t)nq * (j - 1);
         M[0] = amax; M[1] = vmax; M[2] = umax; M[3] = wmax;
+        all_reduce(*this, M, 4, 0);  // statistics.f90:78 over the parts
         bool bad = false;
         for (int q = 0; q < 4; q++)
             if (!(M[q] == M[q]) || M[q] > (double)std::numeric_limits<float>::max()) bad = true;
@@ -490,7 +506,7 @@ void Solver::stats() {
     timers[2] = clock_us() - t3;
     int i = (it - 1) % prm.itio + 1;
     for (int q = 0; q < 4; q++) prof[(size_t)4 * (i - 1) + q] = (int32_t)timers[q];
-    if (i == prm.itio || it == nt) {
+    if ((i == prm.itio || it == nt) && part == 0) {
         static const char* np_[4] = {"prof-halo.bin", "prof-io.bin", "prof-stats.bin", "prof-step.bin"};
         for (int q = 0; q < 4; q++) {
             std::vector<int32_t> col(i);
@@ -509,6 +525,7 @@ void Solver::stats() {
 }
 
 void Solver::write_stats(const std::string& name, const std::vector<float>& col, int m, int o, bool& opened) {
+    if (part != 0) return;  // the master writes the statistics of all parts (statistics.f90:82)
     std::string fn = path(name);
     FILE* fp;
     if (!opened && o == 0) {
@@ -562,7 +579,7 @@ void Solver::destroy() {
     fr(d.vc); fr(d.mr); fr(d.lam); fr(d.mu); fr(d.gam); fr(d.yy); fr(d.s1); fr(d.s2); fr(d.pmlc); fr(d.red); fr(d.inj); fr(d.fp);
     for (int i = 0; i < 6; i++) { fr(d.slabs.p[i]); fr(d.slabs.g[i]); fr(d.gb[i]); }
     for (int i = 0; i < 3; i++) { fr(d.vb[i]); fr(d.ub[i]); }
-    fr(d.x1d); fr(d.y1d);
+    fr(d.x1d); fr(d.y1d); fr(xbuf);
     for (auto& io : ops) fr(io.dbuf);
     probes_free(*this);
     fused_free(*this);
@@ -615,14 +632,70 @@ static int fail(sord_handle* h, const std::exception& e) {
     return code;
 }
 
+namespace sordgpu {
+
+// Halo planes along l of a partitioned run (the reference's
+// scalar_swap_halo / vector_swap_halo, process_mpi.f90:179-246, for the l
+// direction): the first and last core planes of each field are copied into
+// contiguous device send buffers, the caller's callback moves them between
+// neighbouring parts, and the received planes are copied into the halo
+// planes.  Planes are contiguous in the j-fastest layout.
+void halo_exchange(Solver& s, float* const* fields, int nf) {
+    if (s.nparts <= 1) return;
+    const Geom& g = s.g;
+    const size_t sz = (size_t)g.sz, n = sz * (size_t)nf;
+    if (s.xcap < n) {
+        dev_free(s, s.xbuf);
+        s.xbuf = nullptr;
+        s.xcap = 0;
+        SORD_CUDA(dev_malloc(s, (void**)&s.xbuf, sizeof(float) * 4 * n));
+        s.xcap = n;
+    }
+    float *send_lo = s.xbuf, *recv_lo = s.xbuf + n, *send_hi = s.xbuf + 2 * n, *recv_hi = s.xbuf + 3 * n;
+    const bool lo = s.part > 0, hi = s.part < s.nparts - 1;
+    const size_t core1 = (size_t)(g.i1core[2] - 1) * sz, core2 = (size_t)(g.i2core[2] - 1) * sz;
+    const size_t halo1 = (size_t)(g.i1core[2] - 2) * sz, halo2 = (size_t)g.i2core[2] * sz;
+    for (int i = 0; i < nf; i++) {
+        if (lo) SORD_CUDA(cudaMemcpyAsync(send_lo + i * sz, fields[i] + core1, sizeof(float) * sz, cudaMemcpyDeviceToDevice, s.stream));
+        if (hi) SORD_CUDA(cudaMemcpyAsync(send_hi + i * sz, fields[i] + core2, sizeof(float) * sz, cudaMemcpyDeviceToDevice, s.stream));
+    }
+    SORD_CUDA(cudaStreamSynchronize(s.stream));
+    if (!s.halo_fn) throw SordError(SORD_E_PARAM, "partitioned run without a halo-exchange callback");
+    const int rc = s.halo_fn(s.cb_ctx, s.part, lo ? send_lo : nullptr, lo ? recv_lo : nullptr, hi ? send_hi : nullptr,
+                             hi ? recv_hi : nullptr, (long long)n);
+    if (rc) throw SordError(SORD_E_STATE, "halo exchange failed (" + std::to_string(rc) + ")");
+    for (int i = 0; i < nf; i++) {
+        if (lo) SORD_CUDA(cudaMemcpyAsync(fields[i] + halo1, recv_lo + i * sz, sizeof(float) * sz, cudaMemcpyDeviceToDevice, s.stream));
+        if (hi) SORD_CUDA(cudaMemcpyAsync(fields[i] + halo2, recv_hi + i * sz, sizeof(float) * sz, cudaMemcpyDeviceToDevice, s.stream));
+    }
+}
+
+void all_reduce(Solver& s, double* vals, int n, int op) {
+    if (s.nparts <= 1) return;
+    if (!s.reduce_fn) throw SordError(SORD_E_PARAM, "partitioned run without a reduction callback");
+    const int rc = s.reduce_fn(s.cb_ctx, s.part, vals, n, op);
+    if (rc) throw SordError(SORD_E_STATE, "reduction failed (" + std::to_string(rc) + ")");
+}
+
+}  // namespace sordgpu
+
 extern "C" {
 
-int sord_create(const char* workdir, const char* sord_in_text, int device, sord_handle** out) {
+static int create(const char* workdir, const char* sord_in_text, int device, int part, sord_halo_fn halo,
+                  sord_reduce_fn reduce, void* ctx, bool partitioned, sord_handle** out) {
     if (!out || !sord_in_text) return SORD_E_PARAM;
     *out = nullptr;
     sord_handle* h = new sord_handle();
     Solver& s = h->s;
     try {
+        if (partitioned) {
+            if (part < 0 || !halo || !reduce) throw SordError(SORD_E_PARAM, "bad part index or missing callbacks");
+            s.part = part;
+            s.nparts = -1;  // set from nproc3 by setup
+            s.halo_fn = halo;
+            s.reduce_fn = reduce;
+            s.cb_ctx = ctx;
+        }
         int n = 0;
         if (cudaGetDeviceCount(&n) != cudaSuccess || n < 1) throw SordError(SORD_E_CUDA, "no CUDA device available");
         if (device < 0 || device >= n) throw SordError(SORD_E_CUDA, "bad device index");
@@ -650,6 +723,15 @@ int sord_create(const char* workdir, const char* sord_in_text, int device, sord_
     return SORD_OK;
 }
 
+int sord_create(const char* workdir, const char* sord_in_text, int device, sord_handle** out) {
+    return create(workdir, sord_in_text, device, 0, nullptr, nullptr, nullptr, false, out);
+}
+
+int sord_create_part(const char* workdir, const char* sord_in_text, int device, int part, sord_halo_fn halo,
+                     sord_reduce_fn reduce, void* ctx, sord_handle** out) {
+    return create(workdir, sord_in_text, device, part, halo, reduce, ctx, true, out);
+}
+
 int sord_step(sord_handle* h, int nsteps) {
     if (!h) return SORD_E_PARAM;
     Solver& s = h->s;
@@ -675,6 +757,7 @@ int sord_adjoint_forward(sord_handle* h, int segment) {
     Solver& s = h->s;
     try {
         SORD_CUDA(cudaSetDevice(s.device));
+        if (s.nparts > 1) throw SordError(SORD_E_PARAM, "not available on a part of a partitioned run");
         const int seg = adjoint_segment(s, segment);
         adjoint_begin(s, seg);
         SORD_CUDA(cudaEventRecord(s.ev0, s.stream));
@@ -783,6 +866,7 @@ int sord_get_field(sord_handle* h, const char* name, float* host, size_t n) {
     Solver& s = h->s;
     try {
         SORD_CUDA(cudaSetDevice(s.device));
+        if (s.nparts > 1) throw SordError(SORD_E_PARAM, "not available on a part of a partitioned run");
         std::string f = name;
         float* src = nullptr;
         bool cell = false;
@@ -817,6 +901,7 @@ int sord_set_field(sord_handle* h, const char* name, const float* host, size_t n
     Solver& s = h->s;
     try {
         SORD_CUDA(cudaSetDevice(s.device));
+        if (s.nparts > 1) throw SordError(SORD_E_PARAM, "not available on a part of a partitioned run");
         std::string f = name;
         float* dst = nullptr;
         bool cell = false;

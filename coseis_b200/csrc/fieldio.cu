@@ -287,14 +287,17 @@ float host_time_function(const std::string& pulse, float t, float dt, float tau)
 
 static inline float wgt(float x, int j, bool plane) { return plane ? 1.0f : 1.0f - std::fabs(x - (float)j); }
 
-static bool applies(Solver& s, const IoOp& io, const char* field, char pass) {
+// as_read: by the op as read from sord.in (the same on every part of a
+// partitioned run), not by whether this process holds any of its region
+static bool applies(Solver& s, const IoOp& io, const char* field, char pass, bool as_read = false) {
+    const std::string& op = as_read ? io.op0 : io.op;
     int it1 = io.ii[3][0], it2 = io.ii[3][1], dit = io.ii[3][2];
     if (s.it > it2) return false;
-    if (io.op[0] == '#') return false;
+    if (op[0] == '#') return false;
     if (s.it < it1) return false;
     if (imod(s.it - it1, dit) != 0) return false;
     if (io.field != field) return false;
-    char op2 = io.op.size() > 1 ? io.op[1] : ' ';
+    char op2 = op.size() > 1 ? op[1] : ' ';
     if (pass == '<' && op2 == '>') return false;
     if (pass == '>' && op2 != '>') return false;
     return true;
@@ -312,12 +315,19 @@ struct PointGeom {
     float xi[3];
     bool plane[3];
 };
-static void point_geom(Solver& s, const IoOp& io, const FieldView& f, PointGeom& P) {
+// probe: a '.>' op of a partitioned run, whose stencil may reach the halo
+// planes of the l split (they hold the neighbours' current values); it is
+// taken by the part whose core holds the stencil's upper plane
+static void point_geom(Solver& s, const IoOp& io, const FieldView& f, PointGeom& P, bool probe = false) {
     const Geom& g = s.g;
     for (int i = 0; i < 3; i++) {
         int i3, i4;
         if (io.reg == 'n') { i3 = g.i1node[i]; i4 = g.i2node[i]; P.xi[i] = io.x1[i] - (float)g.nnoff[i] + 1.0f; }
         else { i3 = g.i1cell[i]; i4 = g.i2cell[i]; P.xi[i] = io.x1[i] - (float)g.nnoff[i] + 0.5f; }
+        if (probe && s.nparts > 1 && i == 2) {
+            if (s.part > 0) i3 = 1;
+            if (s.part < s.nparts - 1) i4 = g.nm[2];
+        }
         int fl = (int)std::floor(P.xi[i]);
         P.i1[i] = std::max(i3, fl);
         P.i2[i] = std::min(i4, fl + 1);
@@ -378,8 +388,35 @@ bool point_weights(Solver& s, IoOp& io, const FieldView& f, std::vector<PointWei
     return true;
 }
 
+// file-name suffix of a process's own part of a region (mpin / mpout 0)
+static std::string part_suffix(const Solver& s) {
+    char b[16];
+    snprintf(b, sizeof b, "-%06d", s.part);
+    return b;
+}
+
 static void file_write(Solver& s, IoOp& io, const float* data, int recl, int nrec, const std::string& filename, int m, int o) {
     std::string fn = s.path(filename);
+    if (s.nparts > 1 && s.prm.mpout != 0 && io.grecl != (long long)recl) {
+        // a partitioned run's shared file: each part writes its part of every
+        // record at its offset (the reference writes with MPI-IO,
+        // input_output.f90:494-508); no part checks that the file is new
+        const int fd = ::open(fn.c_str(), O_WRONLY | O_CREAT, 0644);
+        if (fd < 0) throw SordError(SORD_E_IO, "cannot open " + filename);
+        for (int r = 0; r < nrec; r++) {
+            const size_t bytes = sizeof(float) * (size_t)recl;
+            const off_t pos = (off_t)(((size_t)(o + r) * (size_t)io.grecl + (size_t)io.loff) * sizeof(float));
+            size_t done = 0;
+            while (done < bytes) {
+                const ssize_t w = pwrite(fd, reinterpret_cast<const char*>(data + (size_t)r * recl) + done, bytes - done,
+                                         pos + (off_t)done);
+                if (w <= 0) { ::close(fd); throw SordError(SORD_E_IO, "write failed: " + filename); }
+                done += (size_t)w;
+            }
+        }
+        ::close(fd);
+        return;
+    }
     FILE* fp;
     if (!io.open && o == 0) {
         fp = fopen(fn.c_str(), "rb");
@@ -423,7 +460,7 @@ static int probe_id(Solver& s, size_t opi, const IoOp& io, const FieldView& f) {
     if (T.id_of_op.size() != s.ops.size()) T.id_of_op.assign(s.ops.size(), -1);
     if (T.id_of_op[opi] >= 0) return T.id_of_op[opi];
     PointGeom P;
-    point_geom(s, io, f, P);
+    point_geom(s, io, f, P, true);
     int i1[3], i2[3];
     for (int i = 0; i < 3; i++) { i1[i] = P.i1[i]; i2[i] = P.i2[i]; if (f.n[i] == 1) { i1[i] = i2[i] = 1; } }
     Probe pr;
@@ -577,7 +614,7 @@ static void flush_output(Solver& s, IoOp& io, int n3[3], int m3[3]) {
     int m4 = (it2 - it1) / dit + 1;
     int o4 = (s.it - it1) / dit + 1 - n4;
     std::string filename = io.fname;
-    if ((n3[0] != m3[0] || n3[1] != m3[1] || n3[2] != m3[2]) && s.prm.mpout == 0) filename += "-000000";
+    if ((n3[0] != m3[0] || n3[1] != m3[1] || n3[2] != m3[2]) && s.prm.mpout == 0) filename += part_suffix(s);
     if (!(n3[0] < 1 || n3[1] < 1 || n3[2] < 1 || n4 < 1)) write_async(s, io, n4, filename, m4, o4);
     io.ib = 0;
     if (s.it == it2 || n3[0] < 1 || n3[1] < 1 || n3[2] < 1 || n4 < 1) {
@@ -676,7 +713,8 @@ static bool device_volume_input(Solver& s, IoOp& io, FieldView f, const int* i1,
     if (code < 0 || io.ib >= 0 || s.it != it2) return false;
     if (code != 0 && f.p == s.d.s1) return false;  // f aliases the staging scratch: host path order
     for (int i = 0; i < 3; i++)
-        if (f.n[i] != g.nm[i] || di[i] != 1 || m[i] != n[i] || m[i] == 1 || n[i] < 1) return false;
+        if (f.n[i] != g.nm[i] || di[i] != 1 || (m[i] != n[i] && !(s.nparts > 1 && i == 2)) || m[i] == 1 || n[i] < 1)
+            return false;
     const size_t nsp = (size_t)n[0] * n[1] * n[2];
     if (nsp == 0) return false;
     if (s.stage_cap < nsp) {
@@ -692,7 +730,7 @@ static bool device_volume_input(Solver& s, IoOp& io, FieldView f, const int* i1,
     unsigned* bad = reinterpret_cast<unsigned*>(s.d_stage + nsp);
     SORD_CUDA(cudaMemsetAsync(bad, 0, sizeof(unsigned), s.stream));
     const int o4 = (s.it - it1) / dit;
-    read_to_device(s, io.fname, nsp * (size_t)o4, nsp, s.d_stage);
+    read_to_device(s, io.fname, (size_t)io.grecl * (size_t)o4 + (size_t)io.loff, nsp, s.d_stage);
     Region R;
     for (int i = 0; i < 3; i++) { R.n[i] = f.n[i]; R.i1[i] = i1[i]; R.i2[i] = i2[i]; R.di[i] = 1; }
     R.vsy = g.sy;
@@ -731,14 +769,26 @@ static void disk_input(Solver& s, IoOp& io, FieldView f, int* i1, int* i2, int* 
         int n4 = std::min(io.nb, (it2 - s.it) / dit + 1);
         int o4 = (s.it - it1) / dit;
         std::string filename = io.fname;
-        if ((n[0] != m[0] || n[1] != m[1] || n[2] != m[2]) && s.prm.mpin == 0) filename += "-000000";
+        if ((n[0] != m[0] || n[1] != m[1] || n[2] != m[2]) && s.prm.mpin == 0) filename += part_suffix(s);
         io.ib = 0;
         if (n[0] < 1 || n[1] < 1 || n[2] < 1 || n4 < 1) { io.hbuf.clear(); io.op = "#"; return; }
         FILE* fp = fopen(s.path(filename).c_str(), "rb");
         if (!fp) throw SordError(SORD_E_IO, "cannot open " + filename);
         size_t recl = (size_t)nsp;
-        fseek(fp, (long)(recl * sizeof(float) * (size_t)o4), SEEK_SET);
-        size_t got = fread(io.hbuf.data(), sizeof(float), recl * n4, fp);
+        // records of the whole region, this process's part of each (one
+        // read when that is the whole record)
+        const bool whole = s.prm.mpin == 0 || (size_t)io.grecl == recl;
+        const size_t frecl = whole ? recl : (size_t)io.grecl, foff = whole ? 0 : (size_t)io.loff;
+        size_t got = 0;
+        if (frecl == recl) {
+            fseek(fp, (long)(recl * sizeof(float) * (size_t)o4), SEEK_SET);
+            got = fread(io.hbuf.data(), sizeof(float), recl * n4, fp);
+        } else {
+            for (int r = 0; r < n4; r++) {
+                fseek(fp, (long)(((size_t)(o4 + r) * frecl + foff) * sizeof(float)), SEEK_SET);
+                got += fread(io.hbuf.data() + (size_t)r * recl, sizeof(float), recl, fp);
+            }
+        }
         fclose(fp);
         if (got != recl * n4) throw SordError(SORD_E_IO, "short read " + filename);
         for (size_t q = 0; q < recl * n4; q++) {
@@ -834,7 +884,7 @@ static void field_io_op(Solver& s, size_t opi, FieldView f, ProbeBatch& batch) {
     int i1[3], i2[3], i3[3], i4[3], di[3], m[4], n[4], o[4];
     char op2 = io.op.size() > 1 ? io.op[1] : ' ';
     PointGeom P;
-    point_geom(s, io, f, P);
+    point_geom(s, io, f, P, io.op == ".>");
     if (io.op[0] == '.') {
         for (int i = 0; i < 3; i++) { i1[i] = P.i1[i]; i2[i] = P.i2[i]; di[i] = 1; }
     } else {
@@ -907,6 +957,12 @@ static void field_io_op(Solver& s, size_t opi, FieldView f, ProbeBatch& batch) {
             if (n[i] < 1) { io.op = "#"; return; }
             i1[i] = 1; i2[i] = 1; m[i] = 1; n[i] = 1; o[i] = 0;
         }
+    // this process's part of each file record: contiguous when only l is
+    // split (a partitioned run); the whole record otherwise
+    io.grecl = (long long)m[0] * m[1] * m[2];
+    io.loff = (long long)o[0] + (long long)m[0] * ((long long)o[1] + (long long)m[1] * o[2]);
+    if ((n[0] != m[0] || n[1] != m[1]) && n[2] > 1 && n[0] > 0 && n[1] > 0 && n[2] > 0 && s.nparts > 1)
+        throw SordError(SORD_E_PARAM, "partitioned run: a disk region split in j or k");
     if (op2 == '<') {
         disk_input(s, io, f, i1, i2, di, m, n, o, &P);
         return;
@@ -969,10 +1025,18 @@ void field_io(Solver& s, const char* passes, const char* field, FieldView f) {
         ProbeBatch batch;
         batch.count = 0;
         batch.probes = nullptr;
+        bool any = false;
         for (size_t i = 0; i < s.ops.size(); i++) {
+            if (applies(s, s.ops[i], field, pass, true)) any = true;
             if (!applies(s, s.ops[i], field, pass)) continue;
             field_io_op(s, i, f, batch);
         }
+        // a partitioned run takes the halo planes of an input volume field
+        // from its neighbours (input_output.f90:218-238, 367 swap the staged
+        // values); `any` goes by the ops as read, so every part makes the
+        // same exchanges
+        if (pass == '<' && any && s.nparts > 1 && f.n[0] == s.g.nm[0] && f.n[1] == s.g.nm[1] && f.n[2] == s.g.nm[2])
+            halo_exchange(s, &f.p, 1);
         if (batch.count) {
             k_probe<<<1, 128, 0, s.stream>>>(f.p, batch);
             FCHK(s);

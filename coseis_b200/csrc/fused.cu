@@ -393,7 +393,9 @@ __global__ void __launch_bounds__(SJ * SK, GEOM == GEOM_GENERAL ? 1 : 2) k_shell
 #pragma unroll
                     for (int t = 0; t < 8; t++) B[2][t] = A.br.bnc[2][t];
             }
-            const bool own = owncol && l >= L0;
+            // a cell plane below the first node plane is a halo of a partitioned run;
+            // the part takes it (the PML g memory of that halo cell advances here)
+            const bool own = owncol && (l >= L0 || l < g.i1node[2]);
             if constexpr (F) {
                 // strain of an interior cell: gradients of w = u + gam v
 #pragma unroll

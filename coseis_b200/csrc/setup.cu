@@ -308,15 +308,44 @@ static void setup_dimensions(Solver& s) {
         case 'z': ifn = 3; break;
         default: throw SordError(SORD_E_PARAM, "Error in faultnormal");
     }
-    if (P.nproc3[0] * P.nproc3[1] * P.nproc3[2] != 1) throw SordError(SORD_E_PARAM, "MPI build required for multiprocessing");
+    const bool part = s.nparts != 1;
+    if (!part && P.nproc3[0] * P.nproc3[1] * P.nproc3[2] != 1)
+        throw SordError(SORD_E_PARAM, "a run split by nproc3 needs sord_create_part for each part");
+    if (part) {
+        // a run split along l (sord_create_part)
+        if (P.nproc3[0] != 1 || P.nproc3[1] != 1 || P.nproc3[2] < 1)
+            throw SordError(SORD_E_PARAM, "partitioned runs split l only: nproc3 must be [1, 1, P]");
+        if (ifn) throw SordError(SORD_E_PARAM, "partitioned runs take no fault");
+        if (P.gridnoise > 0.f) throw SordError(SORD_E_PARAM, "partitioned runs take no gridnoise (random per process)");
+        for (const IoOp& io : s.ops)
+            if (io.op.find('~') != std::string::npos)
+                throw SordError(SORD_E_PARAM, "partitioned runs take no random ('~') field ops (random per process)");
+    }
     for (int i = 0; i < 3; i++) {
         if (g.nn[i] < 1) throw SordError(SORD_E_PARAM, "Error in shape");
         g.nhalo[i] = 1;
     }
     if (ifn) g.nhalo[ifn - 1] = 2;
     for (int i = 0; i < 3; i++) {
-        int nl3 = std::max(g.nn[i], g.nhalo[i]);
-        g.nnoff[i] = -g.nhalo[i];
+        // setup.f90:33-38 and 48-50: planes per part and this part's offset
+        int nl3 = std::max(g.nn[i], g.nhalo[i]), ip3 = 0;
+        if (part && i == 2) {
+            nl3 = std::max((g.nn[i] - 1) / P.nproc3[2] + 1, g.nhalo[i]);
+            const int nproc = (g.nn[i] - 1) / nl3 + 1;
+            if (s.part >= nproc)
+                throw SordError(SORD_E_PARAM, "part " + std::to_string(s.part) + " beyond the " + std::to_string(nproc) +
+                                                  " parts that nproc3 gives for " + std::to_string(g.nn[i]) + " planes");
+            s.nparts = nproc;
+            ip3 = s.part;
+            // the PML of an l face, and one plane more, inside the first
+            // or last part (the PML memories are kept per face)
+            const int near = P.i1pml[2], far = P.i2pml[2], last0 = nl3 * (nproc - 1) + 1;
+            if ((near >= 1 && nl3 < near + 1) || (far <= g.nn[2] && last0 > far - 1))
+                throw SordError(SORD_E_PARAM, "partitioned runs need the PML of each l face and one plane more "
+                                              "inside the first and last part (" + std::to_string(nl3) +
+                                              " planes per part)");
+        }
+        g.nnoff[i] = nl3 * ip3 - g.nhalo[i];
         int nl = std::min(nl3, g.nn[i] - g.nnoff[i] - g.nhalo[i]);
         g.nm[i] = nl + 2 * g.nhalo[i];
         g.i1bc[i] = 1 - g.nnoff[i];
@@ -411,6 +440,10 @@ static void init_grid(Solver& s) {
         for (int i = 0; i < 3; i++) { a1[i] = g.i1bc[i] - 1; a2[i] = g.i2bc[i] + 1; }
         float* X[3] = {d.x[0], d.x[1], d.x[2]};
         launch_vector_bc(s, X, bc, bc, a1, a2);
+        // a partitioned run takes the coordinates of its halo planes from
+        // its neighbours (the volume and bracket stencils of its halo cells
+        // read them)
+        halo_exchange(s, X, 3);
     }
     field_io(s, ">", "x", vol(s, d.x[0]));
     field_io(s, ">", "y", vol(s, d.x[1]));
@@ -464,6 +497,13 @@ static void init_material(Solver& s) {
         maxg[q] = -dev_reduce_min(s, vol(s, arrs[q]), a1, a2);
         maxg[q + 7] = dev_reduce_max(s, vol(s, arrs[q]), a1, a2);
     }
+    {
+        // extrema over all parts of a partitioned run (material_model.f90:138)
+        double mg[14];
+        for (int q = 0; q < 14; q++) mg[q] = maxg[q];
+        all_reduce(s, mg, 14, 0);
+        for (int q = 0; q < 14; q++) maxg[q] = (float)mg[q];
+    }
     field_io(s, ">", "rho", vol(s, d.mr));
     field_io(s, ">", "vp", vol(s, d.s1));
     field_io(s, ">", "vs", vol(s, d.s2));
@@ -481,7 +521,7 @@ static void init_material(Solver& s) {
     float r = g.dx[0] * g.dx[0] + g.dx[1] * g.dx[1] + g.dx[2] * g.dx[2];
     float cfl1 = g.dt * vmx * std::sqrt(3.0f / r);
     float cfl2 = g.dt * vmx * 3.0f / std::sqrt(r);
-    FILE* fp = fopen(s.path("material.json").c_str(), "w");
+    FILE* fp = s.part == 0 ? fopen(s.path("material.json").c_str(), "w") : nullptr;
     if (fp) {
         fprintf(fp, "{\n");
         fprintf(fp, "    \"cfl\": [%.9g, %.9g],\n", (double)cfl1, (double)cfl2);
@@ -611,6 +651,7 @@ static void resample_material(Solver& s) {
     LAUNCH_CHECK(s);
     dev_rinvert(s, d.mr, nv);
     launch_scalar_bc(s, d.mr, g.nm, P.bc1, P.bc2, g.i1bc, g.i2bc);
+    halo_exchange(s, &d.mr, 1);  // material_resample.f90:20
     dev_rinvert(s, d.vc, nv);
     {
         int bc[3] = {4, 4, 4}, a1[3], a2[3];
@@ -623,6 +664,7 @@ static void resample_material(Solver& s) {
     LAUNCH_CHECK(s);
     dev_set_halo(s, vol(s, d.gam), 0.f, g.i1bc, g.i2bc);
     launch_scalar_bc(s, d.gam, g.nm, P.bc1, P.bc2, g.i1bc, g.i2bc);
+    halo_exchange(s, &d.gam, 1);  // material_resample.f90:34
     {
         int a2[3];
         for (int i = 0; i < 3; i++) a2[i] = g.i2bc[i] - 1;

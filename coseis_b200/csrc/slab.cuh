@@ -207,7 +207,9 @@ __global__ void __launch_bounds__(SJ * SK, GEOM == GEOM_GENERAL ? 1 : 2) k_slab(
         const bool sj = cnj || cfj, sk = cnk || cfk, sl = cnl || cfl;
         const bool anyS = sj || sk || sl;
         const bool inEc = ceJ && ceK && (!DL || (l >= g.i1pml[2] && l <= g.i2pml[2] - 1));
-        const bool own = owncol && l >= L0;
+        // a cell plane below the first node plane is a halo of a partitioned run;
+        // the part takes it (the PML g memory of that halo cell advances here)
+        const bool own = owncol && (l >= L0 || l < g.i1node[2]);
         // brackets scaled by h; divergence brackets = negated gradient brackets
         float B[3][8];
         float cnb[NDIR > 0 ? NDIR : 1][8];

@@ -54,6 +54,12 @@ struct IoOp {
     float* dbuf = nullptr;     // device output buffer (bufn * nb)
     std::vector<float> hbuf;   // host staging of input / output records
     bool open = false;         // output file created (direct-access append state)
+    // disk ops: floats per record in the file (the whole region) and the
+    // offset of this process's part of it (nonzero in a partitioned run)
+    long long grecl = 0, loff = 0;
+    // the op as read from sord.in: `op` becomes "#" where this process holds
+    // none of the region, op0 is the same on every part of a partitioned run
+    std::string op0;
 };
 
 Params parse_sord_in(const std::string& text, std::vector<IoOp>& ops);
@@ -237,6 +243,8 @@ struct FieldView {
 void field_io(Solver& s, const char* passes, const char* field, FieldView f);
 void field_io_flush_all(Solver& s);
 InjectList upload_inject(Solver& s, int slot, const std::vector<Inject>& e);  // through the slot's ring (api.cu)
+void halo_exchange(Solver& s, float* const* fields, int nf);  // halo planes along l from the neighbouring parts
+void all_reduce(Solver& s, double* vals, int n, int op);      // over the parts: op 0 max, 1 sum
 void writer_drain(Solver& s);  // every queued output record on disk; throws the first write error
 void writer_free(Solver& s);
 bool field_active(Solver& s, const char* field, char pass);
@@ -320,6 +328,15 @@ struct Solver {
     FusedPlan* fplan = nullptr;
     struct AdjointState* adj = nullptr;  // checkpoints and adjoint fields (adjoint.cu)
     struct OutWriter* writer = nullptr;  // output-record writer thread (fieldio.cu)
+    // partitioned run (sord_create_part): part `part` of `nparts` slabs along
+    // l, the caller's halo-exchange and reduction callbacks, and the device
+    // buffers of the exchange (send / receive planes below and above)
+    int part = 0, nparts = 1;
+    sord_halo_fn halo_fn = nullptr;
+    sord_reduce_fn reduce_fn = nullptr;
+    void* cb_ctx = nullptr;
+    float* xbuf = nullptr;
+    size_t xcap = 0;
     bool mem_attached = false;  // holds a reference on the device's memory pool
     cudaEvent_t inj_done[kInjectSlots][kInjectRing] = {};
     int inj_ring[kInjectSlots] = {};

@@ -472,7 +472,8 @@ def stage(args=None, **kwargs):
     job['name'] = 'sord'
     job['executable'] = 'libsordgpu.so'
 
-    # partition (one GPU: the whole mesh is one block)
+    # partition: nproc3 splits l into slabs, one solver handle per slab
+    # (coseis_b200.parallel); j and k stay whole
     nx, ny, nz, nt = prm['shape']
     j, k, l = prm['nproc3']
     nl = [(nx - 1) // j + 1, (ny - 1) // k + 1, (nz - 1) // l + 1]
@@ -484,9 +485,9 @@ def stage(args=None, **kwargs):
     k = (ny - 1) // nl[1] + 1
     l = (nz - 1) // nl[2] + 1
     prm['nproc3'] = [j, k, l]
-    job['nproc'] = n = j * k * l
-    if n > 1:
-        raise Exception('MPI build required for multiprocessing')
+    job['nproc'] = j * k * l
+    if j * k > 1:
+        raise Exception('runs split into processes split l only: nproc3 must be [1, 1, P]')
 
     # resources
     nvars = 23
@@ -517,10 +518,16 @@ def stage(args=None, **kwargs):
 
 
 def run(args=None, **kwargs):
-    """Stage in the current directory and run the CUDA solver in-process."""
+    """Stage in the current directory and run the CUDA solver in-process.
+    A run split by nproc3 = [1, 1, P] runs as P parts, spread over the
+    visible devices (coseis_b200.parallel.run_local)."""
     job, meta = stage(args, **kwargs)
-    from . import _lib
-    _lib.run_directory(os.getcwd())
+    if job['nproc'] > 1:
+        from . import parallel
+        parallel.run_local(os.getcwd(), job['nproc'], devices=range(parallel.device_count()))
+    else:
+        from . import _lib
+        _lib.run_directory(os.getcwd())
     return meta
 
 

@@ -45,6 +45,40 @@ enum {
  * Replaces: the start of `sord.x` (sord/sord.f90:24-37). */
 int sord_create(const char* workdir, const char* sord_in_text, int device, sord_handle** out);
 
+/* Halo exchange of a partitioned run.  The part's halo planes along l are
+ * filled from its neighbours: recv_lo (the plane below the part's first
+ * plane) from part - 1's send_hi, recv_hi from part + 1's send_lo.  Each
+ * buffer holds n floats of device memory, NULL where the part has no such
+ * neighbour.  Called with the part's stream idle; the transfer must be
+ * complete when it returns.  Returns 0 on success.
+ * Replaces: vector_swap_halo / scalar_swap_halo (sord/process_mpi.f90:179-246). */
+typedef int (*sord_halo_fn)(void* ctx, int part, const float* send_lo, float* recv_lo, const float* send_hi,
+                            float* recv_hi, long long n);
+
+/* All-reduce of n host doubles in place over the parts of a run: op 0 the
+ * maximum, op 1 the sum.  Returns 0 on success.
+ * Replaces: rreduce1 / rreduce2 (sord/process_mpi.f90:137-177). */
+typedef int (*sord_reduce_fn)(void* ctx, int part, double* vals, int n, int op);
+
+/* Create part `part` of a run split along l into nproc3[2] parts of the
+ * sord.in parameter nproc3 (= [1, 1, P]): the planes of each part, its
+ * global offset and its index ranges follow sord/setup.f90:33-84 (nl3 =
+ * (nn - 1) / P + 1 planes per part).  Each part runs setup and steps on its
+ * own device; `halo` and `reduce` carry the communication (the halo planes
+ * of coordinates, mass and viscosity at setup, of v, u and a after every
+ * step; material extrema and statistics).  Output files are shared: each
+ * part writes its planes at their offsets (mpout = 1); part 0 writes the
+ * statistics files and material.json.  Rejected (SORD_E_PARAM): nproc3
+ * splitting j or k, a fault, gridnoise or random ('~') field ops (the
+ * reference seeds these per process, setup.f90:41-44, so they depend on
+ * the split), and a first or last part that does not hold the PML of
+ * its l face and one plane more.  Every step exchanges the halo planes of the acceleration (the
+ * reference's force-halo swap, acceleration.f90:229-233) and, after a fused
+ * step that also advanced v and u, of v and u.
+ * Replaces: one MPI rank of sord.x built with process_mpi.f90. */
+int sord_create_part(const char* workdir, const char* sord_in_text, int device, int part, sord_halo_fn halo,
+                     sord_reduce_fn reduce, void* ctx, sord_handle** out);
+
 /* Advance `nsteps` time steps (sord/sord.f90:39-47: step_time, step_stress,
  * step_accel, stats), including every field-I/O hook of those steps. */
 int sord_step(sord_handle* h, int nsteps);
