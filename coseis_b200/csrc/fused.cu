@@ -1218,7 +1218,17 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
 #pragma unroll
                 for (int d = 0; d < 3; d++) inE = inE && cc[d] >= g.i1pml[d] && cc[d] <= g.i2pml[d] - 1;
             }
-            if (inE && (!F || !kPaired)) {
+            if (FM && inE) {
+                // the four mode sums by butterflies (stencil.cuh: hg_modes)
+                const float y = cur[3];
+#pragma unroll
+                for (int ic = 0; ic < 3; ic++) {
+                    float m[4];
+                    hg_modes<float>(Hc[ic], m);
+#pragma unroll
+                    for (int iq = 0; iq < 4; iq++) he[3 * iq + ic] = m[iq] * y;
+                }
+            } else if (inE && (!F || !kPaired)) {
                 const float y = cur[3];
 #pragma unroll
                 for (int ic = 0; ic < 3; ic++) {
@@ -1255,20 +1265,19 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
             float4* cw = sC + tid;
             cw[0] = make_float4(ed[0], ed[1], ed[2], eo[0]);
             reinterpret_cast<float2*>(sC + NCL)[tid] = make_float2(eo[1], eo[2]);
+            // the reading columns' sums from four shared sums per component
+            // (stencil.cuh: hg_readers_pre / hg_reader)
+            float hr[3][4];
+#pragma unroll
+            for (int ic = 0; ic < 3; ic++) {
+                const float m[4] = {he[ic], he[3 + ic], he[6 + ic], he[9 + ic]};
+                hg_readers_pre<float>(m, hr[ic]);
+            }
 #pragma unroll
             for (int q = 0; q < 4; q++) {
-                const int hu = hg_term(7 - (q + 4)), hl = hg_term(7 - q);
                 float yu[3], yl[3];
 #pragma unroll
-                for (int ic = 0; ic < 3; ic++) {
-                    yu[ic] = hg_neg(0, hu) ? he[ic] : -he[ic];
-                    yl[ic] = hg_neg(0, hl) ? he[ic] : -he[ic];
-#pragma unroll
-                    for (int iq = 1; iq < 4; iq++) {
-                        yu[ic] = hg_neg(iq, hu) ? yu[ic] + he[3 * iq + ic] : yu[ic] - he[3 * iq + ic];
-                        yl[ic] = hg_neg(iq, hl) ? yl[ic] + he[3 * iq + ic] : yl[ic] - he[3 * iq + ic];
-                    }
-                }
+                for (int ic = 0; ic < 3; ic++) hg_reader<float>(hr[ic], q, yu[ic], yl[ic]);
                 float4* cq = cw + (2 + NQ * q) * NCL;
                 cq[0] = make_float4(yu[0], yu[1], yu[2], yl[0]);
                 if constexpr (NDIR == 3) {

@@ -41,19 +41,6 @@ struct LaySl {
     static constexpr size_t bytes = sizeof(float) * (size_t)RAWSZ + sizeof(float4) * (size_t)(3 * NPL * NGN + NCL * NGCF);
 };
 
-// hourglass sums of the 12 cell values (mode iq, component ic at 3 iq + ic)
-// that the node reading this cell as its hourglass_cn term `term` adds to
-// its force (acceleration.f90:190-199 subtracts them)
-__device__ __forceinline__ void reader_sums(const float (&he)[12], int term, float (&y)[3]) {
-#pragma unroll
-    for (int ic = 0; ic < 3; ic++) {
-        float r = hg_neg(0, term) ? he[ic] : -he[ic];
-#pragma unroll
-        for (int iq = 1; iq < 4; iq++) r = hg_neg(iq, term) ? r + he[3 * iq + ic] : r - he[3 * iq + ic];
-        y[ic] = r;
-    }
-}
-
 template <int GEOM, int MASK>
 __global__ void __launch_bounds__(SJ * SK, GEOM == GEOM_GENERAL ? 1 : 2) k_slab(StepArgs A) {
     constexpr int TJ = SJ, TK = SK, TNJ = TJ + 1, TOJ = TJ - 1, TOK = TK - 1;
@@ -297,17 +284,17 @@ __global__ void __launch_bounds__(SJ * SK, GEOM == GEOM_GENERAL ? 1 : 2) k_slab(
             const bool visc = A.hgvisc && anyS;
 #pragma unroll
             for (int ic = 0; ic < 3; ic++) {
-                float H[8], Vh[8];
+                // corner values (corner id order) and their four mode sums
+                // by butterflies (stencil.cuh: hg_modes)
+                float H[8], me[4], mv[4];
 #pragma unroll
-                for (int t = 0; t < 8; t++) {
-                    const int n = hg_corner(t);
-                    H[t] = fmaf(A.dh2, Vc[ic][n], A.hg1 * Uc[ic][n]);
-                    Vh[t] = Vc[ic][n];
-                }
+                for (int n = 0; n < 8; n++) H[n] = fmaf(A.dh2, Vc[ic][n], A.hg1 * Uc[ic][n]);
+                hg_modes<float>(H, me);
+                hg_modes<float>(Vc[ic], mv);
 #pragma unroll
                 for (int iq = 0; iq < 4; iq++) {
-                    const float e = inEc ? hg_sum(H, iq) * y : 0.f;
-                    const float v = visc ? yv * hg_sum(Vh, iq) : 0.f;
+                    const float e = inEc ? me[iq] * y : 0.f;
+                    const float v = visc ? yv * mv[iq] : 0.f;
                     he[3 * iq + ic] = inEc ? e : v;
                     hv[3 * iq + ic] = v;
                 }
@@ -319,12 +306,21 @@ __global__ void __launch_bounds__(SJ * SK, GEOM == GEOM_GENERAL ? 1 : 2) k_slab(
         float4* cw = sC + tid;
         cw[0] = make_float4(ed[0], ed[1], ed[2], eo[0]);
         reinterpret_cast<float2*>(sC + NCL_)[tid] = make_float2(eo[1], eo[2]);
+        // the reading columns' sums from four shared sums per component
+        // (stencil.cuh: hg_readers_pre / hg_reader)
+        float her[3][4], hvr[3][4];
+#pragma unroll
+        for (int ic = 0; ic < 3; ic++) {
+            const float me[4] = {he[ic], he[3 + ic], he[6 + ic], he[9 + ic]};
+            const float mv[4] = {hv[ic], hv[3 + ic], hv[6 + ic], hv[9 + ic]};
+            hg_readers_pre<float>(me, her[ic]);
+            hg_readers_pre<float>(mv, hvr[ic]);
+        }
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-            const int hu = hg_term(7 - (q + 4)), hl = hg_term(7 - q);
             float yu[3], yl[3];
-            reader_sums(he, hu, yu);
-            reader_sums(he, hl, yl);
+#pragma unroll
+            for (int ic = 0; ic < 3; ic++) hg_reader<float>(her[ic], q, yu[ic], yl[ic]);
             if (dual) {
                 // readers of node column (J + 1 - cj, K + 1 - ck), planes l and l + 1
                 const int rj = J + 1 - (q & 1), rk = K + 1 - (q >> 1);
@@ -333,8 +329,8 @@ __global__ void __launch_bounds__(SJ * SK, GEOM == GEOM_GENERAL ? 1 : 2) k_slab(
                 const bool pu = pjk || (DL && (l <= g.i1pml[2] || l >= g.i2pml[2]));
                 const bool pl = pjk || (DL && (l + 1 <= g.i1pml[2] || l + 1 >= g.i2pml[2]));
                 float vu[3], vl[3];
-                reader_sums(hv, hu, vu);
-                reader_sums(hv, hl, vl);
+#pragma unroll
+                for (int ic = 0; ic < 3; ic++) hg_reader<float>(hvr[ic], q, vu[ic], vl[ic]);
 #pragma unroll
                 for (int ic = 0; ic < 3; ic++) {
                     yu[ic] = pu ? vu[ic] : yu[ic];

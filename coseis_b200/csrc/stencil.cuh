@@ -233,6 +233,51 @@ SORD_HD void terrain_brackets_1(float s, const float z[8], float B[8]) {
     B[7] = -B[0];
 }
 
+// Hourglass by butterflies.  With x = (-1)^dj, y = (-1)^dk, z = (-1)^dl at
+// corner n = dj + 2 dk + 4 dl, the four hourglass modes of hourglass_op.f90
+// (hg_sum over the term order) are the sign patterns y z, x z, x y and
+// x y z.  hg_modes forms all four from the corner values by a pruned
+// Walsh-Hadamard transform: pair sums and differences along x, then along
+// y, then along z (18 additions instead of 28).
+template <class T>
+SORD_HD void hg_modes(const T X[8], T m[4]) {
+    T Sy[2], Dx[2], Dxy[2];
+#pragma unroll
+    for (int dl = 0; dl < 2; dl++) {
+        const T* P = X + 4 * dl;
+        const T s0 = P[0] + P[1], s1 = P[2] + P[3], d0 = P[0] - P[1], d1 = P[2] - P[3];
+        Sy[dl] = s0 - s1;
+        Dx[dl] = d0 + d1;
+        Dxy[dl] = d0 - d1;
+    }
+    m[0] = Sy[0] - Sy[1];
+    m[1] = Dx[0] - Dx[1];
+    m[2] = Dxy[0] + Dxy[1];
+    m[3] = Dxy[0] - Dxy[1];
+}
+// The hourglass_cn sums of one cell for the node column q = cj + 2 ck that
+// reads it (the node above the cell: yu, below it: yl), from the cell's four
+// mode values m: the signed sums over the modes of the cell's term for that
+// node (hg_neg(iq, hg_term(7 - p)) at cell position p), which are
+// -(z (y m0 + x m1) + x y (m2 + z m3)) with x = 2 cj - 1, y = 2 ck - 1,
+// z = +1 (yu) or -1 (yl).  hg_readers_pre forms the four shared sums once
+// (a, b, pp, pm), hg_reader the two values of column q from them.
+template <class T>
+SORD_HD void hg_readers_pre(const T m[4], T r[4]) {
+    r[0] = m[0] + m[1];
+    r[1] = m[0] - m[1];
+    r[2] = m[2] + m[3];
+    r[3] = m[2] - m[3];
+}
+template <class T>
+SORD_HD void hg_reader(const T r[4], int q, T& yu, T& yl) {
+    const T a = r[0], b = r[1], pp = r[2], pm = r[3];
+    if (q == 0) { yu = a - pp; yl = -a - pm; }
+    else if (q == 1) { yu = b + pp; yl = pm - b; }
+    else if (q == 2) { yu = pp - b; yl = b + pm; }
+    else { yu = -a - pp; yl = a - pm; }
+}
+
 // F . B with fused multiply-adds (B already scaled by h).
 SORD_HD float dot8(const float F[8], const float B[8]) {
     float d = F[0] * B[0];

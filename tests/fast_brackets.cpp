@@ -5,7 +5,9 @@
 //   * terrain cells (x = x(j), y = y(k)): terrain_brackets_0 / _1 against
 //     brackets_nc_g of directions 0 and 1;
 //   * general cells: -nc[cn_of_nc(t)] against the divergence brackets;
-//   * hg_term, the inverse of hg_corner.
+//   * hg_term, the inverse of hg_corner;
+//   * the hourglass butterflies hg_modes / hg_reader against hg_sum and the
+//     signed mode sums of the reading node's term.
 // Prints the largest error relative to the largest bracket of each cell for
 // both checks.  Built and run by tests/test_stencil.py.
 #include <cmath>
@@ -56,6 +58,32 @@ int main(int argc, char** argv) {
             for (int t = 0; t < 8; t++) m = fmax(m, fabs(nc[t]));
             for (int t = 0; t < 8; t++) ecn = fmax(ecn, fabs(cn[t] + nc[cn_of_nc(t)]) / m);
         }
+    }
+    // hourglass butterflies: hg_modes against hg_sum over the term order, and
+    // hg_reader against the signed mode sums of the reading node's term
+    double ehg = 0;
+    for (int trial = 0; trial < 2000; trial++) {
+        double X[8], W2[8], m[4], r[4];
+        for (int n = 0; n < 8; n++) X[n] = U(rng);
+        for (int t = 0; t < 8; t++) W2[t] = X[hg_corner(t)];
+        hg_modes<double>(X, m);
+        for (int iq = 0; iq < 4; iq++) ehg = fmax(ehg, fabs(m[iq] - hg_sum<double>(W2, iq)));
+        hg_readers_pre<double>(m, r);
+        for (int q = 0; q < 4; q++) {
+            const int hu = hg_term(7 - (q + 4)), hl = hg_term(7 - q);
+            double yu = hg_neg(0, hu) ? m[0] : -m[0], yl = hg_neg(0, hl) ? m[0] : -m[0];
+            for (int iq = 1; iq < 4; iq++) {
+                yu = hg_neg(iq, hu) ? yu + m[iq] : yu - m[iq];
+                yl = hg_neg(iq, hl) ? yl + m[iq] : yl - m[iq];
+            }
+            double bu, bl;
+            hg_reader<double>(r, q, bu, bl);
+            ehg = fmax(ehg, fmax(fabs(bu - yu), fabs(bl - yl)));
+        }
+    }
+    if (ehg > 1e-14) {
+        printf("hourglass butterflies differ: %.3e\n", ehg);
+        return 1;
     }
     // hg_term inverts hg_corner (the fast kernel finds a cell's hourglass term by its corner)
     for (int t = 0; t < 8; t++)
