@@ -87,7 +87,11 @@ struct Lay {
     // (terrain: 2 groups per q, the lower-cell brackets of all q in 2 float2 groups)
     static constexpr int NQ = NDIR == 3 ? 3 : 2;
     static constexpr int NGCF = 2 + 4 * NQ + (NDIR == 2 ? 2 : 0);
-    static constexpr size_t bytes_fm = sizeof(float) * (size_t)RAWSZ + sizeof(float4) * (size_t)(3 * NPL * NGN + NCL * NGCF);
+    // the interior kernel in fast arithmetic stores, per reading node column
+    // q, that node's whole force terms from the cell: (fu_x, fu_y, fu_z,
+    // fl_x) as float4 group q and (fl_y, fl_z) as float2 in groups 4-5
+    static constexpr int NGCR = 6;
+    static constexpr size_t bytes_fm = sizeof(float) * (size_t)RAWSZ + sizeof(float4) * (size_t)(3 * NPL * NGN + NCL * NGCR);
 };
 // scalar field numbers of the node and cell groups
 __host__ __device__ constexpr int nf_co(int c) { return c == 0 ? 3 : c == 1 ? 7 : 8; }
@@ -756,6 +760,16 @@ __device__ __forceinline__ void zero_cell_fm(float4* sC, int tid, int ncl) {
     }
 }
 
+// Zero one cell of the interior kernel's fast-arithmetic cell plane (Lay:
+// NGCR groups: four float4 groups, then four float2 arrays).
+__device__ __forceinline__ void zero_cell_fr(float4* sC, int tid, int ncl) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        sC[q * ncl + tid] = make_float4(0.f, 0.f, 0.f, 0.f);
+        reinterpret_cast<float2*>(sC + 4 * ncl)[q * ncl + tid] = make_float2(0.f, 0.f);
+    }
+}
+
 // Interior kernel: tiles of 31 x 7 nodes from (A.jf, A.kf), planes A.lf0..A.lf1,
 // strictly inside the non-PML region, with no PML or boundary terms.
 // FM (fast arithmetic): fused multiply-adds, brackets scaled by h once per
@@ -919,7 +933,7 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
         const bool valid = (F || cellcol) && l >= g.i1cell[2] && l <= g.i2cell[2];
         if (!valid) {
             if constexpr (FM) {
-                zero_cell_fm<NDIR, NQ>(sC, tid, NCL);
+                zero_cell_fr(sC, tid, NCL);
             } else {
                 float4* cw = sC + cs * (NGC * NCL) + tid;
 #pragma unroll
@@ -1258,15 +1272,14 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
             }
         }
         if constexpr (FM) {
-            // fast layout: for each node column q that reads this cell, the
-            // hourglass sum it adds to the node above the cell (u) and below
-            // it (l) -- the signs of hourglass_cn terms hg_term(7 - p) at cell
-            // position p -- and its divergence brackets
-            float4* cw = sC + tid;
-            cw[0] = make_float4(ed[0], ed[1], ed[2], eo[0]);
-            reinterpret_cast<float2*>(sC + NCL)[tid] = make_float2(eo[1], eo[2]);
-            // the reading columns' sums from four shared sums per component
-            // (stencil.cuh: hg_readers_pre / hg_reader)
+            // fast layout: for each node column q = cj + 2 ck that reads this
+            // cell, the cell's whole terms of that column's force at node
+            // plane l (fu, the node above the cell) and l + 1 (fl, the node
+            // below it): the hourglass_cn sums (the signs of hourglass_cn
+            // terms hg_term(7 - p) at cell position p, stencil.cuh:
+            // hg_reader) plus the divergence of the cell's stress with that
+            // node's diff_cn brackets
+            const float S[6] = {ed[0], ed[1], ed[2], eo[0], eo[1], eo[2]};
             float hr[3][4];
 #pragma unroll
             for (int ic = 0; ic < 3; ic++) {
@@ -1275,22 +1288,27 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
             }
 #pragma unroll
             for (int q = 0; q < 4; q++) {
-                float yu[3], yl[3];
+                const int cj = q & 1, ck = q >> 1;
+                const int tu = cj + 2 + 4 * ck, tl = cj + 4 * ck;
+                float Bu[3], Bl[3];
 #pragma unroll
-                for (int ic = 0; ic < 3; ic++) hg_reader<float>(hr[ic], q, yu[ic], yl[ic]);
-                float4* cq = cw + (2 + NQ * q) * NCL;
-                cq[0] = make_float4(yu[0], yu[1], yu[2], yl[0]);
-                if constexpr (NDIR == 3) {
-                    const int tu = (q & 1) + 2 + 4 * (q >> 1), tl = (q & 1) + 4 * (q >> 1);
-                    cq[NCL] = make_float4(yl[1], yl[2], cnb[0][tu], cnb[1][tu]);
-                    cq[2 * NCL] = make_float4(cnb[0][tl], cnb[1][tl], cnb[NDIR - 1][tu], cnb[NDIR - 1][tl]);
-                } else if constexpr (NDIR == 2) {
-                    const int tu = (q & 1) + 2 + 4 * (q >> 1), tl = (q & 1) + 4 * (q >> 1);
-                    cq[NCL] = make_float4(yl[1], yl[2], cnb[0][tu], cnb[1][tu]);
-                    reinterpret_cast<float2*>(sC + (2 + 4 * NQ) * NCL)[q * NCL + tid] = make_float2(cnb[0][tl], cnb[1][tl]);
-                } else {
-                    cq[NCL] = make_float4(yl[1], yl[2], 0.f, 0.f);
+                for (int a = 0; a < 3; a++) {
+                    Bu[a] = a < NDIR ? cnb[a < NDIR ? a : 0][tu] : A.brh.bcn[a][tu];
+                    Bl[a] = a < NDIR ? cnb[a < NDIR ? a : 0][tl] : A.brh.bcn[a][tl];
                 }
+                float fu[3], fl[3];
+#pragma unroll
+                for (int ic = 0; ic < 3; ic++) hg_reader<float>(hr[ic], q, fu[ic], fl[ic]);
+#pragma unroll
+                for (int ic = 0; ic < 3; ic++)
+#pragma unroll
+                    for (int iid = 0; iid < 3; iid++) {
+                        const int id = (ic + iid) % 3, comp = ic == id ? ic : 3 + (3 - ic - id);
+                        fu[ic] = fmaf(S[comp], Bu[id], fu[ic]);
+                        fl[ic] = fmaf(S[comp], Bl[id], fl[ic]);
+                    }
+                sC[q * NCL + tid] = make_float4(fu[0], fu[1], fu[2], fl[0]);
+                reinterpret_cast<float2*>(sC + 4 * NCL)[q * NCL + tid] = make_float2(fl[1], fl[2]);
             }
         } else {
             WRITE_CELL(cs, ed, eo, he, cnb);
@@ -1560,55 +1578,25 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
     float fc[3] = {0.f, 0.f, 0.f};
     auto nodes_fm = [&](int l, bool finish) {
         if (!outcol) return;
-        float fu[3] = {fc[0], fc[1], fc[2]}, fl[3] = {0.f, 0.f, 0.f};
+        // the four cells of plane l around the node column: their terms for
+        // node l (above them) and for node l + 1 (below), the latter carried
+        float fu[3] = {fc[0], fc[1], fc[2]}, fl[3];
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-            const int cj = q & 1, ck = q >> 1;
-            const int ci = tid + cj + FJ * ck;  // the cell (J + cj, K + ck)
-            const float4 a = sC[ci];
-            const float2 e = reinterpret_cast<const float2*>(sC + NCL)[ci];
-            const float S[6] = {a.x, a.y, a.z, a.w, e.x, e.y};
-            const float4* cq = sC + (2 + NQ * q) * NCL + ci;
-            const float4 y0 = cq[0], y1 = cq[NCL];
-            // diff_cn terms of this cell for node l (above it: cl = 1) and node l + 1 (cl = 0)
-            const int tu = cj + 2 + 4 * ck, tl = cj + 4 * ck;
-            float Bu[3], Bl[3];
-            if constexpr (NDIR == 3) {
-                const float4 y2 = cq[2 * NCL];
-                Bu[0] = y1.z;
-                Bu[1] = y1.w;
-                Bl[0] = y2.x;
-                Bl[1] = y2.y;
-                Bu[2] = y2.z;
-                Bl[2] = y2.w;
-            } else if constexpr (NDIR == 2) {
-                const float2 bl = reinterpret_cast<const float2*>(sC + (2 + 4 * NQ) * NCL)[q * NCL + ci];
-                Bu[0] = y1.z;
-                Bu[1] = y1.w;
-                Bl[0] = bl.x;
-                Bl[1] = bl.y;
-            }
-#pragma unroll
-            for (int id = NDIR; id < 3; id++) {
-                Bu[id] = A.brh.bcn[id][tu];
-                Bl[id] = A.brh.bcn[id][tl];
-            }
-#pragma unroll
-            for (int ic = 0; ic < 3; ic++)
-#pragma unroll
-                for (int iid = 0; iid < 3; iid++) {
-                    const int id = (ic + iid) % 3, comp = ic == id ? ic : 3 + (3 - ic - id);
-                    fu[ic] = fmaf(S[comp], Bu[id], fu[ic]);
-                    fl[ic] = fmaf(S[comp], Bl[id], fl[ic]);
-                }
-            // hourglass_cn: the cell's signed sums for the nodes above and below it
-            if (A.hourglass) {
-                fu[0] = fu[0] + y0.x;
-                fu[1] = fu[1] + y0.y;
-                fu[2] = fu[2] + y0.z;
-                fl[0] = fl[0] + y0.w;
-                fl[1] = fl[1] + y1.x;
-                fl[2] = fl[2] + y1.y;
+            const int ci = tid + (q & 1) + FJ * (q >> 1);  // the cell (J + cj, K + ck)
+            const float4 a = sC[q * NCL + ci];
+            const float2 b = reinterpret_cast<const float2*>(sC + 4 * NCL)[q * NCL + ci];
+            fu[0] = fu[0] + a.x;
+            fu[1] = fu[1] + a.y;
+            fu[2] = fu[2] + a.z;
+            if (q == 0) {
+                fl[0] = a.w;
+                fl[1] = b.x;
+                fl[2] = b.y;
+            } else {
+                fl[0] = fl[0] + a.w;
+                fl[1] = fl[1] + b.x;
+                fl[2] = fl[2] + b.y;
             }
         }
 #pragma unroll
