@@ -887,16 +887,46 @@ def run_ensemble_bench(n, nthreads, device, nt=ENS_NT, seed=SEED):
                    for a, b, o in zip(ser, ens, outs))
         nfiles = sum(len(o) for o in outs)
         nodes = [int(np.prod(rupture_scenario(i, seed, nt)[0]['shape'][:3])) for i in range(n)]
+        account = ensemble_account(stage_scenarios(range(0, n, 8), os.path.join(work, 'account'), seed, nt),
+                                   device, nt)
         return {'metric': 'scenarios/s', 'value': n / t_ens, 'unit': 'scenarios/s',
                 'one_at_a_time': n / t_ser, 'speedup': t_ser / t_ens, 'scenarios': n,
                 'concurrent': nthreads, 'steps': nt, 'wall_s': round(t_ens, 3), 'serial_wall_s': round(t_ser, 3),
                 'node_updates_per_s': float(sum(nodes)) * nt / t_ens, 'outputs_identical': bool(same),
-                'files_compared': nfiles,
+                'files_compared': nfiles, 'account': account,
                 'arithmetic': os.environ.get('SORD_ARITHMETIC', 'reference'),
                 'workload': 'rupture ensemble: seeded grids 64x64x64..192x96x96, dx 100 m, dt 0.008 s, '
                             'slip-weakening +z fault, seeded friction / stresses (scenarios 0..%d)' % (n - 1)}
     finally:
         shutil.rmtree(work, ignore_errors=True)
+
+
+def ensemble_account(dirs, device, nt):
+    """Where one scenario's time goes, on a sample of freshly staged
+    scenarios run one after another through the handle calls: setup from the staged
+    files (host clock), the nt steps on the device (CUDA events around one
+    sord_step call), the rest of the call (output files, host clock) and
+    teardown.  Per scenario, averaged over the sample."""
+    from coseis_b200 import _lib
+    t = {'setup': 0.0, 'steps_device': 0.0, 'steps_host': 0.0, 'teardown': 0.0}
+    for d in dirs:
+        text = open(os.path.join(d, 'sord.in')).read()
+        t0 = time.time()
+        s = _lib.Solver(d, text, device=device)
+        t1 = time.time()
+        s.step(nt)
+        t2 = time.time()
+        dev = s.last_step_ms() / 1e3
+        s.close()
+        t3 = time.time()
+        t['setup'] += t1 - t0
+        t['steps_device'] += dev
+        t['steps_host'] += t2 - t1
+        t['teardown'] += t3 - t2
+    n = max(len(dirs), 1)
+    out = {k + '_ms': round(1e3 * v / n, 2) for k, v in t.items()}
+    out['sample'] = len(dirs)
+    return out
 
 
 def wave_workload(shape):

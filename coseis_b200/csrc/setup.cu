@@ -736,16 +736,27 @@ static void rect_check(Solver& s) {
 void fault_init(Solver& s);
 
 void setup_all(Solver& s) {
-    setup_dimensions(s);
-    allocate_arrays(s);
-    init_grid(s);
-    init_material(s);
-    init_pml(s);
-    init_finite_source(s);
-    fault_init(s);
-    resample_material(s);
-    rect_check(s);
+    // SORD_SETUP_TIMES=1: wait for the device after each phase and print the
+    // phases' wall times (ms) to stderr, for finding where setup goes
+    const char* env = getenv("SORD_SETUP_TIMES");
+    const bool timed = env && env[0] == '1';
+    static const char* names[9] = {"dimensions", "allocate", "grid", "material", "pml", "finite_source", "fault",
+                                   "resample", "mesh_class"};
+    void (*phase[9])(Solver&) = {setup_dimensions, allocate_arrays, init_grid, init_material, init_pml,
+                                 init_finite_source, fault_init, resample_material, rect_check};
+    double ms[9];
+    for (int i = 0; i < 9; i++) {
+        const long long t0 = s.clock_us();
+        phase[i](s);
+        if (timed) SORD_CUDA(cudaStreamSynchronize(s.stream));
+        ms[i] = 1e-3 * (double)(s.clock_us() - t0);
+    }
     SORD_CUDA(cudaStreamSynchronize(s.stream));
+    if (timed) {
+        fprintf(stderr, "{\"setup_ms\": {");
+        for (int i = 0; i < 9; i++) fprintf(stderr, "%s\"%s\": %.3f", i ? ", " : "", names[i], ms[i]);
+        fprintf(stderr, "}}\n");
+    }
 }
 
 }  // namespace sordgpu
