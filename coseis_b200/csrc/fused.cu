@@ -91,7 +91,11 @@ struct Lay {
     // q, that node's whole force terms from the cell: (fu_x, fu_y, fu_z,
     // fl_x) as float4 group q and (fl_y, fl_z) as float2 in groups 4-5
     static constexpr int NGCR = 6;
-    static constexpr size_t bytes_fm = sizeof(float) * (size_t)RAWSZ + sizeof(float4) * (size_t)(3 * NPL * NGN + NCL * NGCR);
+    // ... and on rectilinear and terrain meshes copies each node plane
+    // straight into the ring as raw (u, gam), (v, z) groups: no staging plane
+    static constexpr bool RAWRING = GEOM != GEOM_GENERAL;
+    static constexpr size_t bytes_fm = sizeof(float) * (size_t)(RAWRING ? 0 : RAWSZ) +
+                                       sizeof(float4) * (size_t)(3 * NPL * NGN + NCL * NGCR);
 };
 // scalar field numbers of the node and cell groups
 __host__ __device__ constexpr int nf_co(int c) { return c == 0 ? 3 : c == 1 ? 7 : 8; }
@@ -781,8 +785,12 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
     using L = Lay<GEOM>;
     constexpr int NGN = L::NGN, NGC = L::NGC, NDIR = L::NDIR;
     extern __shared__ float4 sm4[];
+    // fast arithmetic on rectilinear and terrain meshes: the ring holds the
+    // raw (u, gam) and (v, z) of each node, copied in by cp.async, and a
+    // cell forms w and the hourglass input of its corners from them
+    constexpr bool RR = FM && L::RAWRING;
     float* sR = reinterpret_cast<float*>(sm4);  // [RAWF][NPL] staged plane
-    float4* sN = sm4 + L::RAWSZ / 4;            // [3 slots][NGN][NPL]
+    float4* sN = sm4 + (RR ? 0 : L::RAWSZ / 4);  // [3 slots][NGN][NPL]
     float4* sC = sN + 3 * NGN * NPL;            // [2 slots][NGC][NCL]; fast arithmetic [NGCF][NCL]
     constexpr int NQ = L::NQ, NGCF = L::NGCF;
 #define RAW(f, i) sR[(f) * NPL + (i)]
@@ -835,7 +843,25 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
                 const int nj = n % FNJ, nk = n / FNJ;
                 const int j = j0 - 1 + nj, k = k0 - 1 + nk;
                 const bool ok = j <= g.nm[0] && k <= g.nm[1] && l >= 1 && l <= g.nm[2];
-                if (ok) {
+                if (RR) {
+                    // ring slot of plane l: group 0 (u, gam), group 1 (v, z)
+                    float* d0 = reinterpret_cast<float*>(sN + (l % 3) * (NGN * NPL) + n);
+                    float* d1 = reinterpret_cast<float*>(sN + (l % 3) * (NGN * NPL) + NPL + n);
+                    if (ok) {
+                        const long long q = g.idx(j, k, l);
+#pragma unroll
+                        for (int c = 0; c < 3; c++) {
+                            cp_async4(d0 + c, A.uin[c] + q);
+                            cp_async4(d1 + c, A.vin[c] + q);
+                        }
+                        cp_async4(d0 + 3, A.gam + q);
+                        if (GEOM == GEOM_TERRAIN) cp_async4(d1 + 3, A.x[2] + q);
+                        else d1[3] = 0.f;
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < 4; c++) { d0[c] = 0.f; d1[c] = 0.f; }
+                    }
+                } else if (ok) {
                     const long long q = g.idx(j, k, l);
 #pragma unroll
                     for (int c = 0; c < 3; c++) {
@@ -959,6 +985,15 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
                 } else {
                     a = p[0];
                     b = p[NPL];
+                    if constexpr (RR) {
+                        // raw (u, gam), (v, z) -> (w, z), (hourglass input, 0):
+                        // w1 = u + gam * v (time_integration.f90:36) and
+                        // hg1 u + dt hg2 v (acceleration.f90:141)
+                        const float4 u = a, v = b;
+                        a = make_float4(fmaf(u.w, v.x, u.x), fmaf(u.w, v.y, u.y), fmaf(u.w, v.z, u.z), v.w);
+                        b = make_float4(fmaf(A.dh2, v.x, A.hg1 * u.x), fmaf(A.dh2, v.y, A.hg1 * u.y),
+                                        fmaf(A.dh2, v.z, A.hg1 * u.z), 0.f);
+                    }
                 }
                 if (CARRY && n >= 4) {
                     ca[n - 4] = a;
@@ -1601,12 +1636,57 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
         }
 #pragma unroll
         for (int i = 0; i < 3; i++) fc[i] = fl[i];
-        if (finish) finish_node<FM>(A, g.idx(jn, kn, l), jn, kn, l, fu, cur[4], uv, dt, st_a, st_v, st_u);
+        if (!finish) return;
+        if constexpr (RR) {
+            // this node's raw u, v from ring slot l
+            const float4* pn = sN + (l % 3) * (NGN * NPL) + (tx + 1) + FNJ * (ty + 1);
+            const float4 a = pn[0], b = pn[NPL];
+            const float uvl[6] = {a.x, a.y, a.z, b.x, b.y, b.z};
+            finish_node<FM>(A, g.idx(jn, kn, l), jn, kn, l, fu, cur[4], uvl, dt, st_a, st_v, st_u);
+        } else {
+            finish_node<FM>(A, g.idx(jn, kn, l), jn, kn, l, fu, cur[4], uv, dt, st_a, st_v, st_u);
+        }
     };
 
     // ---------------------------------------------------------------- stream
     // ring: planes L0-1, L0, L0+1; staged: L0+2 in flight
     constexpr std::integral_constant<bool, FASTK> path{};
+    if constexpr (RR) {
+        // raw ring: planes L0-1, L0, L0+1 straight into their slots; plane
+        // l + 3 goes into slot l once cells(l) and nodes(l) are done with it
+#pragma unroll 1
+        for (int p = -1; p <= 1; p++) fetch(L0 + p);
+        cp_async_wait_all();
+        __syncthreads();
+        stat_load(L0 - 1, cur);
+        cells(L0 - 1, path);
+        __syncthreads();  // cell plane L0-1 complete: its terms for node L0
+        nodes_fm(L0 - 1, false);
+        __syncthreads();  // one cell slot: read before cells(L0) overwrites it; slot L0-1 free
+        fetch(L0 + 2);
+        stat_load(L0, cur);
+#pragma unroll 1
+        for (int l = L0; l <= L1; l++) {
+            cells(l, path);
+            float nxt[5];
+            stat_load(l + 1, nxt);
+            cp_async_wait_all();
+            __syncthreads();  // cell plane l complete, plane l+2 landed
+            nodes_fm(l, true);
+            __syncthreads();  // cell plane and ring slot l free
+            fetch(l + 3);
+#pragma unroll
+            for (int i = 0; i < 5; i++) cur[i] = nxt[i];
+        }
+        cp_async_wait_all();
+        if (A.stats) {
+            bmax(A.red + 0, st_a);
+            bmax(A.red + 1, st_v);
+            bmax(A.red + 2, st_u);
+            bmax(A.red + 3, st_w);
+        }
+        return;
+    }
 #pragma unroll 1
     for (int p = -1; p <= 1; p++) {
         fetch(L0 + p);
