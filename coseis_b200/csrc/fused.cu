@@ -952,6 +952,9 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
     // ---------------------------------------------------------------- cell phase
     constexpr bool CARRY = FM && GEOM != GEOM_GENERAL;
     float4 ca[4], cb[4];  // plane l+1 corners of the last cell computed, for plane l+1's cell
+    // fast arithmetic: the terms of this thread's own cell for its own node
+    // column (reader q = 0) stay in registers for the node phase
+    float ownu[3] = {0.f, 0.f, 0.f}, ownl[3] = {0.f, 0.f, 0.f};
     int carry_l = -1000;  // the plane of that cell
     auto cells = [&](int l, auto fast_tag) {
         constexpr bool F = decltype(fast_tag)::value;
@@ -960,6 +963,8 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
         if (!valid) {
             if constexpr (FM) {
                 zero_cell_fr(sC, tid, NCL);
+#pragma unroll
+                for (int i = 0; i < 3; i++) { ownu[i] = 0.f; ownl[i] = 0.f; }
             } else {
                 float4* cw = sC + cs * (NGC * NCL) + tid;
 #pragma unroll
@@ -1342,6 +1347,11 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
                         fu[ic] = fmaf(S[comp], Bu[id], fu[ic]);
                         fl[ic] = fmaf(S[comp], Bl[id], fl[ic]);
                     }
+                if (q == 0) {
+#pragma unroll
+                    for (int i = 0; i < 3; i++) { ownu[i] = fu[i]; ownl[i] = fl[i]; }
+                    continue;
+                }
                 sC[q * NCL + tid] = make_float4(fu[0], fu[1], fu[2], fl[0]);
                 reinterpret_cast<float2*>(sC + 4 * NCL)[q * NCL + tid] = make_float2(fl[1], fl[2]);
             }
@@ -1615,24 +1625,20 @@ __global__ void __launch_bounds__(NTH, GEOM == GEOM_GENERAL ? 1 : 2) k_interior(
         if (!outcol) return;
         // the four cells of plane l around the node column: their terms for
         // node l (above them) and for node l + 1 (below), the latter carried
-        float fu[3] = {fc[0], fc[1], fc[2]}, fl[3];
+        // q = 0 is this thread's own cell, whose terms are in registers
+        float fu[3] = {fc[0] + ownu[0], fc[1] + ownu[1], fc[2] + ownu[2]};
+        float fl[3] = {ownl[0], ownl[1], ownl[2]};
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
+        for (int q = 1; q < 4; q++) {
             const int ci = tid + (q & 1) + FJ * (q >> 1);  // the cell (J + cj, K + ck)
             const float4 a = sC[q * NCL + ci];
             const float2 b = reinterpret_cast<const float2*>(sC + 4 * NCL)[q * NCL + ci];
             fu[0] = fu[0] + a.x;
             fu[1] = fu[1] + a.y;
             fu[2] = fu[2] + a.z;
-            if (q == 0) {
-                fl[0] = a.w;
-                fl[1] = b.x;
-                fl[2] = b.y;
-            } else {
-                fl[0] = fl[0] + a.w;
-                fl[1] = fl[1] + b.x;
-                fl[2] = fl[2] + b.y;
-            }
+            fl[0] = fl[0] + a.w;
+            fl[1] = fl[1] + b.x;
+            fl[2] = fl[2] + b.y;
         }
 #pragma unroll
         for (int i = 0; i < 3; i++) fc[i] = fl[i];
