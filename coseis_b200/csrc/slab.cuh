@@ -153,6 +153,22 @@ __global__ void __launch_bounds__(SJ * SK, GEOM == GEOM_GENERAL ? 1 : 2) k_slab(
             zero_cell_fm<NDIR, NQ>(sC, tid, NCL_);
             return;
         }
+        // one damped axis (classes 1, 2, 4): this cell's g memory is loaded
+        // first, so its latency passes under the corner loads and brackets
+        constexpr bool PF = MASK == 1 || MASK == 2 || MASK == 4;
+        constexpr int PD = MASK == 1 ? 0 : MASK == 2 ? 1 : 2;
+        float gpre[3] = {0.f, 0.f, 0.f};
+        if constexpr (PF) {
+            const bool pn = PD == 0 ? cnj : PD == 1 ? cnk : (DL && l <= g.i1pml[2]);
+            const bool pf = PD == 0 ? cfj : PD == 1 ? cfk : (DL && l >= g.i2pml[2] - 1);
+            if (pn || pf) {
+                const int c = PD == 0 ? J : PD == 1 ? K : l;
+                const int sb = pn ? PD : 3 + PD;
+#pragma unroll
+                for (int ic = 0; ic < 3; ic++)
+                    gpre[ic] = A.sl.g[sb][slab_idx(g, PD, A.sl.tg[sb], pn ? c - g.i1cell[PD] : g.i2cell[PD] - c, J, K, l, ic)];
+            }
+        }
         float Uc[3][8], Vc[3][8], Gc[8], X0[8], X1[8], X2[8];
         {
             const float4* p0 = sN + (l % 3) * (NGN * NPL_) + (tx + TNJ * ty);
@@ -249,7 +265,8 @@ __global__ void __launch_bounds__(SJ * SK, GEOM == GEOM_GENERAL ? 1 : 2) k_slab(
                         const int p = nr ? c + g.nnoff[id] : g.nn[id] - c - g.nnoff[id];
                         const int sb = nr ? id : 3 + id;
                         const long long gi = slab_idx(g, id, A.sl.tg[sb], nr ? c - g.i1cell[id] : g.i2cell[id] - c, J, K, l, ic);
-                        s = fmaf(A.pmlc[3 * g.npml + p - 1], s, A.pmlc[2 * g.npml + p - 1] * A.sl.g[sb][gi]);
+                        const float gm = PF ? gpre[ic] : A.sl.g[sb][gi];
+                        s = fmaf(A.pmlc[3 * g.npml + p - 1], s, A.pmlc[2 * g.npml + p - 1] * gm);
                         if (own) A.gout[sb][gi] = s;
                     }
                     sg[ic][id] = s;
@@ -360,6 +377,21 @@ __global__ void __launch_bounds__(SJ * SK, GEOM == GEOM_GENERAL ? 1 : 2) k_slab(
     float fcd[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
     auto nodes_fm = [&](int l, bool finish) {
         if (!outcol) return;
+        // one damped axis: this node's p memory is loaded first (see the
+        // cell phase's g memory)
+        constexpr bool PF = MASK == 1 || MASK == 2 || MASK == 4;
+        constexpr int PD = MASK == 1 ? 0 : MASK == 2 ? 1 : 2;
+        float ppre[3] = {0.f, 0.f, 0.f};
+        if constexpr (PF) {
+            const int c = PD == 0 ? jn : PD == 1 ? kn : l;
+            const bool nr = c <= g.i1pml[PD], fr = c >= g.i2pml[PD];
+            if (finish && (nr || fr)) {
+                const int sb = nr ? PD : 3 + PD;
+#pragma unroll
+                for (int ic = 0; ic < 3; ic++)
+                    ppre[ic] = A.sl.p[sb][slab_idx(g, PD, A.sl.tp[sb], nr ? c - g.i1node[PD] : g.i2node[PD] - c, jn, kn, l, ic)];
+            }
+        }
         float fu[3] = {fc[0], fc[1], fc[2]}, fl[3] = {0.f, 0.f, 0.f};
         float fud[3][3], fld[3][3];
 #pragma unroll
@@ -439,7 +471,7 @@ __global__ void __launch_bounds__(SJ * SK, GEOM == GEOM_GENERAL ? 1 : 2) k_slab(
 #pragma unroll
                 for (int ic = 0; ic < 3; ic++) {
                     float* P = A.sl.p[sb] + slab_idx(g, d, A.sl.tp[sb], nr ? c - g.i1node[d] : g.i2node[d] - c, jn, kn, l, ic);
-                    const float pv = *P;
+                    const float pv = PF ? ppre[ic] : *P;
                     const float s = fmaf(dn2, fud[d][ic], dn1 * pv);
                     *P = fmaf(dt, s, pv);
                     fu[ic] = fu[ic] + s;
