@@ -406,7 +406,7 @@ def adjoint_problem(shape=(128, 128, 128), nt=1200, nrec=32, seed=SEED, segment=
     at the centre with a Ricker wavelet of 2 Hz peak frequency ('ricker2',
     tau = 1 / (sqrt(2) pi f0), start time -0.25 s); 32 seeded surface
     receivers (vx, vy, vz every step); free surfaces on all faces (the
-    adjoint has no PML); checkpoints every 35 steps."""
+    configuration names no boundary); checkpoints every 35 steps."""
     from coseis_b200 import adjoint
     nx, ny, nz = shape
     rng = np.random.default_rng([seed, 3])
@@ -431,8 +431,11 @@ def run_adjoint_bench(device, nt=1200):
     """Cost of the misfit gradient against the forward run alone, all on the
     device clock: (adjoint forward with checkpoints + backward) / plain
     forward of the same problem; `value` with a checkpoint every 35 steps
-    (35 checkpoints, each segment recomputed), `stored` keeping every
-    state instead (no recomputation; 9.5 GB here)."""
+    (35 checkpoints, each segment recomputed while the adjoint pass runs
+    over the next), `stored` keeping every state instead (no
+    recomputation; 9.5 GB here), `binomial` binomial checkpointing with 35
+    kept states (the revolve schedule, recomputation and adjoint steps on
+    one stream)."""
     from coseis_b200 import _lib
     p, rho, vp, vs, m = adjoint_problem(nt=nt)
     work = tempfile.mkdtemp(prefix='sord_adjb_')
@@ -447,13 +450,16 @@ def run_adjoint_bench(device, nt=1200):
         t_fwd = s.last_step_ms()
         s.close()
         res = {}
-        for tag, seg in (('checkpointed', 35), ('stored', 1)):
+        for tag, seg in (('checkpointed', 35), ('stored', 1), ('binomial', -35)):
             d = os.path.join(work, tag)
             p.stage(rho, vp, vs, m, d)
             s = _lib.Solver(d, open(os.path.join(d, 'sord.in')).read(), device=device)
             s.set_arithmetic('reference')
             try:
-                s.adjoint_forward(seg)
+                if seg > 0:
+                    s.adjoint_forward(seg)
+                else:
+                    s.adjoint_forward_binomial(-seg)
                 t_af = s.last_step_ms()
                 tr = p.read_traces(d)
                 # misfit against observed traces 0.9 x the computed ones
@@ -464,11 +470,17 @@ def run_adjoint_bench(device, nt=1200):
                 s.close()
             ok = bool(np.isfinite(g['lam']).all() and np.abs(g['mu']).max() > 0)
             res[tag] = {'ratio': (t_af + t_b) / t_fwd, 'adjoint_forward_ms': t_af, 'backward_ms': t_b,
-                        'segment': seg, 'finite_gradients': ok}
+                        'finite_gradients': ok}
+            if seg > 0:
+                res[tag]['segment'] = seg
+            else:
+                res[tag]['snapshots'] = -seg
+                res[tag]['schedule_forward_steps'] = _lib.binomial_cost(nt, -seg)
         return {'metric': 'adjoint gradient cost / forward', 'value': res['checkpointed']['ratio'], 'unit': 'x',
                 'higher_is_better': False, 'forward_ms': t_fwd, 'arithmetic': 'reference',
                 'checkpointed': res['checkpointed'],
                 'stored': res['stored'],
+                'binomial': res['binomial'],
                 'workload': 'adjoint: 128^3 nodes, %d steps, seeded 10%% blob in rho/vp/vs, 32 receivers, '
                             'moment tensor with 2 Hz Ricker, free surfaces' % nt}
     finally:

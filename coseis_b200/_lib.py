@@ -17,6 +17,7 @@ SYMBOLS = [
     'sord_last_error', 'sord_error_string', 'sord_destroy',
     'sord_vector_max_noalloc', 'sord_run_ensemble', 'sord_adjoint_forward', 'sord_adjoint_backward',
     'sord_set_arithmetic', 'sord_get_arithmetic', 'sord_trim_memory', 'sord_adjoint_source_gradients',
+    'sord_adjoint_forward_binomial', 'sord_adjoint_binomial_cost',
     'sord_set_field', 'sord_create_part',
 ]
 
@@ -96,6 +97,10 @@ def load():
     lib.sord_run_ensemble.restype = ctypes.c_int
     lib.sord_adjoint_forward.argtypes = [P, ctypes.c_int]
     lib.sord_adjoint_forward.restype = ctypes.c_int
+    lib.sord_adjoint_forward_binomial.argtypes = [P, ctypes.c_int]
+    lib.sord_adjoint_forward_binomial.restype = ctypes.c_int
+    lib.sord_adjoint_binomial_cost.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]
+    lib.sord_adjoint_binomial_cost.restype = ctypes.c_int
     FP = ctypes.POINTER(ctypes.c_float)
     lib.sord_adjoint_backward.argtypes = [P, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(FP), IP,
                                           FP, FP, FP, FP, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
@@ -137,6 +142,15 @@ def run_ensemble(paths, device=0, nthreads=8):
     st = (ctypes.c_int * max(n, 1))()
     _check(lib.sord_run_ensemble(arr, n, device, nthreads, st))
     return list(st)[:n]
+
+
+def binomial_cost(nt, snapshots):
+    """Forward steps the binomial checkpointing schedule takes for nt steps
+    with `snapshots` kept states (the chain of states that the forward run
+    keeps included)."""
+    n = ctypes.c_longlong(0)
+    _check(load().sord_adjoint_binomial_cost(nt, snapshots, ctypes.byref(n)))
+    return n.value
 
 
 def trim_memory(device=0):
@@ -192,6 +206,11 @@ class Solver(object):
     def adjoint_forward(self, segment):
         """Whole forward run keeping a checkpoint every `segment` steps."""
         _check(load().sord_adjoint_forward(self._h, segment), self._h)
+
+    def adjoint_forward_binomial(self, snapshots):
+        """Whole forward run for a backward pass with binomial checkpointing
+        (at most `snapshots` kept states)."""
+        _check(load().sord_adjoint_forward_binomial(self._h, snapshots), self._h)
 
     def adjoint_backward(self, dtraces, nmoment):
         """dtraces: {receiver file name: dL/d(samples)}.  Returns a dict of

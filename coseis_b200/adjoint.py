@@ -15,10 +15,12 @@ setup (sord/material_model.f90:65-76, 120-134: mu = rho vs^2,
 lambda = rho vp^2 - 2 mu, yy = mu (lambda + mu) s / (lambda + 2 mu) with
 s = sqrt((dx^2 + dy^2 + dz^2) / 3) / 12; sord/material_resample.f90:16-18:
 mr = 1 / mean of rho V over the 8 cells around a node).  Material limits
-(``vp_min`` ...) are not differentiated; leave them unset.
+(``vp_min`` ...) are not differentiated; leave them unset.  With PML
+faces the damping profile is held fixed: give ``vpml`` a value (by default
+it follows the material's extremes).
 
-Supported runs: rectilinear mesh, no PML, no fault, boundary conditions
-that need no plane copies (free), every step a plain step.
+Supported runs: rectilinear mesh, no fault, boundary conditions that need
+no plane copies (free, PML), every step a plain step.
 """
 import math
 import os
@@ -49,14 +51,24 @@ class Problem(object):
                recomputation), 0 or None lets the library choose (1 when
                the states fit in half of the free device memory, else about
                sqrt(nt))
+    snapshots  if given, binomial checkpointing with at most this many
+               kept states instead of uniform segments
     """
 
-    def __init__(self, prm, source, receivers, segment=None, device=0):
+    def __init__(self, prm, source, receivers, segment=None, device=0, snapshots=None):
         self.prm = dict(prm)
         self.source = dict(source)
         self.receivers = [list(r) for r in receivers]
         self.segment = int(segment or 0)
+        self.snapshots = int(snapshots or 0)
         self.device = device
+
+    def forward(self, solver):
+        """The adjoint forward run on `solver` with this problem's schedule."""
+        if self.snapshots > 0:
+            solver.adjoint_forward_binomial(self.snapshots)
+        else:
+            solver.adjoint_forward(self.segment)
 
     @property
     def cells(self):
@@ -159,7 +171,8 @@ def _function():
         def forward(ctx, rho, vp, vs, moment, problem, position=None, delay=None):
             ctx.has_source = (position is not None, delay is not None)
             if position is not None or delay is not None:
-                problem = Problem(problem.prm, problem.source, problem.receivers, problem.segment, problem.device)
+                problem = Problem(problem.prm, problem.source, problem.receivers, problem.segment, problem.device,
+                                  problem.snapshots)
                 if position is not None:
                     problem.source['x'] = [float(a) for a in position.detach().cpu().numpy().ravel()]
                 if delay is not None:
@@ -171,7 +184,7 @@ def _function():
                               moment.detach().cpu().numpy(), d)
                 s = _lib.Solver(d, open(os.path.join(d, 'sord.in')).read(), device=problem.device)
                 try:
-                    s.adjoint_forward(problem.segment)
+                    problem.forward(s)
                     tr = problem.read_traces(d)
                 except Exception:
                     s.close()

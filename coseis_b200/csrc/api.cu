@@ -752,17 +752,19 @@ int sord_step(sord_handle* h, int nsteps) {
     return SORD_OK;
 }
 
-int sord_adjoint_forward(sord_handle* h, int segment) {
+static int adjoint_forward(sord_handle* h, int segment, int snapshots) {
     if (!h) return SORD_E_PARAM;
     Solver& s = h->s;
     try {
         SORD_CUDA(cudaSetDevice(s.device));
         if (s.nparts > 1) throw SordError(SORD_E_PARAM, "not available on a part of a partitioned run");
-        const int seg = adjoint_segment(s, segment);
-        adjoint_begin(s, seg);
+        if (snapshots < 0) throw SordError(SORD_E_PARAM, "adjoint: snapshots must be positive");
+        adjoint_begin(s, snapshots > 0 ? 0 : adjoint_segment(s, segment), snapshots);
         SORD_CUDA(cudaEventRecord(s.ev0, s.stream));
-        while (s.it < s.nt) {
-            const int n = std::min(seg, s.nt - s.it);
+        // run to each step whose state is kept; the last step before a
+        // checkpoint is not folded, so the state it leaves is that step's
+        for (int stop : adjoint_stops(s)) {
+            const int n = stop - s.it;
             for (int i = 0; i < n; i++) s.step(i == n - 1);
             adjoint_checkpoint(s);
         }
@@ -775,6 +777,19 @@ int sord_adjoint_forward(sord_handle* h, int segment) {
     } catch (const std::exception& e) {
         return fail(h, e);
     }
+    return SORD_OK;
+}
+
+int sord_adjoint_forward(sord_handle* h, int segment) { return adjoint_forward(h, segment, 0); }
+
+int sord_adjoint_forward_binomial(sord_handle* h, int snapshots) {
+    if (snapshots < 1) return h ? fail(h, SordError(SORD_E_PARAM, "adjoint: snapshots must be at least 1")) : SORD_E_PARAM;
+    return adjoint_forward(h, 0, snapshots);
+}
+
+int sord_adjoint_binomial_cost(int nt, int snapshots, long long* steps) {
+    if (nt < 0 || snapshots < 1 || !steps) return SORD_E_PARAM;
+    *steps = sordgpu::binomial_cost(nt, snapshots);
     return SORD_OK;
 }
 

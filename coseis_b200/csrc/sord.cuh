@@ -360,7 +360,9 @@ struct Solver {
 void smem_limit(const void* func, int bytes);
 void adjoint_free(Solver& s);
 int adjoint_segment(Solver& s, int seg);
-void adjoint_begin(Solver& s, int seg);
+void adjoint_begin(Solver& s, int seg, int snaps);
+const std::vector<int>& adjoint_stops(Solver& s);
+long long binomial_cost(int l, int s);
 void adjoint_checkpoint(Solver& s);
 void adjoint_backward(Solver& s, int nrec, const char* const* files, const float* const* dtrace, const int* ntrace,
                       float* glam, float* gmu, float* gyy, float* gmr, double* gmom, int nmom);

@@ -105,18 +105,35 @@ int sord_run_ensemble(const char* const* workdirs, int n, int device, int nthrea
 /* Adjoint (no reference counterpart: the reference computes no
  * derivatives).  Gradients of a misfit of '.>' velocity or displacement
  * receivers with respect to the per-cell moduli and node masses and to the
- * value of every '.' moment op, for runs on a rectilinear mesh without PML
- * or fault whose every step is a plain fused step (field-I/O outputs and '.'
- * moment/potency ops only).
+ * value of every '.' moment op, for runs on a rectilinear mesh without
+ * fault whose every step is a plain fused step (field-I/O outputs and '.'
+ * moment/potency ops only).  PML faces are supported (their cell and node
+ * memories are part of the state and have adjoints of their own) unless
+ * the bands of opposite faces meet; the damping profile is held fixed (set
+ * vpml, or it follows the material's extremes, which are not
+ * differentiated).
  *
  * sord_adjoint_forward runs the whole forward run of a fresh handle (it must
  * be at step 0), writing its outputs as sord_run does, and keeps the state
- * (u, v, a) every `segment` steps on the device.  Memory: about
- * 36 B x (nt / segment + segment) per node.  segment 1 keeps every state
+ * (u, v, a), and with PML the memories, every `segment` steps on the
+ * device.  Memory: about 36 B x (nt / segment + 2 segment) per node, plus
+ * the PML memories per state.  segment 1 keeps every state
  * and the backward pass recomputes nothing; segment 0 chooses 1 when all
  * states fit in half of the free device memory, else about sqrt(nt).  sord_last_step_ms gives the
  * device time of the call (and of sord_adjoint_backward after that one). */
 int sord_adjoint_forward(sord_handle* h, int segment);
+
+/* sord_adjoint_forward with binomial checkpointing (the revolve schedule)
+ * instead of uniform segments: at most `snapshots` states are kept on the
+ * device at any time, besides the last state and three work states, and
+ * the backward pass recomputes the others from them with the fewest
+ * forward steps that storage allows.  sord_adjoint_binomial_cost gives the
+ * forward steps the schedule takes for nt steps, counting the chain of
+ * kept states that the forward run itself provides.  With snapshots >= nt
+ * nothing is recomputed.  The backward pass is sord_adjoint_backward; it
+ * runs on one stream (no overlap of recomputation and adjoint steps). */
+int sord_adjoint_forward_binomial(sord_handle* h, int snapshots);
+int sord_adjoint_binomial_cost(int nt, int snapshots, long long* steps);
 
 /* Backward pass after sord_adjoint_forward: files[i] names the output file
  * of a '.>' receiver op on vx/vy/vz/ux/uy/uz and dtrace[i] holds dL/d(sample)

@@ -22,16 +22,21 @@ H_FD = 1e-3
 TOL = 1e-3
 
 
-def problem(segment=7):
+def problem(segment=7, pml=False, snapshots=None):
+    """Free surfaces on every face, or (pml) a free surface at l = 1 and a
+    4-node PML on the other five faces with a fixed damping velocity (vpml
+    derived from the material's extremes would move with the material)."""
     prm = {
         'shape': list(SHAPE) + [NT], 'delta': [100.0, 100.0, 100.0, 0.008],
         'bc1': ['free'] * 3, 'bc2': ['free'] * 3, 'npml': 0, 'hourglass': [1.0, 0.5], 'gam': [0.0],
         'tm0': -0.15, 'itstats': 10, 'itio': 20,
     }
+    if pml:
+        prm.update({'bc1': ['pml', 'pml', 'free'], 'bc2': ['pml'] * 3, 'npml': 4, 'vpml': 4500.0})
     src = {'x': [8.3, 7.6, 6.4], 'pulse': 'ricker2', 'tau': 0.05}
     rng = np.random.default_rng(7)
     rec = [[float(rng.uniform(2, SHAPE[0] - 3)), float(rng.uniform(2, SHAPE[1] - 3)), 0.0] for _ in range(4)]
-    return adjoint.Problem(prm, src, rec, segment=segment)
+    return adjoint.Problem(prm, src, rec, segment=segment, snapshots=snapshots)
 
 
 def model(seed):
@@ -105,9 +110,21 @@ def test_problem_stages_moment_and_receivers(tmp_path):
 @pytest.mark.gpu
 @pytest.mark.parametrize('segment', [7, 1], ids=['recompute', 'stored'])
 def test_adjoint_gradient_vs_finite_differences(segment, tmp_path, oracle_bins, gpu_lib):
+    fd_check(problem(segment), tmp_path, oracle_bins)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize('segment', [7, 1], ids=['recompute', 'stored'])
+def test_adjoint_pml_gradient_vs_finite_differences(segment, tmp_path, oracle_bins, gpu_lib):
+    """The PML adjoint (cell and node memories carried backwards, the
+    viscous PML hourglass), with receivers inside and outside the damped
+    bands, against central differences of the FP64 oracle."""
+    fd_check(problem(segment, pml=True), tmp_path, oracle_bins)
+
+
+def fd_check(p, tmp_path, oracle_bins):
     import torch
     exe = oracle_bins['f64']
-    p = problem(segment)
     rho0, vp0, vs0, m0 = model(11)
     obs = oracle_traces(p, *model(12), str(tmp_path / 'obs'), exe)
 
@@ -141,11 +158,10 @@ def test_adjoint_gradient_vs_finite_differences(segment, tmp_path, oracle_bins, 
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize('change,msg', [({'bc1': ['pml'] * 3, 'bc2': ['pml'] * 3, 'npml': 3}, 'no PML'),
-                                        ({'gridnoise': 0.05}, 'rectilinear')])
+@pytest.mark.parametrize('change,msg', [({'gridnoise': 0.05}, 'rectilinear')])
 def test_adjoint_rejects_unsupported_runs(change, msg, tmp_path, gpu_lib):
-    """PML and non-rectilinear meshes stay forward-only: the adjoint forward
-    refuses them with SORD_E_PARAM before running."""
+    """Non-rectilinear meshes stay forward-only: the adjoint forward refuses
+    them with SORD_E_PARAM before running."""
     from coseis_b200 import _lib
     p = problem()
     p.prm.update(change)
@@ -238,3 +254,59 @@ def test_autograd_source_position_and_delay(tmp_path, oracle_bins, gpu_lib):
     assert np.allclose(pos.grad.numpy(), ref, rtol=1e-5), (pos.grad, ref)
     assert abs(float(delay.grad) - g['delay'].sum()) <= 1e-5 * abs(g['delay'].sum())
     assert np.abs(args[0].grad.numpy()).max() > 0
+
+
+def test_binomial_cost_is_the_optimal_recursion():
+    """sord_adjoint_binomial_cost (the binomial schedule's forward steps, the
+    forward run included) against an exhaustive search over every split of
+    the checkpointing recursion: reversing steps (lo, hi] with S_lo and S_hi
+    kept and c free records costs min over m of (m - lo) + cost(m, hi, c - 1)
+    + cost(lo, m, c); with no free record each state is recomputed from
+    S_lo."""
+    from coseis_b200 import _lib
+    L, C = 60, 6
+    D = [[0] * (C + 1) for _ in range(L + 1)]
+    for l in range(2, L + 1):
+        D[l][0] = l * (l - 1) // 2
+        for c in range(1, C + 1):
+            D[l][c] = min(m + D[l - m][c - 1] + D[m][c] for m in range(1, l))
+    for l in range(1, L + 1):
+        for c in range(0, C + 1):
+            # snapshots = c + 1: S_0 and the c records the recursion may fill
+            assert _lib.binomial_cost(l, c + 1) == D[l][c], (l, c)
+    # with a record for every state each state is computed once
+    assert _lib.binomial_cost(600, 600) == 599
+
+
+def binomial_vs_stored(p_of, tmp_path, snapshots):
+    """Gradients of the binomial schedule equal those of keeping every state."""
+    from coseis_b200 import _lib
+    rho, vp, vs, m = model(11)
+    out = []
+    for tag, kw in (('stored', {'segment': 1}), ('binomial', {'snapshots': snapshots})):
+        p = p_of(**kw)
+        d = str(tmp_path / tag)
+        files = p.stage(rho, vp, vs, m, d)
+        s = _lib.Solver(d, open(os.path.join(d, 'sord.in')).read())
+        try:
+            p.forward(s)
+            tr = p.read_traces(d)
+            dtr = {f: (0.1 * tr[i // 3, i % 3]).astype(np.float32) for i, f in enumerate(files)}
+            out.append(s.adjoint_backward(dtr, 6))
+        finally:
+            s.close()
+    a, b = out
+    for k in ('lam', 'mu', 'yy', 'mr', 'moment'):
+        x, y = np.asarray(a[k], np.float64), np.asarray(b[k], np.float64)
+        assert np.linalg.norm(x - y) <= 1e-6 * np.linalg.norm(x), k
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize('pml', [False, True], ids=['free', 'pml'])
+@pytest.mark.parametrize('snapshots', [3, 6])
+def test_binomial_checkpointing_matches_stored_states(pml, snapshots, tmp_path, gpu_lib):
+    """Binomial checkpointing with 3 and 6 kept states over 40 steps (deep
+    recursions, records recomputed with no free record left) gives the
+    gradients of the run that keeps every state: the recomputed states are
+    the forward run's."""
+    binomial_vs_stored(lambda **kw: problem(pml=pml, **kw), tmp_path, snapshots)
