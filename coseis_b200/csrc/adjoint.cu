@@ -81,6 +81,7 @@ struct AdjointState {
     // recursion keeps, one more the state the forward run ends with;
     // recpos[r] = the step whose state record r holds (-1 free)
     int snaps = 0;
+    bool spent = false;         // the backward pass has run
     std::vector<int> recpos;
     std::vector<int> stops;     // forward: steps after which a state is kept
     float* work[3] = {};        // recomputation records
@@ -1151,14 +1152,17 @@ void adjoint_backward(Solver& s, int nrec, const char* const* files, const float
             throw SordError(SORD_E_STATE, "adjoint: no free checkpoint record");
         };
         // the adjoint steps hi, hi - 1, ..., lo + 1, with S_lo in record rlo,
-        // S_hi in record rhi and c more records free
+        // S_hi in record rhi and c more records free; record rhi is
+        // released once step hi has run, rlo stays with the caller
         std::function<void(int, int, int, int, int)> rev = [&](int lo, int hi, int c, int rlo, int rhi) {
             if (hi - lo == 1) {
                 adjoint_step(hi, A->ckpt[rhi], s.stream);
+                A->recpos[rhi] = -1;
                 return;
             }
             if (c == 0) {
                 adjoint_step(hi, A->ckpt[rhi], s.stream);
+                A->recpos[rhi] = -1;
                 for (int n = hi - 1; n > lo; n--) {
                     advance_to(A->ckpt[rlo], lo, n, A->work[2]);
                     adjoint_step(n, A->work[2], s.stream);
@@ -1172,15 +1176,15 @@ void adjoint_backward(Solver& s, int nrec, const char* const* files, const float
                 advance_to(A->ckpt[rlo], lo, m, A->ckpt[rm]);
             }
             rev(m, hi, c - 1, rm, rhi);
-            A->recpos[rhi] = -1;
             rev(lo, m, c, rlo, rm);
         };
-        const std::vector<int> kept = A->recpos;
+        // the records are reused as the recursion goes: one backward pass
+        // per forward run
+        if (A->spent) throw SordError(SORD_E_STATE, "adjoint: binomial checkpointing allows one backward pass per forward run");
+        A->spent = true;
         const int rend = rec_of(s.nt);
         if (rend < 0 || A->recpos[0] != 0) throw SordError(SORD_E_STATE, "adjoint: missing checkpoints");
         if (s.nt > 0) rev(0, s.nt, A->snaps - 1, 0, rend);
-        // the forward run's records stay for another backward pass
-        A->recpos = kept;
     } else {
         auto recompute = [&](int k) {
             const int n0 = k * seg, n1 = std::min(s.nt, n0 + seg);

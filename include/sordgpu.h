@@ -130,8 +130,9 @@ int sord_adjoint_forward(sord_handle* h, int segment);
  * forward steps that storage allows.  sord_adjoint_binomial_cost gives the
  * forward steps the schedule takes for nt steps, counting the chain of
  * kept states that the forward run itself provides.  With snapshots >= nt
- * nothing is recomputed.  The backward pass is sord_adjoint_backward; it
- * runs on one stream (no overlap of recomputation and adjoint steps). */
+ * nothing is recomputed.  The backward pass is sord_adjoint_backward, once
+ * per forward run (the records are reused as it goes); it runs on one
+ * stream (no overlap of recomputation and adjoint steps). */
 int sord_adjoint_forward_binomial(sord_handle* h, int snapshots);
 int sord_adjoint_binomial_cost(int nt, int snapshots, long long* steps);
 

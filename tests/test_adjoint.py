@@ -310,3 +310,59 @@ def test_binomial_checkpointing_matches_stored_states(pml, snapshots, tmp_path, 
     gradients of the run that keeps every state: the recomputed states are
     the forward run's."""
     binomial_vs_stored(lambda **kw: problem(pml=pml, **kw), tmp_path, snapshots)
+
+
+@pytest.mark.gpu
+def test_adjoint_eight_directions_larger_run(tmp_path, oracle_bins, gpu_lib):
+    """The adjoint configuration's check at a larger size: 48^3 nodes, 240
+    steps, a 10 % Gaussian blob in rho, vp and vs, a seeded moment tensor
+    with a 2 Hz Ricker wavelet, 16 surface receivers, binomial
+    checkpointing with 35 kept states; the gradient along 8 seeded random
+    directions in (rho, vp, vs, moment) together against central
+    differences (h = 1e-3 relative) of the FP64 oracle, bound 1e-3."""
+    import torch
+    exe = oracle_bins['f64']
+    threads = max(1, min(16, os.cpu_count() or 1))
+    n, nt = 48, 240
+    rng = np.random.default_rng(48)
+    prm = {'shape': [n, n, n, nt], 'delta': [100.0, 100.0, 100.0, 0.008], 'bc1': ['free'] * 3,
+           'bc2': ['free'] * 3, 'npml': 0, 'hourglass': [1.0, 1.0], 'gam': [0.0], 'tm0': -0.25,
+           'itstats': 10, 'itio': 60}
+    src = {'x': [n * 0.5 + 0.3, n * 0.5 - 0.2, n * 0.5 + 0.1], 'pulse': 'ricker2',
+           'tau': 1.0 / (math.sqrt(2.0) * math.pi * 2.0)}
+    rec = [[float(rng.uniform(2, n - 3)), float(rng.uniform(2, n - 3)), 0.0] for _ in range(16)]
+    p = adjoint.Problem(prm, src, rec, snapshots=35)
+    nc = (n - 1,) * 3
+    j, k, l = np.meshgrid(*[np.arange(c) + 0.5 for c in nc], indexing='ij')
+
+    def blob_model(seed):
+        r = np.random.default_rng(seed)
+        c = [r.uniform(0.3, 0.7) * m for m in nc]
+        b = np.exp(-((j - c[0]) ** 2 + (k - c[1]) ** 2 + (l - c[2]) ** 2) / (2 * 5.0 ** 2))
+        amp = r.choice([-0.1, 0.1], 3)
+        m = r.standard_normal(6)
+        m *= 1e16 / math.sqrt((m[:3] ** 2).sum() + 2 * (m[3:] ** 2).sum())
+        return [base * (1 + a * b) for base, a in zip((2700.0, 6000.0, 3464.0), amp)] + [m]
+
+    def traces(model, tag):
+        path = str(tmp_path / tag)
+        shutil.rmtree(path, ignore_errors=True)
+        p.stage(*model, path, realsize=8)
+        sc.run_oracle(path, exe, threads)
+        return p.read_traces(path, '<f8')
+
+    obs = traces(blob_model(2), 'obs')
+    base = blob_model(1)
+    t = [torch.tensor(x, dtype=torch.float32, requires_grad=True) for x in base]
+    tr = adjoint.ReceiverTraces.apply(t[0], t[1], t[2], t[3], p)
+    loss = 0.5 * ((tr.double() - torch.as_tensor(obs)) ** 2).sum()
+    loss.backward()
+    G = [x.grad.numpy().astype(np.float64) for x in t]
+    d_rng = np.random.default_rng(2025)
+    for q in range(8):
+        d = [d_rng.standard_normal(np.shape(x)) for x in base]
+        lp = 0.5 * ((traces([x * (1 + H_FD * dx) for x, dx in zip(base, d)], 'p') - obs) ** 2).sum()
+        lm = 0.5 * ((traces([x * (1 - H_FD * dx) for x, dx in zip(base, d)], 'm') - obs) ** 2).sum()
+        fd = (lp - lm) / (2 * H_FD)
+        an = sum((g * x * dx).sum() for g, x, dx in zip(G, base, d))
+        assert abs(an - fd) <= TOL * abs(fd), (q, an, fd)
