@@ -24,6 +24,7 @@ reference-order kernel (bit-identical to the FP32 oracle), reported as
 `reference_order`.
 """
 import argparse
+import copy
 import json
 import math
 import os
@@ -435,24 +436,35 @@ def run_adjoint_bench(device, nt=1200):
     over the next), `stored` keeping every state instead (no
     recomputation; 9.5 GB here), `binomial` binomial checkpointing with 35
     kept states (the revolve schedule, recomputation and adjoint steps on
-    one stream)."""
+    one stream); `pml` the same problem with a free surface at l = 1 and a
+    10-node PML on the other faces (the two-pass PML adjoint), a checkpoint
+    every 35 steps, against its own forward."""
     from coseis_b200 import _lib
     p, rho, vp, vs, m = adjoint_problem(nt=nt)
+    pp = copy.deepcopy(p)
+    pp.prm.update({'bc1': ['pml', 'pml', 'free'], 'bc2': ['pml'] * 3, 'npml': 10, 'vpml': 6000.0})
     work = tempfile.mkdtemp(prefix='sord_adjb_')
-    try:
-        d = os.path.join(work, 'fwd')
-        p.stage(rho, vp, vs, m, d)
+
+    def forward_ms(prob, tag):
+        d = os.path.join(work, tag)
+        prob.stage(rho, vp, vs, m, d)
         s = _lib.Solver(d, open(os.path.join(d, 'sord.in')).read(), device=device)
         # the adjoint kernels transpose the reference-order step; forward and
         # recomputation use that arithmetic here, so the ratio compares like with like
         s.set_arithmetic('reference')
         s.step(nt)
-        t_fwd = s.last_step_ms()
+        t = s.last_step_ms()
         s.close()
+        return t
+
+    try:
+        t_fwd = forward_ms(p, 'fwd')
+        t_fwd_pml = forward_ms(pp, 'fwd_pml')
         res = {}
-        for tag, seg in (('checkpointed', 35), ('stored', 1), ('binomial', -35)):
+        for tag, seg in (('checkpointed', 35), ('stored', 1), ('binomial', -35), ('pml', 35)):
+            prob, tf = (pp, t_fwd_pml) if tag == 'pml' else (p, t_fwd)
             d = os.path.join(work, tag)
-            p.stage(rho, vp, vs, m, d)
+            prob.stage(rho, vp, vs, m, d)
             s = _lib.Solver(d, open(os.path.join(d, 'sord.in')).read(), device=device)
             s.set_arithmetic('reference')
             try:
@@ -461,16 +473,18 @@ def run_adjoint_bench(device, nt=1200):
                 else:
                     s.adjoint_forward_binomial(-seg)
                 t_af = s.last_step_ms()
-                tr = p.read_traces(d)
+                tr = prob.read_traces(d)
                 # misfit against observed traces 0.9 x the computed ones
-                dtr = {f: 0.1 * tr[i // 3, i % 3] for i, f in enumerate(p.files())}
+                dtr = {f: 0.1 * tr[i // 3, i % 3] for i, f in enumerate(prob.files())}
                 g = s.adjoint_backward(dtr, 6)
                 t_b = s.last_step_ms()
             finally:
                 s.close()
             ok = bool(np.isfinite(g['lam']).all() and np.abs(g['mu']).max() > 0)
-            res[tag] = {'ratio': (t_af + t_b) / t_fwd, 'adjoint_forward_ms': t_af, 'backward_ms': t_b,
+            res[tag] = {'ratio': (t_af + t_b) / tf, 'adjoint_forward_ms': t_af, 'backward_ms': t_b,
                         'finite_gradients': ok}
+            if tag == 'pml':
+                res[tag]['forward_ms'] = tf
             if seg > 0:
                 res[tag]['segment'] = seg
             else:
@@ -481,6 +495,7 @@ def run_adjoint_bench(device, nt=1200):
                 'checkpointed': res['checkpointed'],
                 'stored': res['stored'],
                 'binomial': res['binomial'],
+                'pml': res['pml'],
                 'workload': 'adjoint: 128^3 nodes, %d steps, seeded 10%% blob in rho/vp/vs, 32 receivers, '
                             'moment tensor with 2 Hz Ricker, free surfaces' % nt}
     finally:

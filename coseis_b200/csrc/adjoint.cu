@@ -827,6 +827,8 @@ void adjoint_begin(Solver& s, int seg, int snaps) {
     adjoint_free(s);
     AdjointState* A = new AdjointState();
     s.adj = A;
+    // more snapshots than steps keep every state already
+    if (snaps > 0) snaps = std::min(snaps, std::max(s.nt, 1));
     A->seg = snaps > 0 ? 0 : seg;
     A->snaps = snaps;
     for (size_t i = 0; i < s.ops.size(); i++) {
