@@ -816,6 +816,8 @@ int binomial_split(int l, int s) {
 // included)
 long long binomial_cost(int l, int s) {
     if (l <= 1) return 0;
+    // one snapshot: every state is recomputed from the first
+    if (s <= 1) return (long long)l * (l - 1) / 2;
     int r = 0;
     while (beta(s, r, l) < l) r++;
     return (long long)r * l - beta(s + 1, r - 1, (long long)r * l);
