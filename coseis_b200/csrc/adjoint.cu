@@ -103,6 +103,10 @@ struct AdjArgs {
     float hg1, dh2, dt;
     int hourglass;
     int nbx, segl;                    // tiles along j, node planes per block
+    // the nodes this kernel updates (and the cells, by lower corner, whose
+    // gradients it accumulates): all force nodes, or with PML the box whose
+    // 8 cells and their corners lie outside every PML band
+    int box1[3], box2[3];
 };
 
 __device__ __forceinline__ bool in_nodes(const Geom& g, int j, int k, int l) {
@@ -145,8 +149,8 @@ __global__ void __launch_bounds__(AJ * AK, 2) k_adj_step(AdjArgs A) {
     const float dt = A.dt;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + AJ * ty;
     const int bx = blockIdx.x % A.nbx, by = blockIdx.x / A.nbx;
-    const int j0 = g.i1node[0] + bx * (AJ - 1), k0 = g.i1node[1] + by * (AK - 1);
-    const int L0 = g.i1node[2] + blockIdx.y * A.segl, L1 = min(L0 + A.segl - 1, g.i2node[2]);
+    const int j0 = A.box1[0] + bx * (AJ - 1), k0 = A.box1[1] + by * (AK - 1);
+    const int L0 = A.box1[2] + blockIdx.y * A.segl, L1 = min(L0 + A.segl - 1, A.box2[2]);
     const int J = j0 - 1 + tx, K = k0 - 1 + ty;  // this thread's cell column
 
     auto issue = [&](int p) {
@@ -261,7 +265,7 @@ __global__ void __launch_bounds__(AJ * AK, 2) k_adj_step(AdjArgs A) {
 #pragma unroll
             for (int f = 6; f < ACF; f++) o[f * ANC] = 0.f;
         }
-        if (own && tx >= 1 && ty >= 1) {
+        if (own && tx >= 1 && ty >= 1 && J <= A.box2[0] && K <= A.box2[1]) {
             A.glam[q] = A.glam[q] + st * tr;
             A.gmu[q] = A.gmu[q] + 2.0f * (sd[0] * ed[0] + sd[1] * ed[1] + sd[2] * ed[2]) +
                        2.0f * (so[0] * eo[0] + so[1] * eo[1] + so[2] * eo[2]);
@@ -271,7 +275,7 @@ __global__ void __launch_bounds__(AJ * AK, 2) k_adj_step(AdjArgs A) {
 
     auto nodes = [&](int l) {
         const int jn = j0 + tx, kn = k0 + ty;
-        if (tx >= AJ - 1 || ty >= AK - 1 || jn > g.i2node[0] || kn > g.i2node[1]) return;
+        if (tx >= AJ - 1 || ty >= AK - 1 || jn > A.box2[0] || kn > A.box2[1]) return;
         const float* c0 = sC + ((l - 1) & 1) * (ACF * ANC);  // cell plane l - 1
         const float* c1 = sC + (l & 1) * (ACF * ANC);        // cell plane l
         // cells at minus the corner offsets: smem cell (tx + 1 - dj, ty + 1 - dk)
@@ -380,7 +384,11 @@ struct AdjPmlArgs {
     float* cs;                        // CS_COUNT cell volumes
     float hg1, dh2, dt;
     int hourglass, hgvisc;
+    int box1[3], box2[3];             // the nodes k_adj_step updates (see AdjArgs)
 };
+__device__ __forceinline__ bool node_in_box(const int* b1, const int* b2, int j, int k, int l) {
+    return j >= b1[0] && j <= b2[0] && k >= b1[1] && k <= b2[1] && l >= b1[2] && l <= b2[2];
+}
 
 // Slab element of cell or node (j, k, l), component ic: the slab of axis
 // `axis` has thickness t along it and ii counts from the face
@@ -417,6 +425,11 @@ __global__ void __launch_bounds__(128) k_adjp_cells(AdjPmlArgs A) {
     const int K = g.i1cell[1] + blockIdx.y * blockDim.y + threadIdx.y;
     const int L = g.i1cell[2] + blockIdx.z * blockDim.z + threadIdx.z;
     if (J > g.i2cell[0] || K > g.i2cell[1] || L > g.i2cell[2]) return;
+    // cells whose 8 corners k_adj_step updates are its alone; of the others
+    // this pass writes the scratch values, and the gradients of those that
+    // k_adj_step does not own (by lower corner)
+    if (node_in_box(A.box1, A.box2, J, K, L) && node_in_box(A.box1, A.box2, J + 1, K + 1, L + 1)) return;
+    const bool grad = !node_in_box(A.box1, A.box2, J, K, L);
     const long long q = g.idx(J, K, L);
     const long long nv = g.nv;
     const float dt = A.dt, r = A.vc[q], lm = A.lam[q], m2 = 2.0f * A.mu[q], yc = A.yy[q];
@@ -515,9 +528,11 @@ __global__ void __launch_bounds__(128) k_adjp_cells(AdjPmlArgs A) {
             else eo[3 - ic - id] = eo[3 - ic - id] + 0.5f * G;
         }
     }
-    A.glam[q] = A.glam[q] + st * (ed[0] + ed[1] + ed[2]);
-    A.gmu[q] = A.gmu[q] + 2.0f * (sd[0] * ed[0] + sd[1] * ed[1] + sd[2] * ed[2]) +
-               2.0f * (so[0] * eo[0] + so[1] * eo[1] + so[2] * eo[2]);
+    if (grad) {
+        A.glam[q] = A.glam[q] + st * (ed[0] + ed[1] + ed[2]);
+        A.gmu[q] = A.gmu[q] + 2.0f * (sd[0] * ed[0] + sd[1] * ed[1] + sd[2] * ed[2]) +
+                   2.0f * (so[0] * eo[0] + so[1] * eo[1] + so[2] * eo[2]);
+    }
     if (!A.hourglass) return;
     const bool inE = J >= g.i1pml[0] && J <= g.i2pml[0] - 1 && K >= g.i1pml[1] && K <= g.i2pml[1] - 1 &&
                      L >= g.i1pml[2] && L <= g.i2pml[2] - 1;
@@ -544,7 +559,7 @@ __global__ void __launch_bounds__(128) k_adjp_cells(AdjPmlArgs A) {
             A.cs[(CS_HV + 3 * iq + ic) * nv + q] = A.dh2 * (yc * sv);
         }
     }
-    A.gyy[q] = A.gyy[q] + gy;
+    if (grad) A.gyy[q] = A.gyy[q] + gy;
 }
 
 __global__ void __launch_bounds__(128) k_adjp_nodes(AdjPmlArgs A) {
@@ -553,6 +568,7 @@ __global__ void __launch_bounds__(128) k_adjp_nodes(AdjPmlArgs A) {
     const int k = g.i1node[1] + blockIdx.y * blockDim.y + threadIdx.y;
     const int l = g.i1node[2] + blockIdx.z * blockDim.z + threadIdx.z;
     if (j > g.i2node[0] || k > g.i2node[1] || l > g.i2node[2]) return;
+    if (node_in_box(A.box1, A.box2, j, k, l)) return;  // k_adj_step's node
     const long long q = g.idx(j, k, l);
     const long long nv = g.nv;
     const float dt = A.dt;
@@ -635,10 +651,18 @@ __global__ void __launch_bounds__(128) k_adjp_nodes(AdjPmlArgs A) {
 }
 
 // dL/d(moment op value) with PML: the cell pass left vc sigmabar per cell.
-__global__ void k_adjp_moment(const float* __restrict__ sig, long long nv, const MomEntry* e, int n, double* gmom) {
+// A cell (by linear index) whose 8 corners all lie in the node box [b1, b2].
+__device__ __forceinline__ bool cell_in_box(const Geom& g, long long idx, const int* b1, const int* b2) {
+    const int j = (int)(idx % g.sy) + 1, k = (int)((idx / g.sy) % g.nm[1]) + 1, l = (int)(idx / g.sz) + 1;
+    return j >= b1[0] && j + 1 <= b2[0] && k >= b1[1] && k + 1 <= b2[1] && l >= b1[2] && l + 1 <= b2[2];
+}
+// The entries whose cell has a corner outside the box of the fused kernel
+// (k_adj_moment takes the others).
+__global__ void k_adjp_moment(AdjArgs K, const float* __restrict__ sig, const MomEntry* e, int n, double* gmom) {
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const MomEntry E = e[i];
-        atomicAdd(gmom + E.slot, (double)(sig[E.comp * nv + E.idx] * E.w));
+        if (cell_in_box(K.g, E.idx, K.box1, K.box2)) continue;
+        atomicAdd(gmom + E.slot, (double)(sig[E.comp * K.g.nv + E.idx] * E.w));
     }
 }
 
@@ -649,6 +673,7 @@ __global__ void k_adj_moment(AdjArgs A, const MomEntry* e, int n, double* gmom) 
     const float h = g.h;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const MomEntry E = e[i];
+        if (!cell_in_box(g, E.idx, A.box1, A.box2)) continue;
         float F[3][8];
         for (int t = 0; t < 8; t++) {
             const int ct = t & 1, lt = (t >> 1) & 1, kt = (t >> 2) & 1;
@@ -1020,9 +1045,24 @@ void adjoint_backward(Solver& s, int nrec, const char* const* files, const float
     // tiles over the force nodes; planes split so that each SM gets a few blocks
     int sms = 148;
     SORD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s.device));
-    K.nbx = (g.i2node[0] - g.i1node[0] + AJ - 1) / (AJ - 1);
-    const int nby = (g.i2node[1] - g.i1node[1] + AK - 1) / (AK - 1);
-    const int planes = g.i2node[2] - g.i1node[2] + 1;
+    // the nodes of the fused kernel: all force nodes, or with PML those two
+    // nodes or more inside every band (their cells and the cells' corners
+    // carry no PML term); the two-pass kernels take the rest
+    bool fused_box = true;
+    for (int d = 0; d < 3; d++) {
+        K.box1[d] = g.i1node[d];
+        K.box2[d] = g.i2node[d];
+        if (A->pml) {
+            if (g.i1pml[d] >= g.i1node[d]) K.box1[d] = g.i1pml[d] + 2;
+            if (g.i2pml[d] <= g.i2node[d]) K.box2[d] = g.i2pml[d] - 2;
+        }
+        if (K.box1[d] > K.box2[d]) fused_box = false;
+    }
+    if (!fused_box)
+        for (int d = 0; d < 3; d++) { K.box1[d] = 1; K.box2[d] = 0; }
+    K.nbx = std::max(1, (K.box2[0] - K.box1[0] + AJ - 1) / (AJ - 1));
+    const int nby = std::max(1, (K.box2[1] - K.box1[1] + AK - 1) / (AK - 1));
+    const int planes = std::max(1, K.box2[2] - K.box1[2] + 1);
     const int nsg = std::max(1, std::min((4 * sms + K.nbx * nby - 1) / (K.nbx * nby), planes / 8));
     K.segl = (planes + nsg - 1) / nsg;
     const dim3 agrid((unsigned)(K.nbx * nby), (unsigned)((planes + K.segl - 1) / K.segl));
@@ -1042,6 +1082,7 @@ void adjoint_backward(Solver& s, int nrec, const char* const* files, const float
     KP.hg1 = K.hg1; KP.dh2 = K.dh2; KP.dt = K.dt;
     KP.hourglass = K.hourglass;
     KP.hgvisc = (s.prm.hourglass[1] > 0.f && g.npml > 0) ? 1 : 0;
+    for (int d = 0; d < 3; d++) { KP.box1[d] = K.box1[d]; KP.box2[d] = K.box2[d]; }
     const dim3 pblock(32, 4, 1);
     auto pgrid = [&](const int* i1, const int* i2) {
         return dim3((unsigned)((i2[0] - i1[0] + 32) / 32), (unsigned)((i2[1] - i1[1] + 4) / 4), (unsigned)(i2[2] - i1[2] + 1));
@@ -1105,8 +1146,15 @@ void adjoint_backward(Solver& s, int nrec, const char* const* files, const float
                 KP.ubi[i] = K.ubi[i]; KP.vbi[i] = K.vbi[i]; KP.ubo[i] = K.ubo[i]; KP.vbo[i] = K.vbo[i];
             }
             for (int i = 0; i < 6; i++) KP.gf[i] = st + A->gofs[i];
+            // the fused kernel on the nodes away from the PML, the two
+            // passes on the rest (they write disjoint nodes and cells)
+            if (fused_box) {
+                if (nme > 0) k_adj_moment<<<1, 128, 0, as>>>(K, A->mom + moff[n], nme, A->gmom);
+                k_adj_step<<<agrid, dim3(AJ, AK), kAdjSmem, as>>>(K);
+                s.launches += 1 + (nme > 0 ? 1 : 0);
+            }
             k_adjp_cells<<<pcgrid, pblock, 0, as>>>(KP);
-            if (nme > 0) k_adjp_moment<<<1, 128, 0, as>>>(A->cs + (size_t)CS_SIG * nv, (long long)nv, A->mom + moff[n], nme, A->gmom);
+            if (nme > 0) k_adjp_moment<<<1, 128, 0, as>>>(K, A->cs + (size_t)CS_SIG * nv, A->mom + moff[n], nme, A->gmom);
             k_adjp_nodes<<<pngrid, pblock, 0, as>>>(KP);
             s.launches++;
         } else {
