@@ -575,10 +575,10 @@ void Solver::destroy() {
     if (stream) cudaStreamSynchronize(stream);
     writer_free(*this);
     auto fr = [this](void* p) { dev_free(*this, p); };
-    for (int i = 0; i < 3; i++) { fr(d.x[i]); fr(d.v[i]); fr(d.u[i]); fr(d.w1n[i]); fr(d.sd[i]); fr(d.so[i]); }
-    fr(d.vc); fr(d.mr); fr(d.lam); fr(d.mu); fr(d.gam); fr(d.yy); fr(d.s1); fr(d.s2); fr(d.pmlc); fr(d.red); fr(d.inj); fr(d.fp);
+    // the volume fields live in d.vol
+    if (!d.vol_plain) fr(d.vol);
+    fr(d.pmlc); fr(d.red); fr(d.inj); fr(d.fp);
     for (int i = 0; i < 6; i++) { fr(d.slabs.p[i]); fr(d.slabs.g[i]); fr(d.gb[i]); }
-    for (int i = 0; i < 3; i++) { fr(d.vb[i]); fr(d.ub[i]); }
     fr(d.x1d); fr(d.y1d); fr(xbuf);
     for (auto& io : ops) fr(io.dbuf);
     probes_free(*this);
@@ -600,6 +600,8 @@ void Solver::destroy() {
         cudaStreamSynchronize(stream);
         cudaStreamDestroy(stream);
     }
+    if (d.vol && d.vol_plain) cudaFree(d.vol);
+    d.vol = nullptr;
     if (mem_attached) mem_detach(device);
     mem_attached = false;
     hinj = nullptr;

@@ -376,14 +376,25 @@ static void setup_dimensions(Solver& s) {
 static void allocate_arrays(Solver& s) {
     long long nv = s.g.nv;
     Device& d = s.d;
-    for (int i = 0; i < 3; i++) {
-        alloc(s, &d.x[i], nv); alloc(s, &d.v[i], nv); alloc(s, &d.u[i], nv); alloc(s, &d.w1n[i], nv);
-        alloc(s, &d.sd[i], nv); alloc(s, &d.so[i], nv);
+    // the volume fields: one zeroed block, each field at a 256-byte boundary
+    float** const fields[29] = {&d.x[0], &d.x[1], &d.x[2], &d.v[0], &d.v[1], &d.v[2], &d.u[0], &d.u[1], &d.u[2],
+                                &d.w1n[0], &d.w1n[1], &d.w1n[2], &d.sd[0], &d.sd[1], &d.sd[2], &d.so[0], &d.so[1],
+                                &d.so[2], &d.vc, &d.mr, &d.lam, &d.mu, &d.gam, &d.yy, &d.s1, &d.s2,
+                                &d.vb[0], &d.vb[1], &d.vb[2]};
+    const size_t pitch = ((size_t)std::max(nv, 1LL) + 63) / 64 * 64;  // floats
+    const size_t total = pitch * (29 + 3);                            // + ub[3]
+    d.vol_plain = sizeof(float) * total >= ((size_t)4 << 30);
+    cudaError_t e = d.vol_plain ? cudaMalloc(&d.vol, sizeof(float) * total) : dev_malloc(s, &d.vol, sizeof(float) * total);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        d.vol = nullptr;
+        throw SordError(SORD_E_NOMEM, std::string("device memory for the volume fields: ") + cudaGetErrorString(e));
     }
-    alloc(s, &d.vc, nv); alloc(s, &d.mr, nv); alloc(s, &d.lam, nv); alloc(s, &d.mu, nv); alloc(s, &d.gam, nv);
-    alloc(s, &d.yy, nv); alloc(s, &d.s1, nv); alloc(s, &d.s2, nv);
+    SORD_CUDA(cudaMemsetAsync(d.vol, 0, sizeof(float) * total, s.stream));
+    float* base = (float*)d.vol;
+    for (int i = 0; i < 29; i++) *fields[i] = base + (size_t)i * pitch;
+    for (int i = 0; i < 3; i++) d.ub[i] = base + (size_t)(29 + i) * pitch;
     alloc(s, &d.red, kRedFloats);
-    for (int i = 0; i < 3; i++) { alloc(s, &d.vb[i], nv); alloc(s, &d.ub[i], nv); }
     const char* fz = getenv("SORD_FUSED");
     s.use_fused = !(fz && fz[0] == '0');
     const char* ar = getenv("SORD_ARITHMETIC");

@@ -197,6 +197,13 @@ struct Device {
     // fault plane (nm with extent 1 along ifn)
     long long np = 0;
     float* fp = nullptr;                 // all fault arrays in one allocation
+    // the 32 volume fields (x .. ub above) are carved from one block; from
+    // 4 GiB up a plain cudaMalloc (vol_plain): growing the stream-ordered
+    // pool by 26 GB took about 0.16 s and returning it as long again, a
+    // cudaMalloc of the same size about 2 ms; smaller blocks come from the
+    // pool, which concurrent handles reuse without synchronising the device
+    void* vol = nullptr;
+    bool vol_plain = false;
 };
 
 // Fault-plane arrays (dynamic_rupture.f90:22-63), offsets into Device::fp.
