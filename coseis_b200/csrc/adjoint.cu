@@ -360,7 +360,11 @@ __global__ void __launch_bounds__(AJ * AK, 2) k_adj_step(AdjArgs A) {
 // writes the cell's routed strain adjoints and hourglass values to a scratch
 // volume, and a node pass (one thread per node) that gathers them from the 8
 // cells into ubar, vbar and advances pbar.  Cells and nodes each have one
-// owner, so gbar and pbar are updated in place.
+// owner, so gbar and pbar are updated in place.  The nodes two or more
+// inside every band (box1..box2: their cells and the cells' corners carry
+// no PML term) are left to k_adj_step, which runs restricted to that box;
+// the passes skip them, and the cells that k_adj_step owns keep their
+// gradients from it.
 enum {
     CS_Y = 0,     // 9: routed strain adjoint of pair (ic, id) at 3 ic + id
     CS_HE = 9,    // 12: yy sbar of the stiffness-plus-viscous hourglass (3 iq + ic)
